@@ -29,7 +29,7 @@ def load_library(path=LIB_PATH):
     if not os.path.exists(path):
         raise RuntimeError(
             "libeqg.so is not built (%s); run `python -c \"import __graft_entry__ as g; g.build()\"`" % path)
-    lib = capi.bind(ctypes.CDLL(path, mode=ctypes.RTLD_GLOBAL))
+    lib = capi.bind(ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL))
     if path == LIB_PATH:
         _lib = lib
     return lib

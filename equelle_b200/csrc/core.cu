@@ -1,0 +1,494 @@
+// Runtime core: device memory pool, stream, and the Cartesian grid with its
+// helper operators, built on the device once per runtime.
+//
+// Grid numbering is OPM's UnstructuredGrid for Cartesian grids (used by the
+// reference through Opm::GridManager, EquelleRuntimeCPU.cpp:20-49; 2D
+// numbering pinned by backends/cuda/test/gridTest.cpp:104-144): I faces
+// (i fastest, then j, then k), then J faces, then K faces; face_cells =
+// (lower/left neighbour or -1, upper/right neighbour or -1).  Geometry is
+// computed from node coordinates x_i = i*dx as the grid builder does, with
+// explicitly rounded operations so no fused multiply-add changes a value.
+// Helper operators follow Opm::HelperOps (restated in
+// backends/cuda/src/deviceHelperOps.cpp:84-148): grad = -ngrad with ngrad
+// rows (+1 first, -1 second) over interior faces, div = ngrad^T, fulldiv =
+// fullngrad^T over all faces.
+#include "eqg_internal.cuh"
+
+#include <cub/cub.cuh>
+
+#include <cstring>
+
+namespace eqg {
+
+DevBuf::~DevBuf()
+{
+    if (ptr && core) core->free(ptr, bytes);
+}
+
+Core::Core()
+{
+    EQG_CUDA(cudaGetDevice(&device));
+    EQG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    EQG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t threshold = UINT64_MAX;  // keep freed blocks cached in the pool
+    EQG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    EQG_CUDA(cudaMallocHost(&pinned, 64 * sizeof(double)));
+}
+
+Core::~Core()
+{
+    // Release cached device objects before the stream goes away.
+    for (auto& kv : derived_sets) eqg_set_release(kv.second);
+    derived_sets.clear();
+    pattern_cache.clear();
+    opmat_cache.clear();
+    identity_patterns.clear();
+    ones_cache.clear();
+    grad.reset();
+    ngrad.reset();
+    div_interior.reset();
+    div_full.reset();
+    face_cells.reset();
+    face_areas.reset();
+    face_centroids.reset();
+    cell_volumes.reset();
+    cell_centroids.reset();
+    red_partials.reset();
+    red_counter.reset();
+    for (auto& m : marks) cudaEventDestroy(m.ev);
+    if (stream) {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
+    if (pinned) cudaFreeHost(pinned);
+}
+
+Buf Core::alloc(size_t bytes)
+{
+    if (bytes == 0) bytes = 16;
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, bytes, stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(e == cudaErrorMemoryAllocation ? EQG_ERR_MEMORY : EQG_ERR_DEVICE,
+             std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+    }
+    bytes_in_use += (int64_t)bytes;
+    if (bytes_in_use > bytes_peak) bytes_peak = bytes_in_use;
+    auto b = std::make_shared<DevBuf>();
+    b->core = this;
+    b->ptr = p;
+    b->bytes = bytes;
+    return b;
+}
+
+void Core::free(void* p, size_t bytes)
+{
+    cudaFreeAsync(p, stream);
+    bytes_in_use -= (int64_t)bytes;
+}
+
+void Core::sync() { EQG_CUDA(cudaStreamSynchronize(stream)); }
+
+void Core::checkLaunch(const char* what)
+{
+    launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) fail(EQG_ERR_DEVICE, std::string("kernel ") + what + " failed to launch: " + cudaGetErrorString(e));
+}
+
+double Core::param_d(const std::string& k, double d) const
+{
+    auto it = params.find(k);
+    return it == params.end() ? d : std::stod(it->second);
+}
+
+int Core::param_i(const std::string& k, int d) const
+{
+    auto it = params.find(k);
+    if (it == params.end()) return d;
+    if (it->second == "true" || it->second == "yes") return 1;
+    if (it->second == "false" || it->second == "no") return 0;
+    return (int)std::stol(it->second);
+}
+
+std::string Core::param_s(const std::string& k, const std::string& d) const
+{
+    auto it = params.find(k);
+    return it == params.end() ? d : it->second;
+}
+
+// ---------------------------------------------------------------------------
+// Grid construction kernels.
+// ---------------------------------------------------------------------------
+namespace {
+
+#define GRID_STRIDE(i, n) \
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+struct Dims {
+    int dim, nx, ny, nz;
+    double dx, dy, dz;
+    int fx, fy, fz, nf, nc;
+};
+
+__device__ __forceinline__ double node(int i, double h) { return __dmul_rn((double)i, h); }
+__device__ __forceinline__ double width(int i, double h) { return __dsub_rn(node(i + 1, h), node(i, h)); }
+__device__ __forceinline__ double mid(int i, double h) { return __dmul_rn(0.5, __dadd_rn(node(i, h), node(i + 1, h))); }
+__device__ __forceinline__ int cell_of(const Dims& d, int i, int j, int k) { return i + d.nx * (j + d.ny * k); }
+
+__global__ void faces_kernel(Dims d, int32_t* face_cells, double* areas, double* centroids, uint8_t* interior)
+{
+    GRID_STRIDE(f, d.nf)
+    {
+        int axis, i, j, k;
+        if (f < d.fx) {
+            axis = 0;
+            i = (int)(f % (d.nx + 1));
+            const int r = (int)(f / (d.nx + 1));
+            j = r % d.ny;
+            k = r / d.ny;
+        } else if (f < d.fx + d.fy) {
+            axis = 1;
+            const int g = (int)(f - d.fx);
+            i = g % d.nx;
+            const int r = g / d.nx;
+            j = r % (d.ny + 1);
+            k = r / (d.ny + 1);
+        } else {
+            axis = 2;
+            const int h = (int)(f - d.fx - d.fy);
+            i = h % d.nx;
+            const int r = h / d.nx;
+            j = r % d.ny;
+            k = r / d.ny;
+        }
+        int c0, c1;
+        double area, cx, cy, cz;
+        if (axis == 0) {
+            c0 = i > 0 ? cell_of(d, i - 1, j, k) : -1;
+            c1 = i < d.nx ? cell_of(d, i, j, k) : -1;
+            area = d.dim == 3 ? __dmul_rn(width(j, d.dy), width(k, d.dz)) : width(j, d.dy);
+            cx = node(i, d.dx);
+            cy = mid(j, d.dy);
+            cz = mid(k, d.dz);
+        } else if (axis == 1) {
+            c0 = j > 0 ? cell_of(d, i, j - 1, k) : -1;
+            c1 = j < d.ny ? cell_of(d, i, j, k) : -1;
+            area = d.dim == 3 ? __dmul_rn(width(i, d.dx), width(k, d.dz)) : width(i, d.dx);
+            cx = mid(i, d.dx);
+            cy = node(j, d.dy);
+            cz = mid(k, d.dz);
+        } else {
+            c0 = k > 0 ? cell_of(d, i, j, k - 1) : -1;
+            c1 = k < d.nz ? cell_of(d, i, j, k) : -1;
+            area = __dmul_rn(width(i, d.dx), width(j, d.dy));
+            cx = mid(i, d.dx);
+            cy = mid(j, d.dy);
+            cz = node(k, d.dz);
+        }
+        face_cells[2 * f] = c0;
+        face_cells[2 * f + 1] = c1;
+        areas[f] = area;
+        centroids[f] = cx;
+        centroids[(int64_t)d.nf + f] = cy;
+        if (d.dim == 3) centroids[2 * (int64_t)d.nf + f] = cz;
+        interior[f] = (c0 >= 0 && c1 >= 0) ? 1 : 0;
+    }
+}
+
+__global__ void cells_kernel(Dims d, double* volumes, double* centroids, uint8_t* boundary)
+{
+    GRID_STRIDE(c, d.nc)
+    {
+        const int i = (int)(c % d.nx);
+        const int r = (int)(c / d.nx);
+        const int j = r % d.ny;
+        const int k = r / d.ny;
+        double vol = __dmul_rn(width(i, d.dx), width(j, d.dy));
+        if (d.dim == 3) vol = __dmul_rn(vol, width(k, d.dz));
+        volumes[c] = vol;
+        centroids[c] = mid(i, d.dx);
+        centroids[(int64_t)d.nc + c] = mid(j, d.dy);
+        if (d.dim == 3) centroids[2 * (int64_t)d.nc + c] = mid(k, d.dz);
+        bool b = i == 0 || i == d.nx - 1 || j == 0 || j == d.ny - 1;
+        if (d.dim == 3) b = b || k == 0 || k == d.nz - 1;
+        boundary[c] = b ? 1 : 0;
+    }
+}
+
+// The 2*dim faces of a cell in ascending face order, with the sign of the
+// cell in fullngrad^T: +1 where the cell is the face's first cell.
+__device__ __forceinline__ void cell_faces(const Dims& d, int64_t c, int32_t* faces, double* sign)
+{
+    const int i = (int)(c % d.nx);
+    const int r = (int)(c / d.nx);
+    const int j = r % d.ny;
+    const int k = r / d.ny;
+    faces[0] = i + (d.nx + 1) * (j + d.ny * k);
+    faces[1] = faces[0] + 1;
+    faces[2] = d.fx + i + d.nx * (j + (d.ny + 1) * k);
+    faces[3] = faces[2] + d.nx;
+    sign[0] = -1.0;
+    sign[1] = 1.0;
+    sign[2] = -1.0;
+    sign[3] = 1.0;
+    if (d.dim == 3) {
+        faces[4] = d.fx + d.fy + i + d.nx * (j + d.ny * k);
+        faces[5] = faces[4] + d.nx * d.ny;
+        sign[4] = -1.0;
+        sign[5] = 1.0;
+    }
+}
+
+__global__ void div_full_kernel(Dims d, int32_t* ptr, int32_t* src, double* w)
+{
+    const int nfc = 2 * d.dim;
+    GRID_STRIDE(c, d.nc)
+    {
+        int32_t faces[6];
+        double sign[6];
+        cell_faces(d, c, faces, sign);
+        for (int t = 0; t < nfc; ++t) {
+            src[c * nfc + t] = faces[t];
+            w[c * nfc + t] = sign[t];
+        }
+        ptr[c] = (int32_t)(c * nfc);
+        if (c == d.nc - 1) ptr[d.nc] = (int32_t)(d.nc * nfc);
+    }
+}
+
+template <bool FILL>
+__global__ void div_interior_kernel(Dims d, const int32_t* ipos, int64_t* cnt, const int32_t* ptr, int32_t* src,
+                                    double* w)
+{
+    const int nfc = 2 * d.dim;
+    GRID_STRIDE(c, d.nc)
+    {
+        int32_t faces[6];
+        double sign[6];
+        cell_faces(d, c, faces, sign);
+        int o = FILL ? ptr[c] : 0;
+        int64_t n = 0;
+        for (int t = 0; t < nfc; ++t) {
+            const int32_t p = ipos[faces[t]];
+            if (p < 0) continue;
+            if (FILL) {
+                src[o] = p;
+                w[o] = sign[t];
+                ++o;
+            } else {
+                ++n;
+            }
+        }
+        if (!FILL) cnt[c] = n;
+    }
+}
+
+__global__ void grad_kernel(int nif, const int32_t* ifaces, const int32_t* face_cells, double s0, int32_t* ptr,
+                            int32_t* src, double* w)
+{
+    GRID_STRIDE(i, nif)
+    {
+        const int32_t f = ifaces[i];
+        int32_t c0 = face_cells[2 * f], c1 = face_cells[2 * f + 1];
+        double w0 = s0, w1 = -s0;
+        if (c1 < c0) {
+            const int32_t t = c0;
+            c0 = c1;
+            c1 = t;
+            const double u = w0;
+            w0 = w1;
+            w1 = u;
+        }
+        ptr[i] = (int32_t)(2 * i);
+        src[2 * i] = c0;
+        src[2 * i + 1] = c1;
+        w[2 * i] = w0;
+        w[2 * i + 1] = w1;
+        if (i == nif - 1) ptr[nif] = 2 * nif;
+    }
+}
+
+__global__ void iota_kernel(int32_t* out, int64_t n)
+{
+    GRID_STRIDE(i, n) out[i] = (int32_t)i;
+}
+
+__global__ void scatter_pos_kernel(const int32_t* list, int64_t n, int32_t* pos)
+{
+    GRID_STRIDE(i, n) pos[list[i]] = (int32_t)i;
+}
+
+__global__ void negate_u8_kernel(const uint8_t* a, uint8_t* out, int64_t n)
+{
+    GRID_STRIDE(i, n) out[i] = !a[i];
+}
+
+}  // namespace
+
+// Indices i in [0, n) with flags[i] != 0, ascending.
+Buf compact_indices(Core& c, const uint8_t* flags, int64_t n, int64_t& count)
+{
+    Buf out = c.allocN<int32_t>(n > 0 ? n : 1);
+    Buf num = c.allocN<int64_t>(1);
+    cub::CountingInputIterator<int32_t> it(0);
+    size_t tmp_bytes = 0;
+    EQG_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp_bytes, it, flags, out->as<int32_t>(), num->as<int64_t>(), n,
+                                        c.stream));
+    Buf tmp = c.alloc(tmp_bytes);
+    EQG_CUDA(cub::DeviceSelect::Flagged(tmp->ptr, tmp_bytes, it, flags, out->as<int32_t>(), num->as<int64_t>(), n,
+                                        c.stream));
+    c.launches++;
+    EQG_CUDA(cudaMemcpyAsync(c.pinned, num->ptr, sizeof(int64_t), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    std::memcpy(&count, c.pinned, sizeof(int64_t));
+    return out;
+}
+
+void build_grid(Core& c, eqg_set** builtin)
+{
+    if (c.dim != 2 && c.dim != 3) fail(EQG_ERR_ARG, "Cannot handle " + std::to_string(c.dim) + " dimensions.");
+    if (c.nx < 1 || c.ny < 1 || c.nz < 1) fail(EQG_ERR_ARG, "grid dimensions must be positive");
+    if (c.dim == 2) {
+        c.nz = 1;
+        c.dz = 1.0;
+    }
+    Dims d;
+    d.dim = c.dim;
+    d.nx = c.nx;
+    d.ny = c.ny;
+    d.nz = c.nz;
+    d.dx = c.dx;
+    d.dy = c.dy;
+    d.dz = c.dz;
+    const int64_t fx = (int64_t)(c.nx + 1) * c.ny * c.nz;
+    const int64_t fy = (int64_t)c.nx * (c.ny + 1) * c.nz;
+    const int64_t fz = c.dim == 3 ? (int64_t)c.nx * c.ny * (c.nz + 1) : 0;
+    const int64_t nc64 = (int64_t)c.nx * c.ny * c.nz;
+    const int64_t nf64 = fx + fy + fz;
+    if (nf64 * 2 > (int64_t)INT32_MAX || nc64 * 6 > (int64_t)INT32_MAX)
+        fail(EQG_ERR_UNSUPPORTED, "grid too large for 32-bit indices");
+    d.fx = (int)fx;
+    d.fy = (int)fy;
+    d.fz = (int)fz;
+    d.nf = (int)nf64;
+    d.nc = (int)nc64;
+    c.nc = d.nc;
+    c.nf = d.nf;
+
+    c.face_cells = c.allocN<int32_t>(2 * nf64);
+    c.face_areas = c.allocN<double>(nf64);
+    c.face_centroids = c.allocN<double>(c.dim * nf64);
+    Buf face_interior = c.allocN<uint8_t>(nf64);
+    faces_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(d, c.face_cells->as<int32_t>(), c.face_areas->as<double>(),
+                                                             c.face_centroids->as<double>(),
+                                                             face_interior->as<uint8_t>());
+    c.checkLaunch("grid_faces");
+    c.cell_volumes = c.allocN<double>(nc64);
+    c.cell_centroids = c.allocN<double>(c.dim * nc64);
+    Buf cell_boundary = c.allocN<uint8_t>(nc64);
+    cells_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, c.cell_volumes->as<double>(),
+                                                             c.cell_centroids->as<double>(),
+                                                             cell_boundary->as<uint8_t>());
+    c.checkLaunch("grid_cells");
+
+    // index sets
+    auto make = [&](int entity, Buf idx, int64_t n, bool identity) {
+        auto* s = new eqg_set;
+        s->entity = entity;
+        s->n = n;
+        s->idx = idx;
+        s->identity = identity;
+        s->sorted = 1;
+        return s;
+    };
+    Buf all_c = c.allocN<int32_t>(nc64), all_f = c.allocN<int32_t>(nf64);
+    iota_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(all_c->as<int32_t>(), nc64);
+    c.checkLaunch("iota");
+    iota_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(all_f->as<int32_t>(), nf64);
+    c.checkLaunch("iota");
+    int64_t n_bc = 0, n_ic = 0, n_bf = 0, n_if = 0;
+    Buf bc = compact_indices(c, cell_boundary->as<uint8_t>(), nc64, n_bc);
+    Buf not_b = c.allocN<uint8_t>(nc64 > nf64 ? nc64 : nf64);
+    negate_u8_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(cell_boundary->as<uint8_t>(), not_b->as<uint8_t>(),
+                                                                 nc64);
+    c.checkLaunch("negate");
+    Buf ic = compact_indices(c, not_b->as<uint8_t>(), nc64, n_ic);
+    Buf iff = compact_indices(c, face_interior->as<uint8_t>(), nf64, n_if);
+    negate_u8_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(face_interior->as<uint8_t>(), not_b->as<uint8_t>(),
+                                                                 nf64);
+    c.checkLaunch("negate");
+    Buf bf = compact_indices(c, not_b->as<uint8_t>(), nf64, n_bf);
+    c.nif = (int)n_if;
+    builtin[EQG_ALL_CELLS] = make(EQG_CELLS, all_c, nc64, true);
+    builtin[EQG_BOUNDARY_CELLS] = make(EQG_CELLS, bc, n_bc, false);
+    builtin[EQG_INTERIOR_CELLS] = make(EQG_CELLS, ic, n_ic, false);
+    builtin[EQG_ALL_FACES] = make(EQG_FACES, all_f, nf64, true);
+    builtin[EQG_BOUNDARY_FACES] = make(EQG_FACES, bf, n_bf, false);
+    builtin[EQG_INTERIOR_FACES] = make(EQG_FACES, iff, n_if, false);
+
+    // helper operators
+    auto opm = [&](int n_out, int n_src, int max_row, int64_t nnz) {
+        auto m = std::make_shared<OpMatrix>();
+        m->id = c.newId();
+        m->n_out = n_out;
+        m->n_src = n_src;
+        m->max_row = max_row;
+        m->ptr = c.allocN<int32_t>((size_t)n_out + 1);
+        m->src = c.allocN<int32_t>(nnz > 0 ? nnz : 1);
+        m->w = c.allocN<double>(nnz > 0 ? nnz : 1);
+        return m;
+    };
+    c.grad = opm(c.nif, c.nc, 2, 2 * n_if);
+    c.ngrad = opm(c.nif, c.nc, 2, 2 * n_if);
+    if (c.nif > 0) {
+        grad_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(c.nif, iff->as<int32_t>(), c.face_cells->as<int32_t>(),
+                                                                -1.0, c.grad->ptr->as<int32_t>(),
+                                                                c.grad->src->as<int32_t>(), c.grad->w->as<double>());
+        c.checkLaunch("grad_op");
+        grad_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(c.nif, iff->as<int32_t>(), c.face_cells->as<int32_t>(),
+                                                                1.0, c.ngrad->ptr->as<int32_t>(),
+                                                                c.ngrad->src->as<int32_t>(), c.ngrad->w->as<double>());
+        c.checkLaunch("ngrad_op");
+    } else {
+        k_fill_i32(c, c.grad->ptr->as<int32_t>(), 0, 1);
+        k_fill_i32(c, c.ngrad->ptr->as<int32_t>(), 0, 1);
+    }
+    c.div_full = opm(c.nc, c.nf, 2 * c.dim, (int64_t)2 * c.dim * nc64);
+    div_full_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, c.div_full->ptr->as<int32_t>(),
+                                                                c.div_full->src->as<int32_t>(),
+                                                                c.div_full->w->as<double>());
+    c.checkLaunch("div_full_op");
+
+    Buf ipos = c.allocN<int32_t>(nf64);
+    k_fill_i32(c, ipos->as<int32_t>(), -1, nf64);
+    if (n_if > 0) {
+        scatter_pos_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(iff->as<int32_t>(), n_if, ipos->as<int32_t>());
+        c.checkLaunch("interior_pos");
+    }
+    {
+        auto m = std::make_shared<OpMatrix>();
+        m->id = c.newId();
+        m->n_out = c.nc;
+        m->n_src = c.nif;
+        m->max_row = 2 * c.dim;
+        Buf cnt = c.allocN<int64_t>(nc64);
+        div_interior_kernel<false><<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, ipos->as<int32_t>(),
+                                                                               cnt->as<int64_t>(), nullptr, nullptr,
+                                                                               nullptr);
+        c.checkLaunch("div_interior_count");
+        const int64_t nnz = counts_to_rowptr(c, cnt, c.nc, m->ptr);
+        m->src = c.allocN<int32_t>(nnz > 0 ? nnz : 1);
+        m->w = c.allocN<double>(nnz > 0 ? nnz : 1);
+        div_interior_kernel<true><<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, ipos->as<int32_t>(), nullptr,
+                                                                              m->ptr->as<int32_t>(),
+                                                                              m->src->as<int32_t>(),
+                                                                              m->w->as<double>());
+        c.checkLaunch("div_interior_fill");
+        c.div_interior = m;
+    }
+    c.sync();
+}
+
+}  // namespace eqg

@@ -1,0 +1,273 @@
+// Internal types of the device runtime behind include/eqg.h.
+//
+// Data layout in HBM (one runtime = one grid = one CUDA stream):
+//   - every collection value array is a dense double[n];
+//   - a Jacobian is a CSR pattern (int32 rowptr[n+1], int32 colind[nnz],
+//     ascending columns) shared through the pattern cache, plus a double[nnz]
+//     value array owned by the collection;
+//   - entity sets are int32[n] (-1 = outside), masks uint8[n];
+//   - the grid's helper operators (gradient, divergence, On/Extend
+//     selections) are small-row CSR "operator matrices" with double weights.
+// All buffers are immutable once written, so handles share them freely.
+#pragma once
+
+#include "eqg.h"
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+namespace eqg {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] inline void fail(int code, const std::string& msg) { throw Error(code, msg); }
+
+#define EQG_CUDA(call)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            ::eqg::fail(EQG_ERR_DEVICE, std::string(#call " failed: ") + cudaGetErrorString(e_));    \
+    } while (0)
+
+struct Core;
+
+// Device allocation from the runtime's stream-ordered pool.
+struct DevBuf {
+    Core* core = nullptr;
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    ~DevBuf();
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr); }
+};
+using Buf = std::shared_ptr<DevBuf>;
+
+// CSR sparsity pattern on the device.
+struct SolverAnalysis;
+struct Pattern {
+    uint64_t id = 0;
+    int rows = 0, cols = 0;
+    int64_t nnz = 0;
+    int max_row = 0;            // longest row
+    Buf rowptr;                 // int32[rows+1]
+    Buf colind;                 // int32[nnz]
+    Buf rowidx;                 // int32[nnz], built on demand (row of each entry)
+    std::shared_ptr<SolverAnalysis> analysis;  // linear-solver analysis, built on demand
+};
+using PatternP = std::shared_ptr<Pattern>;
+
+// A small-row operator matrix M (n_out x n_src): out = M x and out_J = M J.
+struct OpMatrix {
+    uint64_t id = 0;
+    int n_out = 0, n_src = 0;
+    int max_row = 0;
+    Buf ptr;   // int32[n_out+1]
+    Buf src;   // int32[nnz], ascending within a row
+    Buf w;     // double[nnz]
+};
+using OpMatrixP = std::shared_ptr<OpMatrix>;
+
+struct SolverStats {
+    int64_t linear_solves = 0, krylov_iterations = 0, refinement_sweeps = 0;
+    double last_residual = 0.0;
+};
+
+struct Mark {
+    cudaEvent_t ev;
+};
+
+// Runtime state shared by every handle (a handle keeps the core alive).
+struct Core {
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    cudaMemPool_t pool = nullptr;
+    std::map<std::string, std::string> params;
+
+    // grid
+    int dim = 2, nx = 6, ny = 1, nz = 1;
+    double dx = 1, dy = 1, dz = 1;
+    int nc = 0, nf = 0, nif = 0;
+    Buf face_cells;      // int32[2*nf]
+    Buf face_areas;      // double[nf]
+    Buf face_centroids;  // double[dim*nf] (component-major: d*nf + f)
+    Buf cell_volumes;    // double[nc]
+    Buf cell_centroids;  // double[dim*nc] (component-major)
+    OpMatrixP grad, ngrad, div_interior, div_full;
+
+    // settings
+    int verbose = 0, max_iter = 10;
+    double abs_res_tol = 1e-6;
+
+    // accounting
+    std::atomic<int64_t> launches{0};
+    int64_t bytes_in_use = 0, bytes_peak = 0;
+    int64_t patterns_built = 0, pattern_hits = 0;
+    int64_t newton_solves = 0, newton_iterations = 0;
+    SolverStats solver;
+
+    // caches
+    uint64_t next_id = 1;
+    std::map<std::tuple<int, uint64_t, uint64_t, int64_t>, PatternP> pattern_cache;
+    std::map<std::tuple<int, uint64_t, uint64_t, int64_t>, OpMatrixP> opmat_cache;
+    std::map<int64_t, PatternP> identity_patterns;
+    std::map<int64_t, Buf> ones_cache;
+    std::map<std::tuple<int, uint64_t>, struct eqg_set*> derived_sets;  // owned references
+
+    // scratch for reductions
+    Buf red_partials;   // double[kRedBlocks * 4]
+    Buf red_counter;    // unsigned int
+    double* pinned = nullptr;  // small pinned host buffer
+    std::vector<Mark> marks;
+    std::vector<std::pair<int, int>> solve_marks;
+
+    Core();
+    ~Core();
+
+    uint64_t newId() { return next_id++; }
+    Buf alloc(size_t bytes);
+    template <class T>
+    Buf allocN(size_t n) { return alloc(n * sizeof(T)); }
+    void free(void* p, size_t bytes);
+    void sync();
+    void checkLaunch(const char* what);
+    double param_d(const std::string& k, double d) const;
+    int param_i(const std::string& k, int d) const;
+    std::string param_s(const std::string& k, const std::string& d) const;
+};
+
+using CoreP = std::shared_ptr<Core>;
+
+constexpr int kThreads = 256;
+constexpr int kRedBlocks = 592;  // 4 x 148 SMs
+
+inline int blocksFor(int64_t n, int threads = kThreads, int cap = 148 * 32)
+{
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return (int)b;
+}
+
+// ---- kernels exposed to the C-ABI layer (ops.cu, jacobian.cu, solver.cu) ----
+enum EwOp { EW_ADD = 0, EW_SUB, EW_MUL, EW_DIV };
+
+void k_fill(Core& c, double* out, double v, int64_t n);
+void k_fill_i32(Core& c, int32_t* out, int32_t v, int64_t n);
+void k_binary(Core& c, int op, const double* a, const double* b, double* out, int64_t n);
+void k_binary_scalar(Core& c, int op, const double* a, double s, int scalar_left, double* out, int64_t n);
+void k_unary_value(Core& c, int op, const double* a, double* out, int64_t n);
+void k_compare(Core& c, int op, const double* a, const double* b, uint8_t* out, int64_t n);
+void k_compare_scalar(Core& c, int op, const double* a, double s, int scalar_left, uint8_t* out, int64_t n);
+void k_select_value(Core& c, const uint8_t* m, const double* a, const double* b, double* out, int64_t n);
+void k_mask_logic(Core& c, int op, const uint8_t* a, const uint8_t* b, uint8_t* out, int64_t n);
+void k_set_select(Core& c, const uint8_t* m, const int32_t* a, const int32_t* b, int32_t* out, int64_t n);
+void k_is_empty(Core& c, const int32_t* s, uint8_t* out, int64_t n);
+void k_face_neighbour(Core& c, const int32_t* faces, int side, int32_t* out, int64_t n, int32_t* err);
+void k_gather_i32(Core& c, const int32_t* data, const int32_t* map, int32_t* out, int64_t n, int32_t fill);
+void k_gather_f64(Core& c, const double* data, const int32_t* idx, int stride, int comp, double* out, int64_t n,
+                  int32_t* err);
+void k_normal(Core& c, const int32_t* faces, double* out, int comp, int64_t n, int32_t* err);
+void k_locate(Core& c, const int32_t* sorted, int64_t n_sorted, const int32_t* keys, int32_t* pos, int64_t n_keys,
+              int identity_n, int32_t* err);
+void k_scatter_inverse(Core& c, const int32_t* pos, int64_t n, int32_t* inv, int32_t* err);
+void k_is_strictly_sorted(Core& c, const int32_t* a, int64_t n, int32_t* flag);
+double k_reduce(Core& c, int op, const double* a, int64_t n);
+double k_two_norm(Core& c, const double* a, int64_t n);
+
+// Operator matrices and Jacobians (jacobian.cu)
+OpMatrixP opmat_from_map(Core& c, const int32_t* map_dev, int n_out, int n_src, bool allow_missing);
+OpMatrixP opmat_from_host(Core& c, int n_out, int n_src, const std::vector<int32_t>& ptr,
+                          const std::vector<int32_t>& src, const std::vector<double>& w);
+void opmat_apply_values(Core& c, const OpMatrix& m, const double* x, double* y);
+PatternP pattern_identity(Core& c, int n);
+Buf ones(Core& c, int64_t n);
+PatternP pattern_spgemm(Core& c, const OpMatrix& m, const PatternP& j);
+void spgemm_values(Core& c, const OpMatrix& m, const Pattern& jp, const double* jv, const Pattern& op,
+                   double* ov);
+PatternP pattern_union(Core& c, const PatternP& a, const PatternP& b);
+// Elementwise Jacobian rule: out_row(i) = post_i * (wa_i * A_row(i) (+) wb_i * B_row(i)).
+// Weights come from the operand values per op (see jacobian.cu).
+enum JacRule {
+    JR_ADD = 0, JR_SUB, JR_MUL, JR_DIV,  // two operands, either may be absent
+    JR_SCALE_CONST,                        // out = s * A
+    JR_DIV_BY_CONST,                       // (1/(s*s)) * (s * A)
+    JR_SQRT,                               // (0.5/sqrt(x)) * A
+    JR_SIGN,                               // sign(x) * A
+    JR_NEG,                                // -A
+    JR_SELECT                              // m*A (+) (1-m)*B
+};
+struct JacArgs {
+    int rule = JR_ADD;
+    const double* va = nullptr;   // value of operand a
+    const double* vb = nullptr;   // value of operand b
+    const double* vout = nullptr; // value of the result (sqrt uses it)
+    const uint8_t* mask = nullptr;
+    double s = 0.0;
+    const Pattern* pa = nullptr;
+    const double* ja = nullptr;
+    const Pattern* pb = nullptr;
+    const double* jb = nullptr;
+};
+void jacobian_elementwise(Core& c, const JacArgs& args, const Pattern& out, double* jout);
+void pattern_build_rowidx(Core& c, Pattern& p);
+// Inclusive scan of int64 per-row counts into an int32 rowptr; returns nnz.
+int64_t counts_to_rowptr(Core& c, Buf& counts, int rows, Buf& rowptr);
+// Ascending indices i in [0, n) with flags[i] != 0.
+Buf compact_indices(Core& c, const uint8_t* flags, int64_t n, int64_t& count);
+
+// Linear solver (solver.cu)
+struct SolveResult {
+    bool converged = false;
+    int iterations = 0;
+    int sweeps = 0;
+    double rel_residual = 0.0;
+};
+SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const double* rhs, double* x);
+
+}  // namespace eqg
+
+// ---- handle structs (global namespace, named in eqg.h) -------------------
+struct eqg_set {
+    std::atomic<int> refs{1};
+    eqg::CoreP core;
+    uint64_t id = 0;
+    int entity = EQG_CELLS;
+    int64_t n = 0;
+    eqg::Buf idx;          // int32[n]
+    bool identity = false; // idx[i] == i for all i (all cells / all faces)
+    int sorted = -1;       // strictly ascending: -1 unknown, 0 no, 1 yes
+};
+
+struct eqg_mask {
+    std::atomic<int> refs{1};
+    eqg::CoreP core;
+    int64_t n = 0;
+    eqg::Buf v;  // uint8[n]
+};
+
+struct eqg_coll {
+    std::atomic<int> refs{1};
+    eqg::CoreP core;
+    int64_t n = 0;
+    eqg::Buf val;           // double[n]
+    eqg::PatternP pat;      // null: no Jacobian
+    eqg::Buf jval;          // double[nnz]
+};
+
+struct eqg_runtime {
+    eqg::CoreP core;
+    eqg_set* builtin[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+};

@@ -417,6 +417,14 @@ class Runtime:
         u = self.newtonSolve(combined, u0)
         return tuple(sub(u, i) for i in range(len(num)))
 
+    def spanSubset(self, u, start, num):
+        """Opm::subset(u, ESpan(num, 1, start))."""
+        return self._coll(self.lib.eqg_span_subset, u.h, int(start), int(num))
+
+    def spanSuperset(self, u, start, total):
+        """Opm::superset(u, ESpan(len(u), 1, start), total)."""
+        return self._coll(self.lib.eqg_span_superset, u.h, int(start), int(total))
+
     def solveForUpdate(self, residual):
         return self._coll(self.lib.eqg_solve_for_update, residual.h)
 

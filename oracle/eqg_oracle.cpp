@@ -24,8 +24,9 @@
  *   - Every EquelleRuntimeCPU method (EquelleRuntimeCPU.cpp,
  *     EquelleRuntimeCPU_impl.hpp) including newtonSolve.
  *   - The linear solver: BiCGStab (van der Vorst 1992) right-preconditioned
- *     with ILU(0) in natural order (Saad, Iterative Methods, Alg. 10.4);
- *     the reference delegates to Opm::LinearSolverFactory (not vendored).
+ *     with ILU(0) in natural order (Saad, Iterative Methods, Alg. 10.4),
+ *     with a fixed pseudo-random shadow residual (shadow_entry); the
+ *     reference delegates to Opm::LinearSolverFactory (not vendored).
  *
  * Parity status: grid topology, index sets, geometry and the On/Extend,
  * trinaryIf, Gradient and Divergence values are pinned by the reference's
@@ -564,6 +565,20 @@ double dot(const std::vector<double>& a, const std::vector<double>& b)
     return s;
 }
 
+// Shadow residual of BiCGStab: a fixed, dense pseudo-random vector in
+// [-1, 1) from a 32-bit integer hash of the row index.  The textbook choice
+// rhat = r0 breaks down when r0 is nearly a unit vector, which is the case
+// at the first Newton iteration of well-driven flow (the residual is nonzero
+// only in the well cells).
+double shadow_entry(int64_t i)
+{
+    uint32_t x = (uint32_t)((uint64_t)i * 0x9E3779B1ull);
+    x ^= x >> 16;
+    x *= 0x85EBCA6Bu;
+    x ^= x >> 13;
+    return 2.0 * ((double)x / 4294967296.0) - 1.0;
+}
+
 struct SolveReport {
     bool converged = false;
     int iterations = 0;
@@ -584,7 +599,8 @@ SolveReport bicgstab_ilu0(const Csr& a, const std::vector<double>& b, std::vecto
     }
     Ilu0 prec;
     if (!ilu0_factor(a, prec)) return rep;
-    std::vector<double> r = b, rhat = b, p(n, 0.0), v(n, 0.0), s(n), t(n), ph(n), sh(n);
+    std::vector<double> r = b, rhat(n), p(n, 0.0), v(n, 0.0), s(n), t(n), ph(n), sh(n);
+    for (int64_t i = 0; i < n; ++i) rhat[i] = shadow_entry(i);
     double rho = 1.0, alpha = 1.0, omega = 1.0;
     for (int it = 1; it <= max_iter; ++it) {
         const double rho_new = dot(rhat, r);

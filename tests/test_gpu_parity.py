@@ -1,0 +1,90 @@
+"""Device library vs CPU oracle, through the C ABI (needs a GPU)."""
+import numpy as np
+import pytest
+
+import kat
+import opstream
+from equelle_b200 import programs
+from equelle_b200.runtime import Runtime
+from parity import assert_colls, assert_values
+
+pytestmark = pytest.mark.gpu
+
+
+def test_gpu_grid_4x3_golden(gpu_lib):
+    kat.check_grid_4x3(gpu_lib)
+
+
+def test_gpu_vals_on_grid_golden(gpu_lib):
+    kat.check_vals_on_grid(gpu_lib)
+
+
+@pytest.mark.parametrize("grid", opstream.GRIDS, ids=["2d", "3d"])
+def test_op_stream_parity(gpu_lib, oracle_lib, grid):
+    g = Runtime(gpu_lib, grid)
+    o = Runtime(oracle_lib, grid)
+    og = opstream.op_stream(g)
+    oo = opstream.op_stream(o)
+    for k in oo:
+        assert_colls(og[k], oo[k], k)
+    # a second pass reuses every cached pattern and must give the same numbers
+    og2 = opstream.op_stream(g)
+    for k in oo:
+        assert_colls(og2[k], oo[k], k + " (cached)")
+    assert g.stats()["pattern_cache_hits"] > 0
+
+
+@pytest.mark.parametrize("grid", opstream.GRIDS, ids=["2d", "3d"])
+def test_reductions_and_masks(gpu_lib, oracle_lib, grid):
+    g = Runtime(gpu_lib, grid)
+    o = Runtime(oracle_lib, grid)
+    rg, ro = opstream.reductions(g), opstream.reductions(o)
+    for k in ro:
+        assert_values([rg[k]], [ro[k]], k)
+    mg, mo = opstream.masks(g), opstream.masks(o)
+    for k in mo:
+        assert np.array_equal(mg[k], mo[k]), k
+
+
+@pytest.mark.parametrize("grid", opstream.GRIDS, ids=["2d", "3d"])
+def test_topology_parity(gpu_lib, oracle_lib, grid):
+    g = Runtime(gpu_lib, grid)
+    o = Runtime(oracle_lib, grid)
+    for name in ("allCells", "boundaryCells", "interiorCells", "allFaces", "boundaryFaces", "interiorFaces"):
+        assert np.array_equal(getattr(g, name)().indices(), getattr(o, name)().indices()), name
+    for side in ("firstCell", "secondCell"):
+        assert np.array_equal(getattr(g, side)(g.allFaces()).indices(), getattr(o, side)(o.allFaces()).indices())
+    for s in ("allCells", "allFaces", "boundaryFaces"):
+        for d in range(grid["grid_dim"]):
+            assert np.array_equal(g.centroid(getattr(g, s)())[d].value(), o.centroid(getattr(o, s)())[d].value())
+        assert np.array_equal(g.norm(getattr(g, s)()).value(), o.norm(getattr(o, s)()).value())
+    for d in range(grid["grid_dim"]):
+        assert np.array_equal(g.normal(g.allFaces())[d].value(), o.normal(o.allFaces())[d].value())
+
+
+@pytest.mark.parametrize("ordering", ["multicolor", "natural"])
+def test_heat_64x64_parity(gpu_lib, oracle_lib, ordering):
+    """Implicit heat equation, 64x64, 20 steps: fields within 1e-9 relative."""
+    grid, case = programs.heat_case(64, 64, steps=20)
+    params = dict(grid, abs_res_tol=1e-10, linsolver_residual_tolerance=1e-12)
+    og = programs.heat_equation(Runtime(gpu_lib, dict(params, linsolver_ordering=ordering)), 0.3, 1.0, **case)
+    oo = programs.heat_equation(Runtime(oracle_lib, params), 0.3, 1.0, **case)
+    for step, (a, b) in enumerate(zip(og, oo)):
+        assert np.max(np.abs(a - b) / np.abs(b)) <= 1e-9, "step %d" % step
+
+
+@pytest.mark.parametrize("shape,precision", [((16, 16, None), "double"), ((16, 16, None), "mixed"),
+                                             ((8, 8, 4), "double"), ((8, 8, 4), "mixed")])
+def test_two_phase_parity(gpu_lib, oracle_lib, shape, precision):
+    """Fully implicit two-phase flow: saturation within 1e-8 relative of the
+    FP64 oracle after every step, in plain FP64 and in mixed precision."""
+    grid, case = programs.two_phase_case(*shape, steps=3)
+    params = dict(grid, abs_res_tol=1e-11, linsolver_residual_tolerance=1e-12, linsolver_max_iterations=5000)
+    eg = Runtime(gpu_lib, dict(params, linsolver_precision=precision))
+    og = programs.two_phase(eg, **case)
+    oo = programs.two_phase(Runtime(oracle_lib, params), **case)
+    for step, ((pg, sg), (po, so)) in enumerate(zip(og, oo)):
+        assert np.max(np.abs(sg - so) / np.abs(so)) <= 1e-8, "Sw step %d" % step
+        assert np.max(np.abs(pg - po)) <= 1e-8 * np.max(np.abs(po)), "p step %d" % step
+    if precision == "mixed":
+        assert eg.stats()["refinement_sweeps"] > 0
