@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Benchmark: implicit Newton time steps of a generated-style simulator.
+
+Default workload: the fully implicit oil-water case on a 128x128x64
+Cartesian grid (2 unknowns per cell, 2,097,152 unknowns), seeded
+log-normal permeability, 1-day steps; each "step" is one time step = one
+newtonSolveSystem with BiCGStab + ILU(0) inner solves, run through the
+generated-style C++ simulator equelle_b200/sims/twophase.cpp linked to
+libeqg.so and called in this process.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W]
+                    [--impl ours|reference] [--precision double|mixed]
+                    [--workload twophase3d|twophase2d|heat] [--nx --ny --nz]
+
+`value` (time steps/s) is timed on the device clock between the runtime's
+solve marks of steps W .. W+K-1 (inputs resident in HBM); `e2e` re-runs the
+whole program through its public entry point with host input files and
+host outputs every step, timed on the host clock.  --impl reference times
+the CPU oracle (the restated reference serial backend) on a bounded sample
+of the same workload on the host cores.  Under torchrun each rank runs an
+independent replica (no collective on the data path); rank 0 prints one
+JSON line with the max time over ranks.
+"""
+import argparse
+import csv
+import io
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SPMV_KERNEL = "bicg_spmv_omega"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["double", "mixed"], default="double")
+    ap.add_argument("--ordering", choices=["multicolor", "natural"], default="multicolor")
+    ap.add_argument("--workload", choices=["twophase3d", "twophase2d", "heat"], default="twophase3d")
+    ap.add_argument("--nx", type=int)
+    ap.add_argument("--ny", type=int)
+    ap.add_argument("--nz", type=int)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample-krylov", type=int, default=12,
+                    help="Krylov iterations in the CPU oracle sample")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def workload(a):
+    from equelle_b200 import cases
+    if a.workload == "twophase3d":
+        nx, ny, nz = a.nx or 128, a.ny or 128, a.nz or 64
+        name, key = "twophase", "twophase_%dx%dx%d" % (nx, ny, nz)
+        desc = "two-phase oil-water fully implicit %dx%dx%d, 2 unknowns/cell" % (nx, ny, nz)
+        cells = nx * ny * nz
+
+        def write(d, steps):
+            return cases.two_phase(d, nx, ny, nz, steps=steps)
+        tol = ["abs_res_tol=1e-8", "linsolver_residual_tolerance=1e-8", "linsolver_max_iterations=5000"]
+    elif a.workload == "twophase2d":
+        nx, ny = a.nx or 512, a.ny or 512
+        name, key = "twophase", "twophase_%dx%d" % (nx, ny)
+        desc = "two-phase oil-water fully implicit %dx%d, 2 unknowns/cell" % (nx, ny)
+        cells = nx * ny
+
+        def write(d, steps):
+            return cases.two_phase(d, nx, ny, None, steps=steps, corr_len=4.0)
+        tol = ["abs_res_tol=1e-8", "linsolver_residual_tolerance=1e-8", "linsolver_max_iterations=5000"]
+    else:
+        nx, ny = a.nx or 64, a.ny or 64
+        name, key = "heateq", "heat_%dx%d" % (nx, ny)
+        desc = "implicit heat equation %dx%d" % (nx, ny)
+        cells = nx * ny
+
+        def write(d, steps):
+            return cases.heat(d, nx, ny, steps=steps)
+        tol = []
+    return name, key, desc, cells, write, tol
+
+
+def input_dir(key, steps, rank):
+    d = os.path.join(tempfile.gettempdir(), "eqg_bench", "%s_s%d_r%d" % (key, steps, rank))
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def dir_bytes(d, exclude=("timesteps.txt",)):
+    """Bytes of numeric input the run uploads (8 B per value read)."""
+    n = 0
+    for f in os.listdir(d):
+        if f in exclude or not f.endswith(".txt"):
+            continue
+        with open(os.path.join(d, f)) as fh:
+            n += 8 * len(fh.read().split())
+    return n
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc:
+            self.proc.terminate()
+            out, _ = self.proc.communicate(timeout=10)
+            for r in csv.reader(io.StringIO(out)):
+                if len(r) >= 9:
+                    self.rows.append([x.strip() for x in r])
+        return False
+
+    def summary(self):
+        rows = getattr(self, "rows", [])
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"]}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        loaded = [s for s in sm if s > 0.5 * smax] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        power = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        return {"sm_mhz": loaded[len(loaded) // 2], "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(power) if power else None}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def timed_window(rep, w, k):
+    """Device ms from the start of solve w to the end of solve w+k-1."""
+    ms = sum(rep.gap_ms[i] for i in range(w, w + k - 1)) + rep.solve_ms[w + k - 1]
+    return ms
+
+
+# ---------------------------------------------------------------------------
+def cpu_sample(name, args, sample_krylov, per_step):
+    """Times the CPU oracle on a bounded sample of the same workload: the
+    first Newton iteration of time step 1 (residual + Jacobian assembly,
+    ILU(0) factorization, `sample_krylov` BiCGStab iterations), then scales
+    the measured phase times by the per-step counts `per_step` (residual
+    evaluations, factorizations, Krylov iterations).  Returns (steps/s,
+    description)."""
+    from equelle_b200 import simrun
+    path = os.path.join(ROOT, "oracle", "_build", "libsim_%s_oracle.so" % name)
+    sargs = [a for a in args if not a.startswith(("linsolver_max_iterations", "max_iter"))]
+    sargs += ["max_iter=1", "linsolver_max_iterations=%d" % sample_krylov]
+    t0 = time.perf_counter()
+    rep = simrun.run(name, sargs, path=path, allow_failure=True)
+    wall = time.perf_counter() - t0
+    st = rep.stats
+    t_res = st.residual_ms / max(st.residual_evaluations, 1)
+    t_fac = st.factor_ms / max(st.linear_solves, 1)
+    t_kry = st.krylov_ms / max(st.krylov_iterations, 1)
+    ms_step = per_step["residuals"] * t_res + per_step["solves"] * t_fac + per_step["krylov"] * t_kry
+    desc = ("oracle (serial C++ restatement of the reference backend), 1 thread: first Newton iteration of step 1 "
+            "on the full grid (%d residual evals %.0f ms each, ILU(0) %.0f ms, %d BiCGStab its %.1f ms each; "
+            "%.1f s wall), scaled to %.1f residuals, %.1f factorizations and %.0f Krylov its per step as counted "
+            "on the device run" % (st.residual_evaluations, t_res, t_fac, st.krylov_iterations, t_kry, wall,
+                                   per_step["residuals"], per_step["solves"], per_step["krylov"]))
+    return 1000.0 / ms_step, desc, ms_step
+
+
+# ---------------------------------------------------------------------------
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    name, key, desc, cells, write, tol = workload(a)
+    W, K = a.warmup, a.steps
+    metric = "Newton-steps/s"
+    unit = "steps/s"
+
+    if a.impl == "reference":
+        if rank != 0:
+            if dist:
+                dist.destroy_process_group()
+            return
+        d = input_dir(key, 1, rank)
+        args = write(d, 1) + tol + ["output_values=none"]
+        per = reference_counts(a)
+        times = []
+        descs = None
+        for _ in range(W + K):
+            v, descs, ms = cpu_sample(name, args, a.cpu_sample_krylov, per)
+            times.append(ms)
+        ms_step = sum(times[W:]) / K
+        val = 1000.0 / ms_step
+        line = {
+            "impl": "reference", "metric": metric, "value": val, "unit": unit, "n_gpus": a.gpus, "steps": K,
+            "warmup": W, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": config(a, desc, cells),
+            "cpu_baseline": {"value": val, "unit": unit, "cores": 1, "kind": "port", "sample": descs},
+            "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
+
+    # ---- our arm ----------------------------------------------------------
+    from equelle_b200 import simrun
+    import equelle_b200
+    equelle_b200.load_library()
+    d = input_dir(key, W + K, rank)
+    args = write(d, W + K) + tol + [
+        "output_values=none", "device=%d" % local_rank, "time_kernel=" + SPMV_KERNEL,
+        "linsolver_precision=" + a.precision, "linsolver_ordering=" + a.ordering]
+    if dist:
+        dist.barrier()
+    with ClockSampler(local_rank) as clk:
+        rep = simrun.run(name, args)
+    if rep.solves < W + K:
+        raise SystemExit("simulator ran %d solves, expected %d" % (rep.solves, W + K))
+    ms = timed_window(rep, W, K)
+    infos = window_counts(rep, W, K)
+    if dist:
+        import torch
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * K / (ms / 1000.0)
+    st = rep.stats
+    n_rows, nnz = st.last_matrix_rows, st.last_matrix_nnz
+
+    # roofline of the dominant kernel (BiCGStab SpMV t = A s fused with the
+    # (t,s), (t,t) dots): algorithmic bytes per launch
+    if a.precision == "double":
+        kbytes = 12 * nnz + 4 * (n_rows + 1) + 3 * 8 * n_rows
+    else:
+        kbytes = 8 * nnz + 4 * (n_rows + 1) + 3 * 4 * n_rows
+    launches = max(st.timed_kernel_launches, 1)
+    k_ms = st.timed_kernel_ms / launches
+    achieved = kbytes / (k_ms / 1000.0) / 1e9 if k_ms > 0 else 0.0
+    peak, peak_kind = peaks()
+    roofline = {"kernel": SPMV_KERNEL, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": kbytes, "launches": st.timed_kernel_launches,
+                "avg_launch_ms": k_ms}
+
+    per_step = {"residuals": infos["residuals"] / K, "solves": infos["solves"] / K, "krylov": infos["krylov"] / K}
+
+    line = {
+        "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if a.precision == "double" else "f64+f32",
+        "data": "synthetic (seeded Gaussian-random-field log-permeability, corner wells)",
+        "config": config(a, desc, cells),
+        "newton_iterations_per_step": infos["newton"] / K,
+        "krylov_iterations_per_step": infos["krylov"] / K,
+        "cell_updates_per_s": world * K * cells / (ms / 1000.0),
+        "gpu_launches": infos["launches"],
+        "phase_ms_total": {"residual": st.residual_ms, "factor": st.factor_ms, "krylov": st.krylov_ms},
+        "roofline": roofline,
+        "clocks": clk.summary(),
+    }
+
+    # end to end through the public entry point: host input files in, host
+    # outputs out every step, host wall clock
+    if not a.no_e2e:
+        d2 = input_dir(key, K, rank)
+        args2 = write(d2, K) + tol + ["output_values=none", "device=%d" % local_rank,
+                                      "linsolver_precision=" + a.precision, "linsolver_ordering=" + a.ordering]
+        t0 = time.perf_counter()
+        rep2 = simrun.run(name, args2)
+        wall = time.perf_counter() - t0
+        if dist:
+            import torch
+            t = torch.tensor([wall], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        nfields = 2 if name == "twophase" else 1
+        line["e2e"] = {"value": world * K / wall, "unit": unit,
+                       "h2d_bytes_per_step": dir_bytes(d2) / K,
+                       "d2h_bytes_per_step": nfields * 8 * cells * (K + 1) / K,
+                       "what": "whole program run (grid build, input files, %d steps, output copies) on the "
+                               "host clock" % K, "solves": rep2.solves}
+
+    if rank == 0 and world == 1 and not a.no_cpu:
+        val, sdesc, _ = cpu_sample(name, write(input_dir(key, 1, rank), 1) + tol + ["output_values=none"],
+                                   a.cpu_sample_krylov, per_step)
+        line["cpu_baseline"] = {"value": val, "unit": unit, "cores": 1, "kind": "port", "sample": sdesc}
+
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def config(a, desc, cells):
+    return {"workload": desc, "cells": cells, "precision": a.precision, "ordering": a.ordering,
+            "dt": "1 day" if a.workload != "heat" else "0.5", "solver": "Newton + BiCGStab/ILU(0)",
+            "l2": "working set larger than L2 (126 MB), no flush", "parallelism": "replicas"}
+
+
+def window_counts(rep, w, k):
+    """Counters summed over the timed solves w .. w+k-1."""
+    sel = [rep.info[i] for i in range(w, w + k)]
+    newton = sum(s.newton_iterations for s in sel)
+    return {"newton": newton, "krylov": sum(s.krylov_iterations for s in sel),
+            "launches": sum(s.kernel_launches for s in sel),
+            "residuals": newton + k, "solves": newton,
+            "unconverged_steps": sum(1 for s in sel if not s.converged)}
+
+
+def reference_counts(a):
+    """Per-step counts used to scale the CPU sample when no device run is
+    available (the reference arm runs alone)."""
+    path = os.path.join(ROOT, "equelle_b200", "bench_counts.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        if a.workload in d:
+            return d[a.workload]
+    return {"residuals": 5.0, "solves": 4.0, "krylov": 400.0}
+
+
+if __name__ == "__main__":
+    main()

@@ -20,7 +20,11 @@ CSRC = os.path.join(PKG_DIR, "csrc")
 SIMS = os.path.join(PKG_DIR, "sims")
 OBJ_DIR = os.path.join(PKG_DIR, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-CXX = os.environ.get("CXX", "g++")
+# The system compiler.  A wrapper g++ that puts its own include directories
+# ahead of the system C++ headers built shared objects that crashed in
+# std::istringstream once loaded into a Python process, so the build does
+# not take g++ from $CXX or the PATH.
+CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -28,6 +32,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC",
     "-Xptxas", "-v" if os.environ.get("EQG_PTXAS_VERBOSE") else "-O3",
     "-I" + INCLUDE_DIR, "-I" + CSRC,
+    "-ccbin", CXX,
 ]
 
 
@@ -65,7 +70,9 @@ def build_library(force=False, verbose=False):
         # -Bsymbolic: calls between the library's own exported functions bind
         # inside the library, even when another library exporting the same
         # C ABI (the CPU oracle) is loaded into the process.
-        _run([NVCC, "-shared", "-Xlinker", "-Bsymbolic", "-o", LIB_PATH] + objs + ["-lcudart"])
+        # cudart is linked statically: the library does not depend on which
+        # libcudart.so another component of the process loaded first.
+        _run([NVCC, "-shared", "-cudart", "static", "-Xlinker", "-Bsymbolic", "-o", LIB_PATH] + objs)
     return LIB_PATH
 
 

@@ -48,10 +48,21 @@ class Stats(C.Structure):
         ("patterns_built", C.c_int64), ("pattern_cache_hits", C.c_int64),
         ("device_bytes_in_use", C.c_int64), ("device_bytes_peak", C.c_int64),
         ("last_linear_residual", C.c_double),
+        ("last_matrix_rows", C.c_int64), ("last_matrix_nnz", C.c_int64),
+        ("timed_kernel_launches", C.c_int64), ("timed_kernel_ms", C.c_double),
+        ("residual_evaluations", C.c_int64), ("residual_ms", C.c_double),
+        ("factor_ms", C.c_double), ("krylov_ms", C.c_double),
     ]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [
+        ("start_mark", C.c_int), ("end_mark", C.c_int), ("newton_iterations", C.c_int),
+        ("converged", C.c_int), ("krylov_iterations", C.c_int64), ("kernel_launches", C.c_int64),
+    ]
 
 
 RESIDUAL_FN = C.CFUNCTYPE(C.c_int, vp, vp, vpp)
@@ -69,6 +80,7 @@ SIGNATURES = {
     "eqg_runtime_mark": (C.c_int, [vp, c_int_p]),
     "eqg_runtime_elapsed_ms": (C.c_int, [vp, C.c_int, C.c_int, c_dbl_p]),
     "eqg_runtime_solve_marks": (C.c_int, [vp, C.c_int64, c_int_p, c_int_p]),
+    "eqg_runtime_solve_info": (C.c_int, [vp, C.c_int64, C.POINTER(SolveInfo)]),
     "eqg_set_builtin": (C.c_int, [vp, C.c_int, vpp]),
     "eqg_set_from_host": (C.c_int, [vp, C.c_int, c_i32_p, C.c_int64, vpp]),
     "eqg_set_size": (C.c_int, [vp, c_i64_p]),

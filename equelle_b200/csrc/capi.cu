@@ -11,6 +11,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -24,11 +25,27 @@ namespace {
 
 thread_local std::string g_last_error;
 
-template <class F>
-int guarded(F&& f)
+// EQG_TRACE=1 in the environment prints every C-ABI call to stderr.
+bool trace_enabled()
 {
+    static const bool on = std::getenv("EQG_TRACE") != nullptr;
+    return on;
+}
+
+template <class F>
+int guarded(const char* name, F&& f)
+{
+    const bool trace = trace_enabled();
+    if (trace) {
+        std::fprintf(stderr, "[eqg] %s\n", name);
+        std::fflush(stderr);
+    }
     try {
         f();
+        if (trace) {
+            std::fprintf(stderr, "[eqg] %s ok\n", name);
+            std::fflush(stderr);
+        }
         return EQG_OK;
     } catch (const Error& e) {
         g_last_error = e.what();
@@ -262,13 +279,19 @@ const char* eqg_backend_name(void) { return "cuda-sm100a"; }
 
 int eqg_runtime_create(int nparams, const char* const* keys, const char* const* values, eqg_runtime** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(out, "out");
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
             cudaGetLastError();
             fail(EQG_ERR_DEVICE, "no CUDA device is visible; libeqg.so has no CPU implementation");
         }
+        for (int i = 0; i < nparams; ++i)
+            if (std::string(keys[i]) == "device") {
+                const int dev = std::stoi(values[i]);
+                if (dev < 0 || dev >= ndev) fail(EQG_ERR_ARG, "device index out of range");
+                EQG_CUDA(cudaSetDevice(dev));
+            }
         auto rt = std::make_unique<eqg_runtime>();
         rt->core = std::make_shared<Core>();
         Core& c = *rt->core;
@@ -285,6 +308,7 @@ int eqg_runtime_create(int nparams, const char* const* keys, const char* const* 
         c.verbose = c.param_i("verbose", 0);
         c.max_iter = c.param_i("max_iter", 10);
         c.abs_res_tol = c.param_d("abs_res_tol", 1e-6);
+        c.timed_kernel = c.param_s("time_kernel", "");
         c.red_partials = c.allocN<double>((size_t)kRedBlocks * 4);
         c.red_counter = c.allocN<unsigned int>(1);
         build_grid(c, rt->builtin);
@@ -314,7 +338,7 @@ void eqg_runtime_destroy(eqg_runtime* rt)
 
 int eqg_runtime_grid_info(const eqg_runtime* rt, eqg_grid_info* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         const Core& c = *rt->core;
         out->dimensions = c.dim;
@@ -332,7 +356,7 @@ int eqg_runtime_grid_info(const eqg_runtime* rt, eqg_grid_info* out)
 
 int eqg_runtime_synchronize(eqg_runtime* rt)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         rt->core->sync();
     });
@@ -340,7 +364,7 @@ int eqg_runtime_synchronize(eqg_runtime* rt)
 
 int eqg_runtime_stats(const eqg_runtime* rt, eqg_stats* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         const Core& c = *rt->core;
         out->kernel_launches = c.launches.load();
@@ -354,12 +378,27 @@ int eqg_runtime_stats(const eqg_runtime* rt, eqg_stats* out)
         out->device_bytes_in_use = c.bytes_in_use;
         out->device_bytes_peak = c.bytes_peak;
         out->last_linear_residual = c.solver.last_residual;
+        out->last_matrix_rows = c.solver.last_rows;
+        out->last_matrix_nnz = c.solver.last_nnz;
+        out->timed_kernel_launches = (int64_t)c.timer_pairs.size();
+        double ms = 0.0;
+        for (auto& pr : c.timer_pairs) {
+            float f = 0.f;
+            EQG_CUDA(cudaEventSynchronize(pr.second));
+            EQG_CUDA(cudaEventElapsedTime(&f, pr.first, pr.second));
+            ms += f;
+        }
+        out->timed_kernel_ms = ms;
+        out->residual_evaluations = c.residual_clock.count;
+        out->residual_ms = c.residual_clock.total_ms();
+        out->factor_ms = c.factor_clock.total_ms();
+        out->krylov_ms = c.krylov_clock.total_ms();
     });
 }
 
 int eqg_runtime_reset_stats(eqg_runtime* rt)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         Core& c = *rt->core;
         c.launches = 0;
@@ -367,12 +406,20 @@ int eqg_runtime_reset_stats(eqg_runtime* rt)
         c.solver = SolverStats{};
         c.patterns_built = c.pattern_hits = 0;
         c.bytes_peak = c.bytes_in_use;
+        for (auto& pr : c.timer_pairs) {
+            cudaEventDestroy(pr.first);
+            cudaEventDestroy(pr.second);
+        }
+        c.timer_pairs.clear();
+        c.residual_clock.clear();
+        c.factor_clock.clear();
+        c.krylov_clock.clear();
     });
 }
 
 int eqg_runtime_mark(eqg_runtime* rt, int* mark_id)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         *mark_id = mark(*rt->core);
     });
@@ -380,7 +427,7 @@ int eqg_runtime_mark(eqg_runtime* rt, int* mark_id)
 
 int eqg_runtime_elapsed_ms(eqg_runtime* rt, int a, int b, double* ms)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         Core& c = *rt->core;
         if (a < 0 || b < 0 || a >= (int)c.marks.size() || b >= (int)c.marks.size())
@@ -394,19 +441,29 @@ int eqg_runtime_elapsed_ms(eqg_runtime* rt, int a, int b, double* ms)
 
 int eqg_runtime_solve_marks(const eqg_runtime* rt, int64_t k, int* s, int* e)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         const Core& c = *rt->core;
-        if (k < 0 || k >= (int64_t)c.solve_marks.size()) fail(EQG_ERR_ARG, "solve index out of range");
-        *s = c.solve_marks[k].first;
-        *e = c.solve_marks[k].second;
+        if (k < 0 || k >= (int64_t)c.solves.size()) fail(EQG_ERR_ARG, "solve index out of range");
+        *s = c.solves[k].start_mark;
+        *e = c.solves[k].end_mark;
+    });
+}
+
+int eqg_runtime_solve_info(const eqg_runtime* rt, int64_t k, eqg_solve_info* out)
+{
+    return guarded(__func__, [&] {
+        need(rt, "runtime");
+        const Core& c = *rt->core;
+        if (k < 0 || k >= (int64_t)c.solves.size()) fail(EQG_ERR_ARG, "solve index out of range");
+        *out = c.solves[k];
     });
 }
 
 // ---- sets -------------------------------------------------------------------
 int eqg_set_builtin(eqg_runtime* rt, int which, eqg_set** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         if (which < 0 || which > 5) fail(EQG_ERR_ARG, "unknown builtin set");
         eqg_set_retain(rt->builtin[which]);
@@ -416,7 +473,7 @@ int eqg_set_builtin(eqg_runtime* rt, int which, eqg_set** out)
 
 int eqg_set_from_host(eqg_runtime* rt, int entity, const int32_t* idx, int64_t n, eqg_set** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         Core& c = *rt->core;
         if (entity != EQG_CELLS && entity != EQG_FACES) fail(EQG_ERR_ARG, "bad entity kind");
@@ -430,7 +487,7 @@ int eqg_set_from_host(eqg_runtime* rt, int entity, const int32_t* idx, int64_t n
 
 int eqg_set_size(const eqg_set* s, int64_t* n)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(s, "set");
         *n = s->n;
     });
@@ -438,7 +495,7 @@ int eqg_set_size(const eqg_set* s, int64_t* n)
 
 int eqg_set_entity(const eqg_set* s, int* e)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(s, "set");
         *e = s->entity;
     });
@@ -446,7 +503,7 @@ int eqg_set_entity(const eqg_set* s, int* e)
 
 int eqg_set_to_host(const eqg_set* s, int32_t* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(s, "set");
         download(*s->core, out, s->idx->ptr, (size_t)s->n * 4);
     });
@@ -464,7 +521,7 @@ void eqg_set_release(eqg_set* s)
 
 static int neighbour(eqg_runtime* rt, const eqg_set* faces, int side, eqg_set** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(faces, "faces");
         const CoreP& cp = rt->core;
@@ -488,7 +545,7 @@ int eqg_second_cell(eqg_runtime* rt, const eqg_set* f, eqg_set** out) { return n
 
 int eqg_set_is_empty(eqg_runtime* rt, const eqg_set* s, eqg_mask** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(s, "set");
         Core& c = *rt->core;
@@ -500,7 +557,7 @@ int eqg_set_is_empty(eqg_runtime* rt, const eqg_set* s, eqg_mask** out)
 
 int eqg_set_on(eqg_runtime* rt, const eqg_set* data, const eqg_set* from, const eqg_set* to, eqg_set** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(data, "data");
         need(from, "from");
@@ -517,7 +574,7 @@ int eqg_set_on(eqg_runtime* rt, const eqg_set* data, const eqg_set* from, const 
 
 int eqg_set_extend(eqg_runtime* rt, const eqg_set* data, const eqg_set* from, const eqg_set* to, eqg_set** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(data, "data");
         need(from, "from");
@@ -539,7 +596,7 @@ int eqg_set_extend(eqg_runtime* rt, const eqg_set* data, const eqg_set* from, co
 
 int eqg_set_select(eqg_runtime* rt, const eqg_mask* pred, const eqg_set* a, const eqg_set* b, eqg_set** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(pred, "predicate");
         need(a, "iftrue");
@@ -556,7 +613,7 @@ int eqg_set_select(eqg_runtime* rt, const eqg_mask* pred, const eqg_set* a, cons
 
 int eqg_set_check_subset(eqg_runtime* rt, const eqg_set* sub, const eqg_set* super, int* is_sorted, int* is_included)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(sub, "subset");
         need(super, "superset");
@@ -575,7 +632,7 @@ int eqg_set_check_subset(eqg_runtime* rt, const eqg_set* sub, const eqg_set* sup
 // ---- masks --------------------------------------------------------------------
 int eqg_mask_from_host(eqg_runtime* rt, const uint8_t* v, int64_t n, eqg_mask** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         if (n < 0) fail(EQG_ERR_ARG, "negative size");
         std::vector<uint8_t> norm(v, v + n);
@@ -586,7 +643,7 @@ int eqg_mask_from_host(eqg_runtime* rt, const uint8_t* v, int64_t n, eqg_mask** 
 
 int eqg_mask_size(const eqg_mask* m, int64_t* n)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(m, "mask");
         *n = m->n;
     });
@@ -594,7 +651,7 @@ int eqg_mask_size(const eqg_mask* m, int64_t* n)
 
 int eqg_mask_to_host(const eqg_mask* m, uint8_t* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(m, "mask");
         download(*m->core, out, m->v->ptr, (size_t)m->n);
     });
@@ -612,7 +669,7 @@ void eqg_mask_release(eqg_mask* m)
 
 int eqg_mask_logic(eqg_runtime* rt, int op, const eqg_mask* a, const eqg_mask* b, eqg_mask** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "mask");
         if (op != EQG_NOT) {
@@ -631,7 +688,7 @@ int eqg_mask_logic(eqg_runtime* rt, int op, const eqg_mask* a, const eqg_mask* b
 // ---- scalar collections ------------------------------------------------------------
 int eqg_coll_from_host(eqg_runtime* rt, const double* v, int64_t n, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         if (n < 0) fail(EQG_ERR_ARG, "negative size");
         *out = new_coll(rt->core, n, upload(*rt->core, v, (size_t)n * 8));
@@ -640,7 +697,7 @@ int eqg_coll_from_host(eqg_runtime* rt, const double* v, int64_t n, eqg_coll** o
 
 int eqg_coll_constant(eqg_runtime* rt, double v, int64_t n, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         if (n < 0) fail(EQG_ERR_ARG, "negative size");
         Core& c = *rt->core;
@@ -652,7 +709,7 @@ int eqg_coll_constant(eqg_runtime* rt, double v, int64_t n, eqg_coll** out)
 
 int eqg_coll_size(const eqg_coll* c, int64_t* n)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(c, "collection");
         *n = c->n;
     });
@@ -660,7 +717,7 @@ int eqg_coll_size(const eqg_coll* c, int64_t* n)
 
 int eqg_coll_to_host(const eqg_coll* c, double* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(c, "collection");
         download(*c->core, out, c->val->ptr, (size_t)c->n * 8);
     });
@@ -668,7 +725,7 @@ int eqg_coll_to_host(const eqg_coll* c, double* out)
 
 int eqg_coll_jacobian_info(const eqg_coll* c, int64_t* rows, int64_t* cols, int64_t* nnz)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(c, "collection");
         if (!c->pat) {
             *rows = c->n;
@@ -684,7 +741,7 @@ int eqg_coll_jacobian_info(const eqg_coll* c, int64_t* rows, int64_t* cols, int6
 
 int eqg_coll_jacobian_to_host(const eqg_coll* c, int64_t* rowptr, int32_t* colind, double* vals)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(c, "collection");
         if (!c->pat) fail(EQG_ERR_ARG, "collection has no Jacobian");
         Core& core = *c->core;
@@ -711,7 +768,7 @@ void eqg_coll_release(eqg_coll* c)
 
 int eqg_variable(eqg_runtime* rt, const eqg_coll* init, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(init, "collection");
         Core& c = *rt->core;
@@ -722,7 +779,7 @@ int eqg_variable(eqg_runtime* rt, const eqg_coll* init, eqg_coll** out)
 
 int eqg_value_of(eqg_runtime* rt, const eqg_coll* x, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(x, "collection");
         *out = new_coll(rt->core, x->n, x->val);
@@ -731,7 +788,7 @@ int eqg_value_of(eqg_runtime* rt, const eqg_coll* x, eqg_coll** out)
 
 int eqg_binary(eqg_runtime* rt, int op, const eqg_coll* a, const eqg_coll* b, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "lhs");
         need(b, "rhs");
@@ -761,7 +818,7 @@ int eqg_binary(eqg_runtime* rt, int op, const eqg_coll* a, const eqg_coll* b, eq
 
 int eqg_binary_scalar(eqg_runtime* rt, int op, const eqg_coll* a, double s, int scalar_left, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
         Core& c = *rt->core;
@@ -812,7 +869,7 @@ int eqg_binary_scalar(eqg_runtime* rt, int op, const eqg_coll* a, double s, int 
 
 int eqg_unary(eqg_runtime* rt, int op, const eqg_coll* a, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
         Core& c = *rt->core;
@@ -829,7 +886,7 @@ int eqg_unary(eqg_runtime* rt, int op, const eqg_coll* a, eqg_coll** out)
 
 int eqg_compare(eqg_runtime* rt, int op, const eqg_coll* a, const eqg_coll* b, eqg_mask** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "lhs");
         need(b, "rhs");
@@ -844,7 +901,7 @@ int eqg_compare(eqg_runtime* rt, int op, const eqg_coll* a, const eqg_coll* b, e
 
 int eqg_compare_scalar(eqg_runtime* rt, int op, const eqg_coll* a, double s, int scalar_left, eqg_mask** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
         if (op < EQG_LT || op > EQG_NE) fail(EQG_ERR_ARG, "unknown comparison");
@@ -857,7 +914,7 @@ int eqg_compare_scalar(eqg_runtime* rt, int op, const eqg_coll* a, double s, int
 
 int eqg_gradient(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
         if (a->n != rt->core->nc) fail(EQG_ERR_ARG, "Gradient needs a collection on all cells");
@@ -867,7 +924,7 @@ int eqg_gradient(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
 
 int eqg_neg_gradient(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
         if (a->n != rt->core->nc) fail(EQG_ERR_ARG, "negGradient needs a collection on all cells");
@@ -877,7 +934,7 @@ int eqg_neg_gradient(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
 
 int eqg_interior_divergence(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
         if (a->n != rt->core->nif) fail(EQG_ERR_ARG, "interiorDivergence needs a collection on interior faces");
@@ -887,7 +944,7 @@ int eqg_interior_divergence(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
 
 int eqg_divergence(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
         const Core& c = *rt->core;
@@ -902,7 +959,7 @@ int eqg_divergence(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
 
 int eqg_on(eqg_runtime* rt, const eqg_coll* data, const eqg_set* from, const eqg_set* to, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(data, "data");
         need(from, "from");
@@ -916,7 +973,7 @@ int eqg_on(eqg_runtime* rt, const eqg_coll* data, const eqg_set* from, const eqg
 
 int eqg_extend(eqg_runtime* rt, const eqg_coll* data, const eqg_set* from, const eqg_set* to, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(data, "data");
         need(from, "from");
@@ -930,7 +987,7 @@ int eqg_extend(eqg_runtime* rt, const eqg_coll* data, const eqg_set* from, const
 
 int eqg_select(eqg_runtime* rt, const eqg_mask* pred, const eqg_coll* a, const eqg_coll* b, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(pred, "predicate");
         need(a, "iftrue");
@@ -949,7 +1006,7 @@ int eqg_select(eqg_runtime* rt, const eqg_mask* pred, const eqg_coll* a, const e
 
 int eqg_span_subset(eqg_runtime* rt, const eqg_coll* a, int64_t start, int64_t num, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
         if (start < 0 || num < 0 || start + num > a->n) fail(EQG_ERR_ARG, "span out of range");
@@ -960,7 +1017,7 @@ int eqg_span_subset(eqg_runtime* rt, const eqg_coll* a, int64_t start, int64_t n
 
 int eqg_span_superset(eqg_runtime* rt, const eqg_coll* a, int64_t start, int64_t total, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
         if (start < 0 || start + a->n > total) fail(EQG_ERR_ARG, "span out of range");
@@ -971,7 +1028,7 @@ int eqg_span_superset(eqg_runtime* rt, const eqg_coll* a, int64_t start, int64_t
 
 int eqg_reduce(eqg_runtime* rt, int op, const eqg_coll* a, double* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
         if (op < EQG_MIN || op > EQG_PROD) fail(EQG_ERR_ARG, "unknown reduction");
@@ -982,7 +1039,7 @@ int eqg_reduce(eqg_runtime* rt, int op, const eqg_coll* a, double* out)
 
 int eqg_two_norm(eqg_runtime* rt, const eqg_coll* a, double* out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
         *out = k_two_norm(*rt->core, a->val->as<double>(), a->n);
@@ -991,7 +1048,7 @@ int eqg_two_norm(eqg_runtime* rt, const eqg_coll* a, double* out)
 
 int eqg_measure(eqg_runtime* rt, const eqg_set* s, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(s, "set");
         Core& c = *rt->core;
@@ -1006,7 +1063,7 @@ int eqg_measure(eqg_runtime* rt, const eqg_set* s, eqg_coll** out)
 
 int eqg_centroid(eqg_runtime* rt, const eqg_set* s, int comp, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(s, "set");
         Core& c = *rt->core;
@@ -1023,7 +1080,7 @@ int eqg_centroid(eqg_runtime* rt, const eqg_set* s, int comp, eqg_coll** out)
 
 int eqg_normal(eqg_runtime* rt, const eqg_set* s, int comp, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(s, "set");
         Core& c = *rt->core;
@@ -1039,7 +1096,7 @@ int eqg_normal(eqg_runtime* rt, const eqg_set* s, int comp, eqg_coll** out)
 
 int eqg_solve_for_update(eqg_runtime* rt, const eqg_coll* residual, eqg_coll** du)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(residual, "residual");
         Core& c = *rt->core;
@@ -1052,6 +1109,8 @@ int eqg_solve_for_update(eqg_runtime* rt, const eqg_coll* residual, eqg_coll** d
         c.solver.krylov_iterations += r.iterations;
         c.solver.refinement_sweeps += r.sweeps;
         c.solver.last_residual = r.rel_residual;
+        c.solver.last_rows = residual->pat->rows;
+        c.solver.last_nnz = residual->pat->nnz;
         if (c.verbose > 2)
             std::printf("        solveForUpdate: BiCGStab+ILU0 %d iterations (%d sweeps), rel. residual %g\n",
                         r.iterations, r.sweeps, r.rel_residual);
@@ -1062,13 +1121,15 @@ int eqg_solve_for_update(eqg_runtime* rt, const eqg_coll* residual, eqg_coll** d
 
 int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_coll* u0, eqg_coll** out)
 {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need(rt, "runtime");
         need(u0, "initial guess");
         if (!fn) fail(EQG_ERR_ARG, "null residual function");
         Core& c = *rt->core;
         const int m0 = mark(c);
         c.newton_solves++;
+        const int64_t krylov0 = c.solver.krylov_iterations;
+        const int64_t launches0 = c.launches.load();
         struct Ref {
             eqg_coll* p = nullptr;
             ~Ref() { eqg_coll_release(p); }
@@ -1082,7 +1143,13 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
         if (eqg_variable(rt, u0, &tmp) != EQG_OK) fail(EQG_ERR_ARG, g_last_error);
         u.reset(tmp);
         tmp = nullptr;
-        if (fn(user, u.p, &tmp) != 0 || !tmp) fail(EQG_ERR_CALLBACK, "residual callback failed");
+        auto evaluate = [&](eqg_coll* uu, eqg_coll** r) {
+            c.residual_clock.start(c.stream);
+            const int st = fn(user, uu, r);
+            c.residual_clock.stop(c.stream);
+            return st;
+        };
+        if (evaluate(u.p, &tmp) != 0 || !tmp) fail(EQG_ERR_CALLBACK, "residual callback failed");
         res.reset(tmp);
         if (res.p->n != u.p->n) fail(EQG_ERR_ARG, "newtonSolve: residual and unknown differ in size");
         double norm = k_two_norm(c, res.p->val->as<double>(), res.p->n);
@@ -1101,7 +1168,7 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
             u.reset(un);
             res.reset(nullptr);
             tmp = nullptr;
-            if (fn(user, u.p, &tmp) != 0 || !tmp) fail(EQG_ERR_CALLBACK, "residual callback failed");
+            if (evaluate(u.p, &tmp) != 0 || !tmp) fail(EQG_ERR_CALLBACK, "residual callback failed");
             res.reset(tmp);
             norm = k_two_norm(c, res.p->val->as<double>(), res.p->n);
             ++iter;
@@ -1115,8 +1182,14 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
             else std::printf("Newton solver converged in %d iterations\n", iter);
         }
         *out = new_coll(rt->core, u.p->n, u.p->val);
-        const int m1 = mark(c);
-        c.solve_marks.emplace_back(m0, m1);
+        eqg_solve_info info{};
+        info.start_mark = m0;
+        info.newton_iterations = iter;
+        info.converged = norm <= c.abs_res_tol ? 1 : 0;
+        info.krylov_iterations = c.solver.krylov_iterations - krylov0;
+        info.kernel_launches = c.launches.load() - launches0;
+        info.end_mark = mark(c);
+        c.solves.push_back(info);
     });
 }
 

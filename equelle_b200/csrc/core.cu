@@ -56,6 +56,13 @@ Core::~Core()
     red_partials.reset();
     red_counter.reset();
     for (auto& m : marks) cudaEventDestroy(m.ev);
+    for (auto& pr : timer_pairs) {
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
+    residual_clock.clear();
+    factor_clock.clear();
+    krylov_clock.clear();
     if (stream) {
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);

@@ -83,10 +83,54 @@ using OpMatrixP = std::shared_ptr<OpMatrix>;
 struct SolverStats {
     int64_t linear_solves = 0, krylov_iterations = 0, refinement_sweeps = 0;
     double last_residual = 0.0;
+    int64_t last_rows = 0, last_nnz = 0;
 };
 
 struct Mark {
     cudaEvent_t ev;
+};
+
+// Accumulated device time of one phase (pairs of events on the stream).
+struct PhaseClock {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pairs;
+    cudaEvent_t open = nullptr;
+    int64_t count = 0;
+    void start(cudaStream_t s)
+    {
+        cudaEventCreate(&open);
+        cudaEventRecord(open, s);
+    }
+    void stop(cudaStream_t s)
+    {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, s);
+        pairs.emplace_back(open, e);
+        open = nullptr;
+        ++count;
+    }
+    double total_ms() const
+    {
+        double ms = 0.0;
+        for (auto& p : pairs) {
+            float f = 0.f;
+            cudaEventSynchronize(p.second);
+            cudaEventElapsedTime(&f, p.first, p.second);
+            ms += f;
+        }
+        return ms;
+    }
+    void clear()
+    {
+        for (auto& p : pairs) {
+            cudaEventDestroy(p.first);
+            cudaEventDestroy(p.second);
+        }
+        pairs.clear();
+        if (open) cudaEventDestroy(open);
+        open = nullptr;
+        count = 0;
+    }
 };
 
 // Runtime state shared by every handle (a handle keeps the core alive).
@@ -131,7 +175,11 @@ struct Core {
     Buf red_counter;    // unsigned int
     double* pinned = nullptr;  // small pinned host buffer
     std::vector<Mark> marks;
-    std::vector<std::pair<int, int>> solve_marks;
+    std::vector<eqg_solve_info> solves;
+    // device timing of one named kernel (parameter time_kernel)
+    std::string timed_kernel;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timer_pairs;
+    PhaseClock residual_clock, factor_clock, krylov_clock;
 
     Core();
     ~Core();
@@ -149,6 +197,26 @@ struct Core {
 };
 
 using CoreP = std::shared_ptr<Core>;
+
+// Launches a kernel through `f`, checks the launch, and brackets it with
+// CUDA events on the runtime stream when `name` is the timed kernel.
+template <class F>
+inline void launch(Core& c, const char* name, F&& f)
+{
+    const bool timed = !c.timed_kernel.empty() && c.timed_kernel == name;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (timed) {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, c.stream);
+    }
+    f();
+    c.checkLaunch(name);
+    if (timed) {
+        cudaEventRecord(b, c.stream);
+        c.timer_pairs.emplace_back(a, b);
+    }
+}
 
 constexpr int kThreads = 256;
 constexpr int kRedBlocks = 592;  // 4 x 148 SMs

@@ -343,9 +343,8 @@ int64_t counts_to_rowptr(Core& c, Buf& counts, int rows, Buf& rowptr)
     }
     if (total > (int64_t)INT_MAX) fail(EQG_ERR_UNSUPPORTED, "sparsity pattern with more than 2^31-1 entries");
     rowptr = c.allocN<int>((size_t)rows + 1);
-    i64_to_rowptr_kernel<<<blocksFor((int64_t)rows + 1), kThreads, 0, c.stream>>>(incl->as<int64_t>(), rows,
-                                                                                  rowptr->as<int>());
-    c.checkLaunch("rowptr");
+    launch(c, "rowptr", [&] { i64_to_rowptr_kernel<<<blocksFor((int64_t)rows + 1), kThreads, 0, c.stream>>>(incl->as<int64_t>(), rows,
+                                                                                  rowptr->as<int>()); });
     return total;
 }
 
@@ -357,18 +356,16 @@ void spgemm_symbolic(Core& c, const OpMatrix& m, const Pattern& j, Pattern& out)
     Buf cnt = c.allocN<int64_t>(m.n_out > 0 ? m.n_out : 1);
     const int nb = blocksFor(m.n_out);
     if (m.n_out > 0) {
-        spgemm_count_kernel<KMAX><<<nb, kThreads, 0, c.stream>>>(m.n_out, m.ptr->as<int>(), m.src->as<int>(),
+        launch(c, "spgemm_count", [&] { spgemm_count_kernel<KMAX><<<nb, kThreads, 0, c.stream>>>(m.n_out, m.ptr->as<int>(), m.src->as<int>(),
                                                                 j.rowptr->as<int>(), j.colind->as<int>(),
-                                                                cnt->as<int64_t>());
-        c.checkLaunch("spgemm_count");
+                                                                cnt->as<int64_t>()); });
     }
     out.nnz = counts_to_rowptr(c, cnt, m.n_out, out.rowptr);
     out.colind = c.allocN<int>(out.nnz > 0 ? out.nnz : 1);
     if (m.n_out > 0) {
-        spgemm_fill_kernel<KMAX><<<nb, kThreads, 0, c.stream>>>(m.n_out, m.ptr->as<int>(), m.src->as<int>(),
+        launch(c, "spgemm_fill", [&] { spgemm_fill_kernel<KMAX><<<nb, kThreads, 0, c.stream>>>(m.n_out, m.ptr->as<int>(), m.src->as<int>(),
                                                                j.rowptr->as<int>(), j.colind->as<int>(),
-                                                               out.rowptr->as<int>(), out.colind->as<int>());
-        c.checkLaunch("spgemm_fill");
+                                                               out.rowptr->as<int>(), out.colind->as<int>()); });
     }
 }
 
@@ -376,10 +373,9 @@ template <int KMAX>
 void spgemm_numeric(Core& c, const OpMatrix& m, const Pattern& jp, const double* jv, const Pattern& op, double* ov)
 {
     if (m.n_out <= 0) return;
-    spgemm_numeric_kernel<KMAX><<<blocksFor(m.n_out), kThreads, 0, c.stream>>>(
+    launch(c, "spgemm_numeric", [&] { spgemm_numeric_kernel<KMAX><<<blocksFor(m.n_out), kThreads, 0, c.stream>>>(
         m.n_out, m.ptr->as<int>(), m.src->as<int>(), m.w->as<double>(), jp.rowptr->as<int>(), jp.colind->as<int>(),
-        jv, op.rowptr->as<int>(), op.colind->as<int>(), ov);
-    c.checkLaunch("spgemm_numeric");
+        jv, op.rowptr->as<int>(), op.colind->as<int>(), ov); });
 }
 
 int kmax_for(int max_row)
@@ -426,9 +422,8 @@ OpMatrixP opmat_from_map(Core& c, const int32_t* map_dev, int n_out, int n_src, 
     Buf err = c.allocN<int32_t>(1);
     EQG_CUDA(cudaMemsetAsync(err->ptr, 0, 4, c.stream));
     if (n_out > 0) {
-        map_count_kernel<<<blocksFor(n_out), kThreads, 0, c.stream>>>(map_dev, n_out, cnt->as<int64_t>(), n_src,
-                                                                      err->as<int32_t>());
-        c.checkLaunch("map_count");
+        launch(c, "map_count", [&] { map_count_kernel<<<blocksFor(n_out), kThreads, 0, c.stream>>>(map_dev, n_out, cnt->as<int64_t>(), n_src,
+                                                                      err->as<int32_t>()); });
     }
     const int64_t nnz = counts_to_rowptr(c, cnt, n_out, m->ptr);
     int32_t herr = 0;
@@ -440,9 +435,8 @@ OpMatrixP opmat_from_map(Core& c, const int32_t* map_dev, int n_out, int n_src, 
     m->src = c.allocN<int32_t>(nnz > 0 ? nnz : 1);
     m->w = c.allocN<double>(nnz > 0 ? nnz : 1);
     if (n_out > 0) {
-        map_fill_kernel<<<blocksFor(n_out), kThreads, 0, c.stream>>>(map_dev, n_out, m->ptr->as<int>(),
-                                                                    m->src->as<int>(), m->w->as<double>());
-        c.checkLaunch("map_fill");
+        launch(c, "map_fill", [&] { map_fill_kernel<<<blocksFor(n_out), kThreads, 0, c.stream>>>(map_dev, n_out, m->ptr->as<int>(),
+                                                                    m->src->as<int>(), m->w->as<double>()); });
     }
     return m;
 }
@@ -450,9 +444,8 @@ OpMatrixP opmat_from_map(Core& c, const int32_t* map_dev, int n_out, int n_src, 
 void opmat_apply_values(Core& c, const OpMatrix& m, const double* x, double* y)
 {
     if (m.n_out <= 0) return;
-    opmat_apply_kernel<<<blocksFor(m.n_out), kThreads, 0, c.stream>>>(m.n_out, m.ptr->as<int>(), m.src->as<int>(),
-                                                                     m.w->as<double>(), x, y);
-    c.checkLaunch("opmat_apply");
+    launch(c, "opmat_apply", [&] { opmat_apply_kernel<<<blocksFor(m.n_out), kThreads, 0, c.stream>>>(m.n_out, m.ptr->as<int>(), m.src->as<int>(),
+                                                                     m.w->as<double>(), x, y); });
 }
 
 PatternP pattern_identity(Core& c, int n)
@@ -466,9 +459,8 @@ PatternP pattern_identity(Core& c, int n)
     p->max_row = n > 0 ? 1 : 0;
     p->rowptr = c.allocN<int>((size_t)n + 1);
     p->colind = c.allocN<int>(n > 0 ? n : 1);
-    identity_pattern_kernel<<<blocksFor((int64_t)n + 1), kThreads, 0, c.stream>>>(n, p->rowptr->as<int>(),
-                                                                                 p->colind->as<int>(), nullptr);
-    c.checkLaunch("identity_pattern");
+    launch(c, "identity_pattern", [&] { identity_pattern_kernel<<<blocksFor((int64_t)n + 1), kThreads, 0, c.stream>>>(n, p->rowptr->as<int>(),
+                                                                                 p->colind->as<int>(), nullptr); });
     c.identity_patterns[n] = p;
     return p;
 }
@@ -479,8 +471,7 @@ Buf ones(Core& c, int64_t n)
     if (it != c.ones_cache.end()) return it->second;
     Buf b = c.allocN<double>(n > 0 ? n : 1);
     if (n > 0) {
-        ones_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(b->as<double>(), n);
-        c.checkLaunch("ones");
+        launch(c, "ones", [&] { ones_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(b->as<double>(), n); });
     }
     c.ones_cache[n] = b;
     return b;
@@ -542,18 +533,16 @@ PatternP pattern_union(Core& c, const PatternP& a, const PatternP& b)
     Buf cnt = c.allocN<int64_t>(p->rows > 0 ? p->rows : 1);
     const int nb = blocksFor(p->rows);
     if (p->rows > 0) {
-        union_kernel<false><<<nb, kThreads, 0, c.stream>>>(p->rows, a->rowptr->as<int>(), a->colind->as<int>(),
+        launch(c, "union_count", [&] { union_kernel<false><<<nb, kThreads, 0, c.stream>>>(p->rows, a->rowptr->as<int>(), a->colind->as<int>(),
                                                           b->rowptr->as<int>(), b->colind->as<int>(),
-                                                          cnt->as<int64_t>(), nullptr, nullptr);
-        c.checkLaunch("union_count");
+                                                          cnt->as<int64_t>(), nullptr, nullptr); });
     }
     p->nnz = counts_to_rowptr(c, cnt, p->rows, p->rowptr);
     p->colind = c.allocN<int>(p->nnz > 0 ? p->nnz : 1);
     if (p->rows > 0) {
-        union_kernel<true><<<nb, kThreads, 0, c.stream>>>(p->rows, a->rowptr->as<int>(), a->colind->as<int>(),
+        launch(c, "union_fill", [&] { union_kernel<true><<<nb, kThreads, 0, c.stream>>>(p->rows, a->rowptr->as<int>(), a->colind->as<int>(),
                                                          b->rowptr->as<int>(), b->colind->as<int>(), nullptr,
-                                                         p->rowptr->as<int>(), p->colind->as<int>());
-        c.checkLaunch("union_fill");
+                                                         p->rowptr->as<int>(), p->colind->as<int>()); });
     }
     c.patterns_built++;
     c.pattern_cache[key] = p;
@@ -565,8 +554,7 @@ void pattern_build_rowidx(Core& c, Pattern& p)
     if (p.rowidx) return;
     p.rowidx = c.allocN<int>(p.nnz > 0 ? p.nnz : 1);
     if (p.rows > 0) {
-        rowidx_kernel<<<blocksFor(p.rows), kThreads, 0, c.stream>>>(p.rows, p.rowptr->as<int>(), p.rowidx->as<int>());
-        c.checkLaunch("rowidx");
+        launch(c, "rowidx", [&] { rowidx_kernel<<<blocksFor(p.rows), kThreads, 0, c.stream>>>(p.rows, p.rowptr->as<int>(), p.rowidx->as<int>()); });
     }
 }
 
@@ -577,15 +565,13 @@ void jacobian_elementwise(Core& c, const JacArgs& a, const Pattern& out, double*
     if (out.nnz <= 0) return;
     if (flat) {
         pattern_build_rowidx(c, const_cast<Pattern&>(out));
-        ew_flat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(r, out.rowidx->as<int>(), a.pa ? a.ja : nullptr,
-                                                                      a.pb ? a.jb : nullptr, jout, out.nnz);
-        c.checkLaunch("jac_flat");
+        launch(c, "jac_flat", [&] { ew_flat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(r, out.rowidx->as<int>(), a.pa ? a.ja : nullptr,
+                                                                      a.pb ? a.jb : nullptr, jout, out.nnz); });
     } else {
-        ew_merge_kernel<<<blocksFor(out.rows), kThreads, 0, c.stream>>>(
+        launch(c, "jac_merge", [&] { ew_merge_kernel<<<blocksFor(out.rows), kThreads, 0, c.stream>>>(
             r, out.rows, a.pa ? a.pa->rowptr->as<int>() : nullptr, a.pa ? a.pa->colind->as<int>() : nullptr,
             a.pa ? a.ja : nullptr, a.pb ? a.pb->rowptr->as<int>() : nullptr, a.pb ? a.pb->colind->as<int>() : nullptr,
-            a.pb ? a.jb : nullptr, out.rowptr->as<int>(), out.colind->as<int>(), jout);
-        c.checkLaunch("jac_merge");
+            a.pb ? a.jb : nullptr, out.rowptr->as<int>(), out.colind->as<int>(), jout); });
     }
 }
 

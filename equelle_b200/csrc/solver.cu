@@ -570,15 +570,13 @@ void precondition(Core& c, const SolverAnalysis& an, const T* lu, const T* in, T
     const int ns = (int)an.stage_ptr.size() - 1;
     for (int s = 0; s < ns; ++s) {
         const int r0 = an.stage_ptr[s], r1 = an.stage_ptr[s + 1];
-        ilu0_lower_stage_kernel<T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
-            r0, r1, an.rowptr->as<int>(), an.col->as<int>(), an.diag->as<int>(), lu, in, out, sc, skip_if_s);
-        c.checkLaunch("ilu0_lower");
+        launch(c, "ilu0_lower", [&] { ilu0_lower_stage_kernel<T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
+            r0, r1, an.rowptr->as<int>(), an.col->as<int>(), an.diag->as<int>(), lu, in, out, sc, skip_if_s); });
     }
     for (int s = ns - 1; s >= 0; --s) {
         const int r0 = an.stage_ptr[s], r1 = an.stage_ptr[s + 1];
-        ilu0_upper_stage_kernel<T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
-            r0, r1, an.rowptr->as<int>(), an.col->as<int>(), an.diag->as<int>(), lu, out, sc, skip_if_s);
-        c.checkLaunch("ilu0_upper");
+        launch(c, "ilu0_upper", [&] { ilu0_upper_stage_kernel<T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
+            r0, r1, an.rowptr->as<int>(), an.col->as<int>(), an.diag->as<int>(), lu, out, sc, skip_if_s); });
     }
 }
 
@@ -593,8 +591,7 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, const T* lu, Vecs<
     double* part = an.partials->as<double>();
     unsigned int* cnt = an.counter->as<unsigned int>();
     const int nb = blocksFor(n, kThreads, kRedBlocks);
-    bicg_init_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.b, v.r, v.rhat, v.p, v.v, v.x, n, part, cnt, sc, tol * tol);
-    c.checkLaunch("bicg_init");
+    launch(c, "bicg_init", [&] { bicg_init_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.b, v.r, v.rhat, v.p, v.v, v.x, n, part, cnt, sc, tol * tol); });
     SolveResult res;
     KScal h{};
     double bb = 0.0;
@@ -602,20 +599,15 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, const T* lu, Vecs<
     for (;;) {
         const int chunk = std::min(check_every, max_iter - enq);
         for (int k = 0; k < chunk; ++k) {
-            bicg_p_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(v.r, v.v, v.p, n, sc);
-            c.checkLaunch("bicg_p");
+            launch(c, "bicg_p", [&] { bicg_p_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(v.r, v.v, v.p, n, sc); });
             precondition<T>(c, an, lu, v.p, v.ph, sc, 0);
-            bicg_spmv_alpha_kernel<T><<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(), a, v.ph,
-                                                                    v.rhat, v.v, n, part, cnt, sc);
-            c.checkLaunch("bicg_spmv_alpha");
-            bicg_s_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.r, v.v, v.s, n, part, cnt, sc);
-            c.checkLaunch("bicg_s");
+            launch(c, "bicg_spmv_alpha", [&] { bicg_spmv_alpha_kernel<T><<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(), a, v.ph,
+                                                                    v.rhat, v.v, n, part, cnt, sc); });
+            launch(c, "bicg_s", [&] { bicg_s_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.r, v.v, v.s, n, part, cnt, sc); });
             precondition<T>(c, an, lu, v.s, v.sh, sc, 1);
-            bicg_spmv_omega_kernel<T><<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(), a, v.sh,
-                                                                    v.s, v.t, n, part, cnt, sc);
-            c.checkLaunch("bicg_spmv_omega");
-            bicg_xr_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.ph, v.sh, v.s, v.t, v.rhat, v.x, v.r, n, part, cnt, sc);
-            c.checkLaunch("bicg_xr");
+            launch(c, "bicg_spmv_omega", [&] { bicg_spmv_omega_kernel<T><<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(), a, v.sh,
+                                                                    v.s, v.t, n, part, cnt, sc); });
+            launch(c, "bicg_xr", [&] { bicg_xr_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.ph, v.sh, v.s, v.t, v.rhat, v.x, v.r, n, part, cnt, sc); });
         }
         enq += chunk;
         EQG_CUDA(cudaMemcpyAsync(c.pinned, sc, sizeof(KScal), cudaMemcpyDeviceToHost, c.stream));
@@ -656,43 +648,41 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         return res;
     }
     // permuted matrix and factorization (FP64)
-    gather_values_kernel<<<blocksFor(an.nnz), kThreads, 0, c.stream>>>(jval, an.vmap->as<int>(), an.a64->as<double>(),
-                                                                       an.nnz);
-    c.checkLaunch("gather_values");
+    c.factor_clock.start(c.stream);
+    launch(c, "gather_values", [&] { gather_values_kernel<<<blocksFor(an.nnz), kThreads, 0, c.stream>>>(jval, an.vmap->as<int>(), an.a64->as<double>(),
+                                                                       an.nnz); });
     EQG_CUDA(cudaMemcpyAsync(an.lu64->ptr, an.a64->ptr, (size_t)an.nnz * 8, cudaMemcpyDeviceToDevice, c.stream));
     EQG_CUDA(cudaMemsetAsync(an.factor_status->ptr, 0, sizeof(int), c.stream));
     const int ns = (int)an.stage_ptr.size() - 1;
     for (int s = 0; s < ns; ++s) {
         const int r0 = an.stage_ptr[s], r1 = an.stage_ptr[s + 1];
-        ilu0_factor_stage_kernel<<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
+        launch(c, "ilu0_factor", [&] { ilu0_factor_stage_kernel<<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
             r0, r1, an.rowptr->as<int>(), an.col->as<int>(), an.diag->as<int>(), an.lu64->as<double>(),
-            an.factor_status->as<int>());
-        c.checkLaunch("ilu0_factor");
+            an.factor_status->as<int>()); });
     }
     Vecs<double> v = vecs<double>(an.vec64->as<double>(), n);
-    permute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(rhs, an.perm->as<int>(), v.b, n);
-    c.checkLaunch("permute");
-    int fstat = 0;
-    EQG_CUDA(cudaMemcpyAsync(c.pinned, an.factor_status->ptr, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    c.sync();
-    std::memcpy(&fstat, c.pinned, sizeof(int));
-    if (fstat) return res;  // zero pivot
-
-    if (!mixed) {
-        res = bicgstab<double>(c, an, an.a64->as<double>(), an.lu64->as<double>(), v, tol, max_iter, check_every);
-        res.sweeps = 1;
-    } else {
+    launch(c, "permute", [&] { permute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(rhs, an.perm->as<int>(), v.b, n); });
+    if (mixed) {
         if (!an.a32) {
             an.a32 = c.allocN<float>((size_t)an.nnz);
             an.lu32 = c.allocN<float>((size_t)an.nnz);
             an.vec32 = c.allocN<float>((size_t)10 * n);
         }
-        to_float_kernel<<<blocksFor(an.nnz), kThreads, 0, c.stream>>>(an.a64->as<double>(), an.a32->as<float>(),
-                                                                      an.nnz);
-        c.checkLaunch("to_float");
-        to_float_kernel<<<blocksFor(an.nnz), kThreads, 0, c.stream>>>(an.lu64->as<double>(), an.lu32->as<float>(),
-                                                                      an.nnz);
-        c.checkLaunch("to_float");
+        launch(c, "to_float", [&] { to_float_kernel<<<blocksFor(an.nnz), kThreads, 0, c.stream>>>(an.a64->as<double>(), an.a32->as<float>(), an.nnz); });
+        launch(c, "to_float", [&] { to_float_kernel<<<blocksFor(an.nnz), kThreads, 0, c.stream>>>(an.lu64->as<double>(), an.lu32->as<float>(), an.nnz); });
+    }
+    c.factor_clock.stop(c.stream);
+    int fstat = 0;
+    EQG_CUDA(cudaMemcpyAsync(c.pinned, an.factor_status->ptr, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    std::memcpy(&fstat, c.pinned, sizeof(int));
+    if (fstat) return res;  // zero pivot
+    c.krylov_clock.start(c.stream);
+
+    if (!mixed) {
+        res = bicgstab<double>(c, an, an.a64->as<double>(), an.lu64->as<double>(), v, tol, max_iter, check_every);
+        res.sweeps = 1;
+    } else {
         Vecs<float> w = vecs<float>(an.vec32->as<float>(), n);
         const double inner_tol = c.param_d("linsolver_inner_tolerance", 1e-4);
         const int max_sweeps = c.param_i("linsolver_max_sweeps", 60);
@@ -701,14 +691,10 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         const int nb = blocksFor(n, kThreads, kRedBlocks);
         // x = 0, r = b
         k_fill(c, v.x, 0.0, n);
-        double* dscal = reinterpret_cast<double*>(an.scal->as<KScal>()) ;
-        (void)dscal;
         Buf rr_dev = c.allocN<double>(2);
-        sumsq_kernel<<<nb, kThreads, 0, c.stream>>>(v.b, n, part, cnt, rr_dev->as<double>());
-        c.checkLaunch("sumsq");
-        residual_kernel<<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(), an.a64->as<double>(),
-                                                       v.x, v.b, v.r, w.b, n, part, cnt, rr_dev->as<double>() + 1);
-        c.checkLaunch("residual");
+        launch(c, "sumsq", [&] { sumsq_kernel<<<nb, kThreads, 0, c.stream>>>(v.b, n, part, cnt, rr_dev->as<double>()); });
+        launch(c, "residual", [&] { residual_kernel<<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(), an.a64->as<double>(),
+                                                       v.x, v.b, v.r, w.b, n, part, cnt, rr_dev->as<double>() + 1); });
         EQG_CUDA(cudaMemcpyAsync(c.pinned, rr_dev->ptr, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
         c.sync();
         const double bb = c.pinned[0];
@@ -720,12 +706,10 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
                                                 max_iter - total_iter, check_every);
             total_iter += inner.iterations;
             ++sweeps;
-            add_float_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, w.x, n);
-            c.checkLaunch("add_float");
-            residual_kernel<<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(),
+            launch(c, "add_float", [&] { add_float_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, w.x, n); });
+            launch(c, "residual", [&] { residual_kernel<<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(),
                                                            an.a64->as<double>(), v.x, v.b, v.r, w.b, n, part, cnt,
-                                                           rr_dev->as<double>() + 1);
-            c.checkLaunch("residual");
+                                                           rr_dev->as<double>() + 1); });
             EQG_CUDA(cudaMemcpyAsync(c.pinned, rr_dev->as<double>() + 1, sizeof(double), cudaMemcpyDeviceToHost,
                                      c.stream));
             c.sync();
@@ -738,8 +722,8 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         res.sweeps = sweeps;
         res.rel_residual = bb > 0 ? std::sqrt(rr / bb) : 0.0;
     }
-    unpermute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, an.perm->as<int>(), xout, n);
-    c.checkLaunch("unpermute");
+    c.krylov_clock.stop(c.stream);
+    launch(c, "unpermute", [&] { unpermute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, an.perm->as<int>(), xout, n); });
     return res;
 }
 

@@ -1,0 +1,83 @@
+// In-process entry point of a generated-style simulator built as a shared
+// library (compiled with -DEQUELLE_NO_MAIN next to the simulator source).
+//
+//   int eqg_sim_main(int argc, char** argv, eqg_sim_report* report)
+//
+// runs the program exactly as its main() would, then fills `report` with the
+// device-clock duration and counters of every Newton solve (from the
+// runtime's solve records) and the runtime's totals.  Returns 0, or 1 with the exception
+// text in report->error.
+#include "equelle/EquelleRuntimeCPU.hpp"
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+void equelleGeneratedCode(equelle::EquelleRuntimeCPU& er);
+
+extern "C" {
+
+struct eqg_sim_report {
+    int64_t solves;
+    double solve_ms[4096];      // duration of solve k
+    double gap_ms[4096];        // start of solve k to start of solve k+1
+    eqg_solve_info info[4096];  // counters of solve k
+    double total_ms;            // first solve start to last solve end
+    eqg_stats stats;
+    char error[512];
+};
+
+int eqg_sim_main(int argc, char** argv, eqg_sim_report* report)
+{
+    std::memset(report, 0, sizeof(*report));
+    const bool trace = std::getenv("EQG_SIM_TRACE") != nullptr;
+    auto note = [&](const char* what) {
+        if (trace) std::fprintf(stderr, "eqg_sim_main: %s\n", what), std::fflush(stderr);
+    };
+    try {
+        note("parameters");
+        Opm::ParameterGroup param(argc, argv, false);
+        note("runtime");
+        equelle::EquelleRuntimeCPU er(param);
+        eqg_runtime* rt = er.handle();
+        note("program");
+        try {
+            equelleGeneratedCode(er);
+        } catch (const std::exception& e) {
+            // keep the counters of a run that stopped early
+            std::strncpy(report->error, e.what(), sizeof(report->error) - 1);
+            eqg_runtime_stats(rt, &report->stats);
+            return 1;
+        }
+        note("report");
+        equelle::detail::check(eqg_runtime_synchronize(rt));
+        int64_t k = 0;
+        int first_start = -1, last_end = -1, prev_start = -1;
+        for (; k < 4096; ++k) {
+            int s = 0, e = 0;
+            if (eqg_runtime_solve_marks(rt, k, &s, &e) != EQG_OK) break;
+            double ms = 0.0;
+            equelle::detail::check(eqg_runtime_elapsed_ms(rt, s, e, &ms));
+            report->solve_ms[k] = ms;
+            equelle::detail::check(eqg_runtime_solve_info(rt, k, &report->info[k]));
+            if (prev_start >= 0) {
+                double g = 0.0;
+                equelle::detail::check(eqg_runtime_elapsed_ms(rt, prev_start, s, &g));
+                report->gap_ms[k - 1] = g;
+            }
+            if (first_start < 0) first_start = s;
+            last_end = e;
+            prev_start = s;
+        }
+        report->solves = k;
+        if (first_start >= 0) equelle::detail::check(eqg_runtime_elapsed_ms(rt, first_start, last_end, &report->total_ms));
+        equelle::detail::check(eqg_runtime_stats(rt, &report->stats));
+        note("done");
+        return 0;
+    } catch (const std::exception& e) {
+        std::strncpy(report->error, e.what(), sizeof(report->error) - 1);
+        return 1;
+    }
+}
+
+}  // extern "C"

@@ -84,6 +84,19 @@ typedef struct eqg_stats {
     int64_t device_bytes_in_use;
     int64_t device_bytes_peak;
     double last_linear_residual; /* relative residual of the last solve      */
+    int64_t last_matrix_rows;    /* size of the last linear system           */
+    int64_t last_matrix_nnz;
+    /* Device time of the kernel named by the runtime parameter time_kernel
+     * (CUDA events around each of its launches; 0 when unset). */
+    int64_t timed_kernel_launches;
+    double timed_kernel_ms;
+    /* Time in the Newton phases (device clock for the product, host clock
+     * for the oracle): residual callbacks, preconditioner set-up (value
+     * gather + ILU(0) factorization), Krylov iterations. */
+    int64_t residual_evaluations;
+    double residual_ms;
+    double factor_ms;
+    double krylov_ms;
 } eqg_stats;
 
 /* ---- errors and identity -------------------------------------------- */
@@ -95,8 +108,12 @@ const char* eqg_backend_name(void);
 /* Builds the grid and the helper operators from key=value parameters.
  * Keys read: grid_dim (2), nx (6), ny (1), nz (1), dx, dy, dz (1.0),
  * verbose (0), max_iter (10), abs_res_tol (1e-6),
- * linsolver_residual_tolerance (1e-8), linsolver_max_iterations (1000),
- * and the device-only keys documented in DESIGN.md.  grid_filename is
+ * linsolver_residual_tolerance (1e-8), linsolver_max_iterations (1000).
+ * The device library also reads linsolver_ordering (multicolor | natural),
+ * linsolver_precision (double | mixed), linsolver_inner_tolerance (1e-4),
+ * linsolver_max_sweeps (60), linsolver_check_every (8), time_kernel
+ * (name of one kernel to time with CUDA events) and device (CUDA device
+ * index; default: the calling thread's current device).  grid_filename is
  * rejected with EQG_ERR_UNSUPPORTED.
  * Replaces EquelleRuntimeCPU::EquelleRuntimeCPU(const ParameterGroup&)
  * and createGridManager (backends/serial/src/EquelleRuntimeCPU.cpp:20-65). */
@@ -114,6 +131,16 @@ int eqg_runtime_elapsed_ms(eqg_runtime* rt, int mark_a, int mark_b, double* ms);
 /* Newton-solve boundaries recorded automatically (one pair per solve):
  * start/end mark ids of solve k, or EQG_ERR_ARG if k is out of range. */
 int eqg_runtime_solve_marks(const eqg_runtime* rt, int64_t k, int* start_mark, int* end_mark);
+
+/* What solve k did. */
+typedef struct eqg_solve_info {
+    int start_mark, end_mark;
+    int newton_iterations;
+    int converged;              /* residual norm <= abs_res_tol at return   */
+    int64_t krylov_iterations;
+    int64_t kernel_launches;    /* device kernels launched during the solve */
+} eqg_solve_info;
+int eqg_runtime_solve_info(const eqg_runtime* rt, int64_t k, eqg_solve_info* out);
 
 /* ---- entity collections (CollOfCell / CollOfFace) -------------------- */
 /* allCells .. interiorFaces: EquelleRuntimeCPU.cpp:80-183.  The reference

@@ -39,6 +39,8 @@ public:
         : param_(param),
           output_to_file_(param.getDefault("output_to_file", false)),
           output_dir_(param.getDefault<std::string>("output_dir", "")),
+          output_values_(param.getDefault<std::string>("output_values", "all") == "all"),
+          output_last_(param.getDefault<std::string>("output_values", "all") == "last"),
           verbose_(param.getDefault("verbose", 0))
     {
         const auto items = param.items();
@@ -52,7 +54,11 @@ public:
     }
     EquelleRuntimeCPU(const EquelleRuntimeCPU&) = delete;
     EquelleRuntimeCPU& operator=(const EquelleRuntimeCPU&) = delete;
-    ~EquelleRuntimeCPU() { eqg_runtime_destroy(rt_); }
+    ~EquelleRuntimeCPU()
+    {
+        writeLastOutputs();
+        eqg_runtime_destroy(rt_);
+    }
 
     eqg_runtime* handle() const { return rt_; }
     const eqg_grid_info& gridInfo() const { return info_; }
@@ -228,10 +234,26 @@ public:
 
     /** @name Output (EquelleRuntimeCPU.cpp:449-482) */
     ///@{
-    void output(const String& tag, Scalar val) const { std::cout << tag << " = " << val << std::endl; }
+    void output(const String& tag, Scalar val) const
+    {
+        if (output_values_) {
+            std::cout << tag << " = " << val << std::endl;
+        }
+    }
+    /// Extensions for timing runs: output_values=none still copies each
+    /// collection to the host but neither prints nor writes it;
+    /// output_values=last keeps the last collection of each tag and writes
+    /// <output_dir><tag>-last.output (precision 17) when the runtime ends.
     void output(const String& tag, const CollOfScalar& vals)
     {
-        const std::vector<double> v = vals.value();
+        std::vector<double> v = vals.value();
+        if (output_last_) {
+            last_output_[tag] = std::move(v);
+            return;
+        }
+        if (!output_values_) {
+            return;
+        }
         if (output_to_file_) {
             int count = 0;
             auto it = outputcount_.find(tag);
@@ -320,6 +342,15 @@ public:
     }
 
 private:
+    void writeLastOutputs()
+    {
+        for (const auto& kv : last_output_) {
+            std::ofstream file((output_dir_ + kv.first + "-last.output").c_str());
+            file.precision(17);
+            std::copy(kv.second.begin(), kv.second.end(), std::ostream_iterator<double>(file, "\n"));
+        }
+    }
+
     template <class F>
     struct Trampoline {
         const F* f;
@@ -469,6 +500,9 @@ private:
     Opm::ParameterGroup param_;
     bool output_to_file_;
     std::string output_dir_;
+    bool output_values_;
+    bool output_last_;
+    std::map<std::string, std::vector<double>> last_output_;
     int verbose_;
     eqg_runtime* rt_ = nullptr;
     eqg_grid_info info_{};

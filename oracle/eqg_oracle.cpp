@@ -583,7 +583,13 @@ struct SolveReport {
     bool converged = false;
     int iterations = 0;
     double rel_residual = 0.0;
+    double factor_ms = 0.0, krylov_ms = 0.0;
 };
+
+double ms_since(std::chrono::steady_clock::time_point t0)
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
 
 // Solves A x = b from x = 0; converged when ||b - A x|| <= tol * ||b||.
 SolveReport bicgstab_ilu0(const Csr& a, const std::vector<double>& b, std::vector<double>& x, double tol,
@@ -598,7 +604,16 @@ SolveReport bicgstab_ilu0(const Csr& a, const std::vector<double>& b, std::vecto
         return rep;
     }
     Ilu0 prec;
-    if (!ilu0_factor(a, prec)) return rep;
+    const auto t0 = std::chrono::steady_clock::now();
+    const bool factored = ilu0_factor(a, prec);
+    rep.factor_ms = ms_since(t0);
+    if (!factored) return rep;
+    const auto t1 = std::chrono::steady_clock::now();
+    struct KrylovClock {
+        SolveReport& r;
+        std::chrono::steady_clock::time_point t;
+        ~KrylovClock() { r.krylov_ms = ms_since(t); }
+    } kclock{rep, t1};
     std::vector<double> r = b, rhat(n), p(n, 0.0), v(n, 0.0), s(n), t(n), ph(n), sh(n);
     for (int64_t i = 0; i < n; ++i) rhat[i] = shadow_entry(i);
     double rho = 1.0, alpha = 1.0, omega = 1.0;
@@ -658,7 +673,7 @@ struct eqg_runtime {
     int lin_max_iter = 1000;
     eqg_set* builtin[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     std::vector<std::chrono::steady_clock::time_point> marks;
-    std::vector<std::pair<int, int>> solve_marks;
+    std::vector<eqg_solve_info> solves;
     eqg_stats stats{};
 };
 
@@ -850,9 +865,18 @@ int eqg_runtime_solve_marks(const eqg_runtime* rt, int64_t k, int* s, int* e)
 {
     return guarded([&] {
         need(rt, "runtime");
-        if (k < 0 || k >= (int64_t)rt->solve_marks.size()) fail(EQG_ERR_ARG, "solve index out of range");
-        *s = rt->solve_marks[k].first;
-        *e = rt->solve_marks[k].second;
+        if (k < 0 || k >= (int64_t)rt->solves.size()) fail(EQG_ERR_ARG, "solve index out of range");
+        *s = rt->solves[k].start_mark;
+        *e = rt->solves[k].end_mark;
+    });
+}
+
+int eqg_runtime_solve_info(const eqg_runtime* rt, int64_t k, eqg_solve_info* out)
+{
+    return guarded([&] {
+        need(rt, "runtime");
+        if (k < 0 || k >= (int64_t)rt->solves.size()) fail(EQG_ERR_ARG, "solve index out of range");
+        *out = rt->solves[k];
     });
 }
 
@@ -1496,6 +1520,10 @@ int eqg_solve_for_update(eqg_runtime* rt, const eqg_coll* residual, eqg_coll** d
         rt->stats.linear_solves++;
         rt->stats.krylov_iterations += rep.iterations;
         rt->stats.last_linear_residual = rep.rel_residual;
+        rt->stats.factor_ms += rep.factor_ms;
+        rt->stats.krylov_ms += rep.krylov_ms;
+        rt->stats.last_matrix_rows = r.jac.rows;
+        rt->stats.last_matrix_nnz = r.jac.nnz();
         if (rt->verbose > 2)
             std::printf("        solveForUpdate: BiCGStab+ILU0 %d iterations, rel. residual %g\n", rep.iterations,
                         rep.rel_residual);
@@ -1513,11 +1541,19 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
         int m0 = 0;
         eqg_runtime_mark(rt, &m0);
         rt->stats.newton_solves++;
+        const int64_t krylov0 = rt->stats.krylov_iterations;
         eqg_coll* u = nullptr;
         if (eqg_variable(rt, u0, &u) != EQG_OK) fail(EQG_ERR_ARG, g_last_error);
         auto cleanup = [&](eqg_coll* a) { eqg_coll_release(a); };
         eqg_coll* res = nullptr;
-        if (fn(user, u, &res) != 0 || !res) {
+        auto evaluate = [&](eqg_coll* uu, eqg_coll** out) {
+            const auto t0 = std::chrono::steady_clock::now();
+            const int st = fn(user, uu, out);
+            rt->stats.residual_ms += ms_since(t0);
+            rt->stats.residual_evaluations++;
+            return st;
+        };
+        if (evaluate(u, &res) != 0 || !res) {
             cleanup(u);
             fail(EQG_ERR_CALLBACK, "residual callback failed");
         }
@@ -1540,7 +1576,7 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
             u = un;
             cleanup(res);
             res = nullptr;
-            if (fn(user, u, &res) != 0 || !res) {
+            if (evaluate(u, &res) != 0 || !res) {
                 cleanup(u);
                 fail(EQG_ERR_CALLBACK, "residual callback failed");
             }
@@ -1556,12 +1592,16 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
             else
                 std::printf("Newton solver converged in %d iterations\n", iter);
         }
+        eqg_solve_info info{};
+        info.start_mark = m0;
+        info.newton_iterations = iter;
+        info.converged = norm(res) <= rt->abs_res_tol ? 1 : 0;
+        info.krylov_iterations = rt->stats.krylov_iterations - krylov0;
         *out = make_coll(adb_constant(u->a.v));
         cleanup(u);
         cleanup(res);
-        int m1 = 0;
-        eqg_runtime_mark(rt, &m1);
-        rt->solve_marks.emplace_back(m0, m1);
+        eqg_runtime_mark(rt, &info.end_mark);
+        rt->solves.push_back(info);
     });
 }
 
