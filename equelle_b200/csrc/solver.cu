@@ -19,7 +19,12 @@
 // The analysis (ordering, permuted pattern, value map) is computed on the
 // host once per Jacobian pattern and cached with it.
 //
-// Precision "mixed": the inner BiCGStab and the ILU(0) factors run in FP32,
+// Preconditioner "multigrid" (default; see the analysis section below):
+// geometric-aggregation V-cycle with these ILU(0) sweeps as smoothers, which
+// keeps the iteration count of the elliptic pressure part from growing with
+// the grid; "ilu0": the staged ILU(0) alone.
+//
+// Precision "mixed": the inner BiCGStab and the preconditioner run in FP32,
 // inside FP64 iterative refinement (r = b - A x in FP64 with FP64 A).
 //
 // Every kernel of an iteration reads a device-side status word first and
@@ -409,68 +414,209 @@ __global__ void sumsq_kernel(const double* __restrict__ a, int n, double* partia
     }
 }
 
+// ---- multilevel preconditioner kernels -------------------------------------
+// Coarse-level values: each coarse entry is the sum of the finer level's
+// entries that aggregate onto it (Galerkin product R A R^T with a 0/1
+// aggregation R), gathered in a fixed order.
+__global__ void galerkin_kernel(int64_t nnz_c, const int* __restrict__ gptr, const int* __restrict__ gidx,
+                                const double* __restrict__ fine, double* __restrict__ coarse)
+{
+    GRID_STRIDE(c, nnz_c)
+    {
+        double s = 0.0;
+        const int k1 = gptr[c + 1];
+        for (int k = gptr[c]; k < k1; ++k) s += fine[gidx[k]];
+        coarse[c] = s;
+    }
+}
+
+__device__ __forceinline__ bool mg_skip(const KScal* sc, int skip_if_s)
+{
+    return stopped(sc) || (skip_if_s && sc->s_conv);
+}
+
+// out = b - A x
+template <class T>
+__global__ void mg_residual_kernel(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
+                                   const T* __restrict__ a, const T* __restrict__ x, const T* __restrict__ b,
+                                   T* __restrict__ out, const KScal* sc, int skip_if_s)
+{
+    if (mg_skip(sc, skip_if_s)) return;
+    GRID_STRIDE(i, n) out[i] = (T)((double)b[i] - row_dot<T>((int)i, rowptr, col, a, x));
+}
+
+// rc[P] = sum of t over the members of aggregate P
+template <class T>
+__global__ void mg_restrict_kernel(int nc, const int* __restrict__ mptr, const int* __restrict__ midx,
+                                   const T* __restrict__ t, T* __restrict__ rc, const KScal* sc, int skip_if_s)
+{
+    if (mg_skip(sc, skip_if_s)) return;
+    GRID_STRIDE(P, nc)
+    {
+        double s = 0.0;
+        const int k1 = mptr[P + 1];
+        for (int k = mptr[P]; k < k1; ++k) s += (double)t[midx[k]];
+        rc[P] = (T)s;
+    }
+}
+
+// z[i] += ec[agg[i]] (piecewise-constant prolongation)
+template <class T>
+__global__ void mg_prolong_kernel(int n, const int* __restrict__ agg, const T* __restrict__ ec, T* __restrict__ z,
+                                  const KScal* sc, int skip_if_s)
+{
+    if (mg_skip(sc, skip_if_s)) return;
+    GRID_STRIDE(i, n) z[i] = (T)((double)z[i] + (double)ec[agg[i]]);
+}
+
+template <class T>
+__global__ void mg_add_kernel(int n, const T* __restrict__ w, T* __restrict__ z, const KScal* sc, int skip_if_s)
+{
+    if (mg_skip(sc, skip_if_s)) return;
+    GRID_STRIDE(i, n) z[i] = (T)((double)z[i] + (double)w[i]);
+}
+
+// Inverse of the coarsest matrix (n <= kCoarsest) by Gauss-Jordan with
+// partial pivoting on [A | I], one block.
+constexpr int kCoarsest = 128;
+
+__global__ void dense_inverse_kernel(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
+                                     const double* __restrict__ a, double* __restrict__ work,
+                                     double* __restrict__ inv, int* status)
+{
+    __shared__ double factor[kCoarsest];
+    __shared__ int piv;
+    __shared__ double pval;
+    const int w2 = 2 * n;
+    for (int idx = threadIdx.x; idx < n * w2; idx += blockDim.x) work[idx] = 0.0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) work[i * w2 + col[e]] = a[e];
+        work[i * w2 + n + i] = 1.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        if (threadIdx.x == 0) {
+            int best = k;
+            double bv = fabs(work[k * w2 + k]);
+            for (int r = k + 1; r < n; ++r) {
+                const double v = fabs(work[r * w2 + k]);
+                if (v > bv) {
+                    bv = v;
+                    best = r;
+                }
+            }
+            piv = best;
+            if (bv == 0.0) *status = 1;
+        }
+        __syncthreads();
+        if (piv != k)
+            for (int j = threadIdx.x; j < w2; j += blockDim.x) {
+                const double t = work[k * w2 + j];
+                work[k * w2 + j] = work[piv * w2 + j];
+                work[piv * w2 + j] = t;
+            }
+        __syncthreads();
+        if (threadIdx.x == 0) pval = work[k * w2 + k];
+        __syncthreads();
+        for (int j = threadIdx.x; j < w2; j += blockDim.x) work[k * w2 + j] /= pval;
+        __syncthreads();
+        for (int r = threadIdx.x; r < n; r += blockDim.x) factor[r] = work[r * w2 + k];
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < n * w2; idx += blockDim.x) {
+            const int r = idx / w2, j = idx - r * w2;
+            if (r != k) work[idx] -= factor[r] * work[k * w2 + j];
+        }
+        __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int r = idx / n, j = idx - r * n;
+        inv[idx] = work[r * w2 + n + j];
+    }
+}
+
+template <class T>
+__global__ void dense_apply_kernel(int n, const T* __restrict__ inv, const T* __restrict__ r, T* __restrict__ z,
+                                   const KScal* sc, int skip_if_s)
+{
+    if (mg_skip(sc, skip_if_s)) return;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double s = 0.0;
+        for (int j = 0; j < n; ++j) s += (double)inv[i * n + j] * (double)r[j];
+        z[i] = (T)s;
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
 // Host analysis, cached per Jacobian pattern.
+//
+// Multilevel preconditioner (the default when the system is laid out as
+// `ncomp` blocks of one unknown per grid cell, as newtonSolve and
+// newtonSolveSystem stack them): geometric aggregation of 2x2x2 cells per
+// unknown block, Galerkin coarse matrices R A R^T, a V(1,1) cycle with one
+// ILU(0) sweep before and after the coarse correction on every level, and a
+// dense inverse on the coarsest level (<= 128 unknowns).  Otherwise plain
+// ILU(0).
 // ---------------------------------------------------------------------------
+struct HostCsr {
+    int n = 0;
+    std::vector<int> ptr, col;
+};
+
+struct Level {
+    int n = 0;
+    int64_t nnz = 0;
+    int cx = 1, cy = 1, cz = 1;    // cells of this level's grid
+    bool coarsest = false;
+    std::vector<int> stage_ptr;    // stages (colours or wavefronts) in the permuted order
+    Buf perm, rowptr, col, diag;   // permuted pattern
+    Buf gptr, gidx;                // Galerkin gather from the finer level (levels > 0)
+    Buf agg, mptr, midx;           // to the next coarser level
+    Buf a64, lu64, a32, lu32;
+    Buf v64, v32;                  // 4 work vectors: r, z, t, w
+    Buf work64, inv64, inv32;      // coarsest level
+};
+
 struct SolverAnalysis {
     int n = 0;
     int64_t nnz = 0;
     bool natural = false;
-    bool ok = true;                 // every row has a diagonal entry
-    std::vector<int> stage_ptr;     // stage boundaries in the new order
-    Buf perm, rowptr, col, vmap, diag;
-    // workspaces
-    Buf a64, lu64, a32, lu32;
-    Buf vec64;   // 10 double vectors
-    Buf vec32;   // 9 float vectors
-    Buf scal;    // KScal
-    Buf partials, counter, factor_status;
+    bool ok = true;  // every row has a diagonal entry
+    bool multigrid = false;
+    std::vector<Level> levels;
+    Buf vmap;        // level-0 permuted entry <- Jacobian entry
+    Buf vec64, vec32, scal, partials, counter, factor_status;
 };
 
 namespace {
 
-std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
+// Stage key of every row: wavefront level of the natural order, or greedy
+// colour, over the symmetrised pattern.
+std::vector<int> stage_keys(const HostCsr& A, bool natural)
 {
-    auto an = std::make_shared<SolverAnalysis>();
-    const int n = p.rows;
-    an->n = n;
-    an->nnz = p.nnz;
-    an->natural = natural;
-    std::vector<int> rp(n + 1), ci(p.nnz > 0 ? p.nnz : 1);
-    EQG_CUDA(cudaMemcpyAsync(rp.data(), p.rowptr->ptr, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, c.stream));
-    if (p.nnz > 0)
-        EQG_CUDA(cudaMemcpyAsync(ci.data(), p.colind->ptr, (size_t)p.nnz * 4, cudaMemcpyDeviceToHost, c.stream));
-    c.sync();
-    // symmetrised adjacency (without the diagonal)
-    std::vector<int> tp(n + 1, 0);
-    for (int64_t e = 0; e < p.nnz; ++e) tp[ci[e] + 1]++;
+    const int n = A.n;
+    const int64_t nnz = A.ptr[n];
+    std::vector<int> tp(n + 1, 0), tr(nnz > 0 ? nnz : 1);
+    for (int64_t e = 0; e < nnz; ++e) tp[A.col[e] + 1]++;
     for (int i = 0; i < n; ++i) tp[i + 1] += tp[i];
-    std::vector<int> tr(p.nnz > 0 ? p.nnz : 1);
     {
         std::vector<int> pos(tp.begin(), tp.end() - 1);
         for (int i = 0; i < n; ++i)
-            for (int e = rp[i]; e < rp[i + 1]; ++e) tr[pos[ci[e]]++] = i;
-    }
-    for (int i = 0; i < n; ++i) {
-        bool has = false;
-        for (int e = rp[i]; e < rp[i + 1]; ++e) has |= (ci[e] == i);
-        if (!has) an->ok = false;
+            for (int e = A.ptr[i]; e < A.ptr[i + 1]; ++e) tr[pos[A.col[e]]++] = i;
     }
     std::vector<int> key(n, 0);
     if (natural) {
-        // wavefront level over the earlier neighbours
         for (int i = 0; i < n; ++i) {
             int lv = 0;
-            for (int e = rp[i]; e < rp[i + 1]; ++e)
-                if (ci[e] < i) lv = std::max(lv, key[ci[e]] + 1);
+            for (int e = A.ptr[i]; e < A.ptr[i + 1]; ++e)
+                if (A.col[e] < i) lv = std::max(lv, key[A.col[e]] + 1);
             for (int e = tp[i]; e < tp[i + 1]; ++e)
                 if (tr[e] < i) lv = std::max(lv, key[tr[e]] + 1);
             key[i] = lv;
         }
     } else {
-        // greedy colouring in natural order
         std::vector<int> mark(64, -1);
         for (int i = 0; i < n; ++i) {
             auto see = [&](int j) {
@@ -480,56 +626,214 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
                     mark[cj] = i;
                 }
             };
-            for (int e = rp[i]; e < rp[i + 1]; ++e) see(ci[e]);
+            for (int e = A.ptr[i]; e < A.ptr[i + 1]; ++e) see(A.col[e]);
             for (int e = tp[i]; e < tp[i + 1]; ++e) see(tr[e]);
-            int col = 0;
-            while (col < (int)mark.size() && mark[col] == i) ++col;
-            key[i] = col;
+            int cc = 0;
+            while (cc < (int)mark.size() && mark[cc] == i) ++cc;
+            key[i] = cc;
         }
     }
-    const int nstages = n > 0 ? *std::max_element(key.begin(), key.end()) + 1 : 0;
-    an->stage_ptr.assign(nstages + 1, 0);
-    for (int i = 0; i < n; ++i) an->stage_ptr[key[i] + 1]++;
-    for (int s = 0; s < nstages; ++s) an->stage_ptr[s + 1] += an->stage_ptr[s];
-    std::vector<int> perm(n), iperm(n);
+    return key;
+}
+
+Buf upload_ints(Core& c, const std::vector<int>& v)
+{
+    Buf b = c.allocN<int>(v.empty() ? 1 : v.size());
+    if (!v.empty()) EQG_CUDA(cudaMemcpyAsync(b->ptr, v.data(), v.size() * 4, cudaMemcpyHostToDevice, c.stream));
+    return b;
+}
+
+// Orders the rows of `A` by stage, builds the permuted pattern with
+// ascending columns, and returns the host permutation (new -> old), its
+// inverse and, for every permuted entry, its entry index in `A`.
+void order_level(Core& c, const HostCsr& A, bool natural, Level& L, std::vector<int>& perm, std::vector<int>& iperm,
+                 std::vector<int>& pcsr_ptr, std::vector<int>& pcsr_col, std::vector<int>& emap, bool& ok)
+{
+    const int n = A.n;
+    const int64_t nnz = A.ptr[n];
+    const std::vector<int> key = stage_keys(A, natural);
+    const int nst = n > 0 ? *std::max_element(key.begin(), key.end()) + 1 : 0;
+    L.stage_ptr.assign(nst + 1, 0);
+    for (int i = 0; i < n; ++i) L.stage_ptr[key[i] + 1]++;
+    for (int s = 0; s < nst; ++s) L.stage_ptr[s + 1] += L.stage_ptr[s];
+    perm.assign(n, 0);
+    iperm.assign(n, 0);
     {
-        std::vector<int> pos(an->stage_ptr.begin(), an->stage_ptr.end() - 1);
-        for (int i = 0; i < n; ++i) perm[pos[key[i]]++] = i;  // stable within a stage
+        std::vector<int> pos(L.stage_ptr.begin(), L.stage_ptr.end() - 1);
+        for (int i = 0; i < n; ++i) perm[pos[key[i]]++] = i;
     }
     for (int r = 0; r < n; ++r) iperm[perm[r]] = r;
-    // permuted pattern with ascending new columns
-    std::vector<int> nrp(n + 1, 0), ncol(p.nnz > 0 ? p.nnz : 1), vmap(p.nnz > 0 ? p.nnz : 1), diag(n, -1);
+    pcsr_ptr.assign(n + 1, 0);
+    pcsr_col.assign(nnz > 0 ? nnz : 1, 0);
+    emap.assign(nnz > 0 ? nnz : 1, 0);
+    std::vector<int> diag(n, 0);
     std::vector<std::pair<int, int>> row;
     for (int r = 0; r < n; ++r) {
         const int i = perm[r];
         row.clear();
-        for (int e = rp[i]; e < rp[i + 1]; ++e) row.emplace_back(iperm[ci[e]], e);
+        for (int e = A.ptr[i]; e < A.ptr[i + 1]; ++e) row.emplace_back(iperm[A.col[e]], e);
         std::sort(row.begin(), row.end());
-        nrp[r + 1] = nrp[r] + (int)row.size();
-        int o = nrp[r];
+        pcsr_ptr[r + 1] = pcsr_ptr[r] + (int)row.size();
+        int o = pcsr_ptr[r];
+        bool has = false;
         for (auto& ce : row) {
-            if (ce.first == r) diag[r] = o;
-            ncol[o] = ce.first;
-            vmap[o] = ce.second;
+            if (ce.first == r) {
+                diag[r] = o;
+                has = true;
+            }
+            pcsr_col[o] = ce.first;
+            emap[o] = ce.second;
             ++o;
         }
+        if (!has) ok = false;
     }
-    auto up = [&](const std::vector<int>& v) {
-        Buf b = c.allocN<int>(v.size());
-        EQG_CUDA(cudaMemcpyAsync(b->ptr, v.data(), v.size() * 4, cudaMemcpyHostToDevice, c.stream));
-        return b;
-    };
-    an->perm = up(perm);
-    an->rowptr = up(nrp);
-    an->col = up(ncol);
-    an->vmap = up(vmap);
-    std::vector<int> diag_safe(diag);
-    for (auto& d : diag_safe)
-        if (d < 0) d = 0;
-    an->diag = up(diag_safe);
-    const size_t nz = (size_t)(p.nnz > 0 ? p.nnz : 1);
-    an->a64 = c.allocN<double>(nz);
-    an->lu64 = c.allocN<double>(nz);
+    L.n = n;
+    L.nnz = nnz;
+    L.perm = upload_ints(c, perm);
+    L.rowptr = upload_ints(c, pcsr_ptr);
+    L.col = upload_ints(c, pcsr_col);
+    L.diag = upload_ints(c, diag);
+    const size_t nz = (size_t)(nnz > 0 ? nnz : 1);
+    L.a64 = c.allocN<double>(nz);
+    L.lu64 = c.allocN<double>(nz);
+    L.v64 = c.allocN<double>((size_t)4 * (n > 0 ? n : 1));
+}
+
+std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
+{
+    auto an = std::make_shared<SolverAnalysis>();
+    const int n = p.rows;
+    an->n = n;
+    an->nnz = p.nnz;
+    an->natural = natural;
+    HostCsr A;
+    A.n = n;
+    A.ptr.resize(n + 1);
+    A.col.resize(p.nnz > 0 ? p.nnz : 1);
+    EQG_CUDA(cudaMemcpyAsync(A.ptr.data(), p.rowptr->ptr, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, c.stream));
+    if (p.nnz > 0)
+        EQG_CUDA(cudaMemcpyAsync(A.col.data(), p.colind->ptr, (size_t)p.nnz * 4, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+
+    std::vector<int> perm, iperm, pptr, pcol, emap;
+    an->levels.emplace_back();
+    order_level(c, A, natural, an->levels[0], perm, iperm, pptr, pcol, emap, an->ok);
+    an->vmap = upload_ints(c, emap);
+
+    const std::string pre = c.param_s("linsolver_preconditioner", "multigrid");
+    if (pre != "multigrid" && pre != "ilu0") fail(EQG_ERR_ARG, "linsolver_preconditioner must be multigrid or ilu0");
+    const int ncomp = (c.nc > 0 && n % c.nc == 0) ? n / c.nc : 0;
+    an->multigrid = pre == "multigrid" && ncomp >= 1 && ncomp <= 8 && n > kCoarsest && an->ok;
+    an->levels[0].cx = c.nx;
+    an->levels[0].cy = c.ny;
+    an->levels[0].cz = c.nz;
+    if (an->multigrid) {
+        // the finer level in its natural ordering, with its permutation
+        HostCsr fine = A;
+        std::vector<int> fperm = perm, fiperm = iperm, fptr = pptr, fcol = pcol;
+        for (;;) {
+            Level& F = an->levels.back();
+            const int fcx = F.cx, fcy = F.cy, fcz = F.cz;
+            const int fcells = fcx * fcy * fcz;
+            const int ccx = (fcx + 1) / 2, ccy = (fcy + 1) / 2, ccz = fcz > 1 ? (fcz + 1) / 2 : 1;
+            const int ccells = ccx * ccy * ccz;
+            const int nc_unk = ncomp * ccells;
+            // aggregate of every fine unknown (natural indices)
+            std::vector<int> agg_nat(fine.n);
+            for (int u = 0; u < fine.n; ++u) {
+                const int comp = u / fcells, cell = u - comp * fcells;
+                const int i = cell % fcx, j = (cell / fcx) % fcy, k = cell / (fcx * fcy);
+                agg_nat[u] = comp * ccells + (i / 2) + ccx * ((j / 2) + ccy * (fcz > 1 ? k / 2 : 0));
+            }
+            // coarse pattern (natural ordering)
+            HostCsr C;
+            C.n = nc_unk;
+            {
+                std::vector<std::vector<int>> rows(nc_unk);
+                std::vector<int> mark(nc_unk, -1);
+                std::vector<std::vector<int>> members(nc_unk);
+                for (int u = 0; u < fine.n; ++u) members[agg_nat[u]].push_back(u);
+                C.ptr.assign(nc_unk + 1, 0);
+                std::vector<int> cols;
+                for (int U = 0; U < nc_unk; ++U) {
+                    for (int u : members[U])
+                        for (int e = fine.ptr[u]; e < fine.ptr[u + 1]; ++e) {
+                            const int V = agg_nat[fine.col[e]];
+                            if (mark[V] != U) {
+                                mark[V] = U;
+                                rows[U].push_back(V);
+                            }
+                        }
+                    std::sort(rows[U].begin(), rows[U].end());
+                    C.ptr[U + 1] = C.ptr[U] + (int)rows[U].size();
+                }
+                C.col.resize(C.ptr[nc_unk] > 0 ? C.ptr[nc_unk] : 1);
+                for (int U = 0; U < nc_unk; ++U) std::copy(rows[U].begin(), rows[U].end(), C.col.begin() + C.ptr[U]);
+            }
+            an->levels.emplace_back();
+            Level& Lc = an->levels.back();
+            Level& Lf = an->levels[an->levels.size() - 2];
+            Lc.cx = ccx;
+            Lc.cy = ccy;
+            Lc.cz = ccz;
+            std::vector<int> cperm, ciperm, cptr, ccol, cemap;
+            bool cok = true;
+            order_level(c, C, natural, Lc, cperm, ciperm, cptr, ccol, cemap, cok);
+            if (!cok) fail(EQG_ERR_DEVICE, "coarse level without a diagonal entry");
+            // aggregation in permuted indices, and aggregate members
+            std::vector<int> aggp(fine.n);
+            for (int pf = 0; pf < fine.n; ++pf) aggp[pf] = ciperm[agg_nat[fperm[pf]]];
+            std::vector<int> mptr(nc_unk + 1, 0), midx(fine.n);
+            for (int pf = 0; pf < fine.n; ++pf) mptr[aggp[pf] + 1]++;
+            for (int P = 0; P < nc_unk; ++P) mptr[P + 1] += mptr[P];
+            {
+                std::vector<int> pos(mptr.begin(), mptr.end() - 1);
+                for (int pf = 0; pf < fine.n; ++pf) midx[pos[aggp[pf]]++] = pf;
+            }
+            Lf.agg = upload_ints(c, aggp);
+            Lf.mptr = upload_ints(c, mptr);
+            Lf.midx = upload_ints(c, midx);
+            // Galerkin gather: coarse permuted entry <- fine permuted entries
+            const int64_t fnnz = fptr[fine.n];
+            std::vector<int> target(fnnz > 0 ? fnnz : 1);
+            for (int pf = 0; pf < fine.n; ++pf) {
+                const int P = aggp[pf];
+                for (int e = fptr[pf]; e < fptr[pf + 1]; ++e) {
+                    const int Q = aggp[fcol[e]];
+                    const int* lo = ccol.data() + cptr[P];
+                    const int* hi = ccol.data() + cptr[P + 1];
+                    const int* q = std::lower_bound(lo, hi, Q);
+                    target[e] = (int)(q - ccol.data());
+                }
+            }
+            const int64_t cnnz = cptr[nc_unk];
+            std::vector<int> gptr(cnnz + 1, 0), gidx(fnnz > 0 ? fnnz : 1);
+            for (int64_t e = 0; e < fnnz; ++e) gptr[target[e] + 1]++;
+            for (int64_t k = 0; k < cnnz; ++k) gptr[k + 1] += gptr[k];
+            {
+                std::vector<int> pos(gptr.begin(), gptr.end() - 1);
+                for (int64_t e = 0; e < fnnz; ++e) gidx[pos[target[e]]++] = (int)e;
+            }
+            Lc.gptr = upload_ints(c, gptr);
+            Lc.gidx = upload_ints(c, gidx);
+            if (nc_unk <= kCoarsest || (ccx == 1 && ccy == 1 && ccz == 1)) {
+                if (nc_unk > kCoarsest) {
+                    an->multigrid = false;  // cannot coarsen further and too large to invert
+                    an->levels.resize(1);
+                    break;
+                }
+                Lc.coarsest = true;
+                Lc.work64 = c.allocN<double>((size_t)2 * nc_unk * nc_unk);
+                Lc.inv64 = c.allocN<double>((size_t)nc_unk * nc_unk);
+                break;
+            }
+            fine = std::move(C);
+            fperm = std::move(cperm);
+            fiperm = std::move(ciperm);
+            fptr = std::move(cptr);
+            fcol = std::move(ccol);
+        }
+    }
     an->vec64 = c.allocN<double>((size_t)10 * (n > 0 ? n : 1));
     an->scal = c.alloc(sizeof(KScal));
     an->partials = c.allocN<double>((size_t)kRedBlocks * 2);
@@ -537,6 +841,11 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     an->factor_status = c.allocN<int>(1);
     EQG_CUDA(cudaMemsetAsync(an->counter->ptr, 0, sizeof(unsigned int), c.stream));
     c.sync();
+    if (c.verbose > 2 && an->multigrid) {
+        std::printf("        multigrid levels:");
+        for (auto& L : an->levels) std::printf(" %d(%zu stages)", L.n, L.stage_ptr.size() - 1);
+        std::printf("\n");
+    }
     return an;
 }
 
@@ -565,55 +874,139 @@ Vecs<T> vecs(T* base, int n)
 }
 
 template <class T>
-void precondition(Core& c, const SolverAnalysis& an, const T* lu, const T* in, T* out, const KScal* sc, int skip_if_s)
+const T* level_a(const Level& L);
+template <>
+const double* level_a<double>(const Level& L) { return L.a64->as<double>(); }
+template <>
+const float* level_a<float>(const Level& L) { return L.a32->as<float>(); }
+template <class T>
+const T* level_lu(const Level& L);
+template <>
+const double* level_lu<double>(const Level& L) { return L.lu64->as<double>(); }
+template <>
+const float* level_lu<float>(const Level& L) { return L.lu32->as<float>(); }
+template <class T>
+T* level_vec(const Level& L, int k);
+template <>
+double* level_vec<double>(const Level& L, int k) { return L.v64->as<double>() + (size_t)k * (L.n > 0 ? L.n : 1); }
+template <>
+float* level_vec<float>(const Level& L, int k) { return L.v32->as<float>() + (size_t)k * (L.n > 0 ? L.n : 1); }
+template <class T>
+const T* level_inv(const Level& L);
+template <>
+const double* level_inv<double>(const Level& L) { return L.inv64->as<double>(); }
+template <>
+const float* level_inv<float>(const Level& L) { return L.inv32->as<float>(); }
+
+// out = M^{-1} in for the ILU(0) factors of one level.
+template <class T>
+void ilu_apply(Core& c, const Level& L, const T* in, T* out, const KScal* sc, int skip_if_s)
 {
-    const int ns = (int)an.stage_ptr.size() - 1;
+    const T* lu = level_lu<T>(L);
+    const int ns = (int)L.stage_ptr.size() - 1;
     for (int s = 0; s < ns; ++s) {
-        const int r0 = an.stage_ptr[s], r1 = an.stage_ptr[s + 1];
-        launch(c, "ilu0_lower", [&] { ilu0_lower_stage_kernel<T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
-            r0, r1, an.rowptr->as<int>(), an.col->as<int>(), an.diag->as<int>(), lu, in, out, sc, skip_if_s); });
+        const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
+        launch(c, "ilu0_lower", [&] {
+            ilu0_lower_stage_kernel<T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
+                r0, r1, L.rowptr->as<int>(), L.col->as<int>(), L.diag->as<int>(), lu, in, out, sc, skip_if_s);
+        });
     }
     for (int s = ns - 1; s >= 0; --s) {
-        const int r0 = an.stage_ptr[s], r1 = an.stage_ptr[s + 1];
-        launch(c, "ilu0_upper", [&] { ilu0_upper_stage_kernel<T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
-            r0, r1, an.rowptr->as<int>(), an.col->as<int>(), an.diag->as<int>(), lu, out, sc, skip_if_s); });
+        const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
+        launch(c, "ilu0_upper", [&] {
+            ilu0_upper_stage_kernel<T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
+                r0, r1, L.rowptr->as<int>(), L.col->as<int>(), L.diag->as<int>(), lu, out, sc, skip_if_s);
+        });
     }
 }
 
-// BiCGStab on the permuted system with values a and factors lu; v.b holds the
-// right-hand side.  Returns (converged, iterations, rr/bb).
+// z = V-cycle(r) on level l.
 template <class T>
-SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, const T* lu, Vecs<T> v, double tol, int max_iter,
-                     int check_every)
+void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const KScal* sc, int skip)
+{
+    const Level& L = an.levels[l];
+    const int n = L.n;
+    if (L.coarsest) {
+        launch(c, "mg_dense_apply",
+               [&] { dense_apply_kernel<T><<<1, kThreads, 0, c.stream>>>(n, level_inv<T>(L), r, z, sc, skip); });
+        return;
+    }
+    const Level& C = an.levels[l + 1];
+    T* t = level_vec<T>(L, 2);
+    T* w = level_vec<T>(L, 3);
+    T* rc = level_vec<T>(C, 0);
+    T* zc = level_vec<T>(C, 1);
+    const T* a = level_a<T>(L);
+    ilu_apply<T>(c, L, r, z, sc, skip);
+    launch(c, "mg_residual", [&] {
+        mg_residual_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.rowptr->as<int>(), L.col->as<int>(), a, z,
+                                                                        r, t, sc, skip);
+    });
+    launch(c, "mg_restrict", [&] {
+        mg_restrict_kernel<T><<<blocksFor(C.n), kThreads, 0, c.stream>>>(C.n, L.mptr->as<int>(), L.midx->as<int>(), t,
+                                                                          rc, sc, skip);
+    });
+    vcycle<T>(c, an, l + 1, rc, zc, sc, skip);
+    launch(c, "mg_prolong", [&] {
+        mg_prolong_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.agg->as<int>(), zc, z, sc, skip);
+    });
+    launch(c, "mg_residual", [&] {
+        mg_residual_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.rowptr->as<int>(), L.col->as<int>(), a, z,
+                                                                        r, t, sc, skip);
+    });
+    ilu_apply<T>(c, L, t, w, sc, skip);
+    launch(c, "mg_add", [&] { mg_add_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, w, z, sc, skip); });
+}
+
+template <class T>
+void precondition(Core& c, const SolverAnalysis& an, const T* in, T* out, const KScal* sc, int skip_if_s)
+{
+    if (an.multigrid) vcycle<T>(c, an, 0, in, out, sc, skip_if_s);
+    else ilu_apply<T>(c, an.levels[0], in, out, sc, skip_if_s);
+}
+
+// BiCGStab on the permuted system with values a; v.b holds the right-hand
+// side.
+template <class T>
+SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double tol, int max_iter, int check_every)
 {
     const int n = an.n;
+    const Level& L0 = an.levels[0];
     KScal* sc = an.scal->as<KScal>();
     double* part = an.partials->as<double>();
     unsigned int* cnt = an.counter->as<unsigned int>();
     const int nb = blocksFor(n, kThreads, kRedBlocks);
-    launch(c, "bicg_init", [&] { bicg_init_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.b, v.r, v.rhat, v.p, v.v, v.x, n, part, cnt, sc, tol * tol); });
+    launch(c, "bicg_init", [&] {
+        bicg_init_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.b, v.r, v.rhat, v.p, v.v, v.x, n, part, cnt, sc, tol * tol);
+    });
     SolveResult res;
     KScal h{};
-    double bb = 0.0;
     int enq = 0;
     for (;;) {
         const int chunk = std::min(check_every, max_iter - enq);
         for (int k = 0; k < chunk; ++k) {
             launch(c, "bicg_p", [&] { bicg_p_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(v.r, v.v, v.p, n, sc); });
-            precondition<T>(c, an, lu, v.p, v.ph, sc, 0);
-            launch(c, "bicg_spmv_alpha", [&] { bicg_spmv_alpha_kernel<T><<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(), a, v.ph,
-                                                                    v.rhat, v.v, n, part, cnt, sc); });
-            launch(c, "bicg_s", [&] { bicg_s_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.r, v.v, v.s, n, part, cnt, sc); });
-            precondition<T>(c, an, lu, v.s, v.sh, sc, 1);
-            launch(c, "bicg_spmv_omega", [&] { bicg_spmv_omega_kernel<T><<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(), a, v.sh,
-                                                                    v.s, v.t, n, part, cnt, sc); });
-            launch(c, "bicg_xr", [&] { bicg_xr_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.ph, v.sh, v.s, v.t, v.rhat, v.x, v.r, n, part, cnt, sc); });
+            precondition<T>(c, an, v.p, v.ph, sc, 0);
+            launch(c, "bicg_spmv_alpha", [&] {
+                bicg_spmv_alpha_kernel<T><<<nb, kThreads, 0, c.stream>>>(L0.rowptr->as<int>(), L0.col->as<int>(), a,
+                                                                        v.ph, v.rhat, v.v, n, part, cnt, sc);
+            });
+            launch(c, "bicg_s",
+                   [&] { bicg_s_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.r, v.v, v.s, n, part, cnt, sc); });
+            precondition<T>(c, an, v.s, v.sh, sc, 1);
+            launch(c, "bicg_spmv_omega", [&] {
+                bicg_spmv_omega_kernel<T><<<nb, kThreads, 0, c.stream>>>(L0.rowptr->as<int>(), L0.col->as<int>(), a,
+                                                                        v.sh, v.s, v.t, n, part, cnt, sc);
+            });
+            launch(c, "bicg_xr", [&] {
+                bicg_xr_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.ph, v.sh, v.s, v.t, v.rhat, v.x, v.r, n, part, cnt,
+                                                                sc);
+            });
         }
         enq += chunk;
         EQG_CUDA(cudaMemcpyAsync(c.pinned, sc, sizeof(KScal), cudaMemcpyDeviceToHost, c.stream));
         c.sync();
         std::memcpy(&h, c.pinned, sizeof(KScal));
-        if (bb == 0.0) bb = h.thr / (tol * tol > 0 ? tol * tol : 1.0);
         if (h.status != ST_RUN || enq >= max_iter) break;
     }
     res.converged = h.status == ST_CONV;
@@ -621,6 +1014,26 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, const T* lu, Vecs<
     const double b2 = tol > 0 ? h.thr / (tol * tol) : 0.0;
     res.rel_residual = b2 > 0 ? std::sqrt(h.rr / b2) : 0.0;
     return res;
+}
+
+void factor_level(Core& c, const Level& L, int* status)
+{
+    EQG_CUDA(cudaMemcpyAsync(L.lu64->ptr, L.a64->ptr, (size_t)L.nnz * 8, cudaMemcpyDeviceToDevice, c.stream));
+    const int ns = (int)L.stage_ptr.size() - 1;
+    for (int s = 0; s < ns; ++s) {
+        const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
+        launch(c, "ilu0_factor", [&] {
+            ilu0_factor_stage_kernel<<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
+                r0, r1, L.rowptr->as<int>(), L.col->as<int>(), L.diag->as<int>(), L.lu64->as<double>(), status);
+        });
+    }
+}
+
+void to_float(Core& c, const Buf& src, Buf& dst, int64_t n)
+{
+    if (!dst) dst = c.allocN<float>((size_t)(n > 0 ? n : 1));
+    launch(c, "to_float",
+           [&] { to_float_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(src->as<double>(), dst->as<float>(), n); });
 }
 
 }  // namespace
@@ -647,29 +1060,44 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         res.converged = true;
         return res;
     }
-    // permuted matrix and factorization (FP64)
+    // level matrices and their factorizations (FP64)
     c.factor_clock.start(c.stream);
-    launch(c, "gather_values", [&] { gather_values_kernel<<<blocksFor(an.nnz), kThreads, 0, c.stream>>>(jval, an.vmap->as<int>(), an.a64->as<double>(),
-                                                                       an.nnz); });
-    EQG_CUDA(cudaMemcpyAsync(an.lu64->ptr, an.a64->ptr, (size_t)an.nnz * 8, cudaMemcpyDeviceToDevice, c.stream));
+    const Level& L0 = an.levels[0];
+    launch(c, "gather_values", [&] {
+        gather_values_kernel<<<blocksFor(an.nnz), kThreads, 0, c.stream>>>(jval, an.vmap->as<int>(),
+                                                                           L0.a64->as<double>(), an.nnz);
+    });
+    for (size_t l = 1; l < an.levels.size(); ++l) {
+        const Level& F = an.levels[l - 1];
+        const Level& C = an.levels[l];
+        launch(c, "mg_galerkin", [&] {
+            galerkin_kernel<<<blocksFor(C.nnz), kThreads, 0, c.stream>>>(C.nnz, C.gptr->as<int>(), C.gidx->as<int>(),
+                                                                         F.a64->as<double>(), C.a64->as<double>());
+        });
+    }
     EQG_CUDA(cudaMemsetAsync(an.factor_status->ptr, 0, sizeof(int), c.stream));
-    const int ns = (int)an.stage_ptr.size() - 1;
-    for (int s = 0; s < ns; ++s) {
-        const int r0 = an.stage_ptr[s], r1 = an.stage_ptr[s + 1];
-        launch(c, "ilu0_factor", [&] { ilu0_factor_stage_kernel<<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
-            r0, r1, an.rowptr->as<int>(), an.col->as<int>(), an.diag->as<int>(), an.lu64->as<double>(),
-            an.factor_status->as<int>()); });
+    for (auto& L : an.levels) {
+        if (L.coarsest) {
+            launch(c, "mg_dense_inverse", [&] {
+                dense_inverse_kernel<<<1, 1024, 0, c.stream>>>(L.n, L.rowptr->as<int>(), L.col->as<int>(),
+                                                               L.a64->as<double>(), L.work64->as<double>(),
+                                                               L.inv64->as<double>(), an.factor_status->as<int>());
+            });
+        } else {
+            factor_level(c, L, an.factor_status->as<int>());
+        }
     }
     Vecs<double> v = vecs<double>(an.vec64->as<double>(), n);
-    launch(c, "permute", [&] { permute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(rhs, an.perm->as<int>(), v.b, n); });
+    launch(c, "permute",
+           [&] { permute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(rhs, L0.perm->as<int>(), v.b, n); });
     if (mixed) {
-        if (!an.a32) {
-            an.a32 = c.allocN<float>((size_t)an.nnz);
-            an.lu32 = c.allocN<float>((size_t)an.nnz);
-            an.vec32 = c.allocN<float>((size_t)10 * n);
+        for (auto& L : an.levels) {
+            to_float(c, L.a64, L.a32, L.nnz);
+            if (L.coarsest) to_float(c, L.inv64, L.inv32, (int64_t)L.n * L.n);
+            else to_float(c, L.lu64, L.lu32, L.nnz);
+            if (!L.v32) L.v32 = c.allocN<float>((size_t)4 * (L.n > 0 ? L.n : 1));
         }
-        launch(c, "to_float", [&] { to_float_kernel<<<blocksFor(an.nnz), kThreads, 0, c.stream>>>(an.a64->as<double>(), an.a32->as<float>(), an.nnz); });
-        launch(c, "to_float", [&] { to_float_kernel<<<blocksFor(an.nnz), kThreads, 0, c.stream>>>(an.lu64->as<double>(), an.lu32->as<float>(), an.nnz); });
+        if (!an.vec32) an.vec32 = c.allocN<float>((size_t)10 * n);
     }
     c.factor_clock.stop(c.stream);
     int fstat = 0;
@@ -680,7 +1108,7 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     c.krylov_clock.start(c.stream);
 
     if (!mixed) {
-        res = bicgstab<double>(c, an, an.a64->as<double>(), an.lu64->as<double>(), v, tol, max_iter, check_every);
+        res = bicgstab<double>(c, an, L0.a64->as<double>(), v, tol, max_iter, check_every);
         res.sweeps = 1;
     } else {
         Vecs<float> w = vecs<float>(an.vec32->as<float>(), n);
@@ -689,12 +1117,15 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         double* part = an.partials->as<double>();
         unsigned int* cnt = an.counter->as<unsigned int>();
         const int nb = blocksFor(n, kThreads, kRedBlocks);
-        // x = 0, r = b
         k_fill(c, v.x, 0.0, n);
         Buf rr_dev = c.allocN<double>(2);
-        launch(c, "sumsq", [&] { sumsq_kernel<<<nb, kThreads, 0, c.stream>>>(v.b, n, part, cnt, rr_dev->as<double>()); });
-        launch(c, "residual", [&] { residual_kernel<<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(), an.a64->as<double>(),
-                                                       v.x, v.b, v.r, w.b, n, part, cnt, rr_dev->as<double>() + 1); });
+        launch(c, "sumsq",
+               [&] { sumsq_kernel<<<nb, kThreads, 0, c.stream>>>(v.b, n, part, cnt, rr_dev->as<double>()); });
+        launch(c, "residual", [&] {
+            residual_kernel<<<nb, kThreads, 0, c.stream>>>(L0.rowptr->as<int>(), L0.col->as<int>(),
+                                                           L0.a64->as<double>(), v.x, v.b, v.r, w.b, n, part, cnt,
+                                                           rr_dev->as<double>() + 1);
+        });
         EQG_CUDA(cudaMemcpyAsync(c.pinned, rr_dev->ptr, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
         c.sync();
         const double bb = c.pinned[0];
@@ -702,14 +1133,17 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         int total_iter = 0, sweeps = 0;
         bool conv = bb == 0.0 || rr <= tol * tol * bb;
         while (!conv && sweeps < max_sweeps && total_iter < max_iter) {
-            SolveResult inner = bicgstab<float>(c, an, an.a32->as<float>(), an.lu32->as<float>(), w, inner_tol,
-                                                max_iter - total_iter, check_every);
+            SolveResult inner = bicgstab<float>(c, an, L0.a32->as<float>(), w, inner_tol, max_iter - total_iter,
+                                                check_every);
             total_iter += inner.iterations;
             ++sweeps;
-            launch(c, "add_float", [&] { add_float_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, w.x, n); });
-            launch(c, "residual", [&] { residual_kernel<<<nb, kThreads, 0, c.stream>>>(an.rowptr->as<int>(), an.col->as<int>(),
-                                                           an.a64->as<double>(), v.x, v.b, v.r, w.b, n, part, cnt,
-                                                           rr_dev->as<double>() + 1); });
+            launch(c, "add_float",
+                   [&] { add_float_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, w.x, n); });
+            launch(c, "residual", [&] {
+                residual_kernel<<<nb, kThreads, 0, c.stream>>>(L0.rowptr->as<int>(), L0.col->as<int>(),
+                                                               L0.a64->as<double>(), v.x, v.b, v.r, w.b, n, part, cnt,
+                                                               rr_dev->as<double>() + 1);
+            });
             EQG_CUDA(cudaMemcpyAsync(c.pinned, rr_dev->as<double>() + 1, sizeof(double), cudaMemcpyDeviceToHost,
                                      c.stream));
             c.sync();
@@ -723,7 +1157,8 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         res.rel_residual = bb > 0 ? std::sqrt(rr / bb) : 0.0;
     }
     c.krylov_clock.stop(c.stream);
-    launch(c, "unpermute", [&] { unpermute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, an.perm->as<int>(), xout, n); });
+    launch(c, "unpermute",
+           [&] { unpermute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, L0.perm->as<int>(), xout, n); });
     return res;
 }
 

@@ -109,7 +109,8 @@ const char* eqg_backend_name(void);
  * Keys read: grid_dim (2), nx (6), ny (1), nz (1), dx, dy, dz (1.0),
  * verbose (0), max_iter (10), abs_res_tol (1e-6),
  * linsolver_residual_tolerance (1e-8), linsolver_max_iterations (1000).
- * The device library also reads linsolver_ordering (multicolor | natural),
+ * The device library also reads linsolver_preconditioner (multigrid |
+ * ilu0), linsolver_ordering (multicolor | natural),
  * linsolver_precision (double | mixed), linsolver_inner_tolerance (1e-4),
  * linsolver_max_sweeps (60), linsolver_check_every (8), time_kernel
  * (name of one kernel to time with CUDA events) and device (CUDA device

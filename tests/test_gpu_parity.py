@@ -62,25 +62,31 @@ def test_topology_parity(gpu_lib, oracle_lib, grid):
         assert np.array_equal(g.normal(g.allFaces())[d].value(), o.normal(o.allFaces())[d].value())
 
 
-@pytest.mark.parametrize("ordering", ["multicolor", "natural"])
-def test_heat_64x64_parity(gpu_lib, oracle_lib, ordering):
+@pytest.mark.parametrize("ordering,precond", [("multicolor", "multigrid"), ("multicolor", "ilu0"),
+                                              ("natural", "ilu0"), ("natural", "multigrid")])
+def test_heat_64x64_parity(gpu_lib, oracle_lib, ordering, precond):
     """Implicit heat equation, 64x64, 20 steps: fields within 1e-9 relative."""
     grid, case = programs.heat_case(64, 64, steps=20)
     params = dict(grid, abs_res_tol=1e-10, linsolver_residual_tolerance=1e-12)
-    og = programs.heat_equation(Runtime(gpu_lib, dict(params, linsolver_ordering=ordering)), 0.3, 1.0, **case)
+    og = programs.heat_equation(Runtime(gpu_lib, dict(params, linsolver_ordering=ordering,
+                                                      linsolver_preconditioner=precond)), 0.3, 1.0, **case)
     oo = programs.heat_equation(Runtime(oracle_lib, params), 0.3, 1.0, **case)
     for step, (a, b) in enumerate(zip(og, oo)):
         assert np.max(np.abs(a - b) / np.abs(b)) <= 1e-9, "step %d" % step
 
 
-@pytest.mark.parametrize("shape,precision", [((16, 16, None), "double"), ((16, 16, None), "mixed"),
-                                             ((8, 8, 4), "double"), ((8, 8, 4), "mixed")])
-def test_two_phase_parity(gpu_lib, oracle_lib, shape, precision):
+@pytest.mark.parametrize("shape,precision,precond", [((16, 16, None), "double", "multigrid"),
+                                                     ((16, 16, None), "mixed", "multigrid"),
+                                                     ((8, 8, 4), "double", "multigrid"),
+                                                     ((8, 8, 4), "mixed", "multigrid"),
+                                                     ((16, 16, 8), "double", "multigrid"),
+                                                     ((16, 16, 8), "mixed", "ilu0")])
+def test_two_phase_parity(gpu_lib, oracle_lib, shape, precision, precond):
     """Fully implicit two-phase flow: saturation within 1e-8 relative of the
     FP64 oracle after every step, in plain FP64 and in mixed precision."""
     grid, case = programs.two_phase_case(*shape, steps=3)
     params = dict(grid, abs_res_tol=1e-11, linsolver_residual_tolerance=1e-12, linsolver_max_iterations=5000)
-    eg = Runtime(gpu_lib, dict(params, linsolver_precision=precision))
+    eg = Runtime(gpu_lib, dict(params, linsolver_precision=precision, linsolver_preconditioner=precond))
     og = programs.two_phase(eg, **case)
     oo = programs.two_phase(Runtime(oracle_lib, params), **case)
     for step, ((pg, sg), (po, so)) in enumerate(zip(og, oo)):
