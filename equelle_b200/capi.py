@@ -77,6 +77,7 @@ SIGNATURES = {
     "eqg_runtime_synchronize": (C.c_int, [vp]),
     "eqg_runtime_stats": (C.c_int, [vp, C.POINTER(Stats)]),
     "eqg_runtime_reset_stats": (C.c_int, [vp]),
+    "eqg_runtime_kernel_profile": (C.c_int, [vp, C.c_char_p, C.c_int64, c_i64_p]),
     "eqg_runtime_mark": (C.c_int, [vp, c_int_p]),
     "eqg_runtime_elapsed_ms": (C.c_int, [vp, C.c_int, C.c_int, c_dbl_p]),
     "eqg_runtime_solve_marks": (C.c_int, [vp, C.c_int64, c_int_p, c_int_p]),

@@ -25,12 +25,36 @@ namespace {
 
 thread_local std::string g_last_error;
 
-// EQG_TRACE=1 in the environment prints every C-ABI call to stderr.
+// EQG_TRACE=1 in the environment prints every C-ABI call to stderr;
+// EQG_HOST_PROFILE=1 prints, at exit, the host time spent in each entry
+// point.
 bool trace_enabled()
 {
     static const bool on = std::getenv("EQG_TRACE") != nullptr;
     return on;
 }
+
+struct HostProfile {
+    bool on = std::getenv("EQG_HOST_PROFILE") != nullptr;
+    struct Entry {
+        int64_t calls = 0, slow = 0;  // slow: over 1 ms
+        double ms = 0.0, max_ms = 0.0;
+    };
+    std::map<std::string, Entry> calls;
+    ~HostProfile()
+    {
+        if (!on) return;
+        std::vector<std::pair<double, std::string>> v;
+        for (auto& kv : calls) v.emplace_back(kv.second.ms, kv.first);
+        std::sort(v.rbegin(), v.rend());
+        for (auto& e : v) {
+            const Entry& x = calls[e.second];
+            std::fprintf(stderr, "[eqg host] %-28s %8lld calls %10.3f ms, %lld over 1 ms, max %.3f ms\n",
+                         e.second.c_str(), (long long)x.calls, x.ms, (long long)x.slow, x.max_ms);
+        }
+    }
+};
+HostProfile g_host_profile;
 
 template <class F>
 int guarded(const char* name, F&& f)
@@ -40,6 +64,21 @@ int guarded(const char* name, F&& f)
         std::fprintf(stderr, "[eqg] %s\n", name);
         std::fflush(stderr);
     }
+    const auto t0 = std::chrono::steady_clock::now();
+    struct Timer {
+        const char* name;
+        std::chrono::steady_clock::time_point t0;
+        ~Timer()
+        {
+            if (!g_host_profile.on) return;
+            auto& e = g_host_profile.calls[name];
+            const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            e.calls++;
+            e.ms += ms;
+            if (ms > 1.0) e.slow++;
+            e.max_ms = std::max(e.max_ms, ms);
+        }
+    } timer{name, t0};
     try {
         f();
         if (trace) {
@@ -384,8 +423,8 @@ int eqg_runtime_stats(const eqg_runtime* rt, eqg_stats* out)
         double ms = 0.0;
         for (auto& pr : c.timer_pairs) {
             float f = 0.f;
-            EQG_CUDA(cudaEventSynchronize(pr.second));
-            EQG_CUDA(cudaEventElapsedTime(&f, pr.first, pr.second));
+            EQG_CUDA(cudaEventSynchronize(pr.b));
+            EQG_CUDA(cudaEventElapsedTime(&f, pr.a, pr.b));
             ms += f;
         }
         out->timed_kernel_ms = ms;
@@ -407,13 +446,45 @@ int eqg_runtime_reset_stats(eqg_runtime* rt)
         c.patterns_built = c.pattern_hits = 0;
         c.bytes_peak = c.bytes_in_use;
         for (auto& pr : c.timer_pairs) {
-            cudaEventDestroy(pr.first);
-            cudaEventDestroy(pr.second);
+            cudaEventDestroy(pr.a);
+            cudaEventDestroy(pr.b);
         }
         c.timer_pairs.clear();
         c.residual_clock.clear();
         c.factor_clock.clear();
         c.krylov_clock.clear();
+    });
+}
+
+int eqg_runtime_kernel_profile(const eqg_runtime* rt, char* buf, int64_t len, int64_t* needed)
+{
+    return guarded(__func__, [&] {
+        need(rt, "runtime");
+        const Core& c = *rt->core;
+        std::map<std::string, std::pair<int64_t, double>> agg;
+        for (auto& pr : c.timer_pairs) {
+            float f = 0.f;
+            EQG_CUDA(cudaEventSynchronize(pr.b));
+            EQG_CUDA(cudaEventElapsedTime(&f, pr.a, pr.b));
+            auto& e = agg[pr.name];
+            e.first++;
+            e.second += f;
+        }
+        std::string js = "{";
+        for (auto& kv : agg) {
+            if (js.size() > 1) js += ", ";
+            char tmp[256];
+            std::snprintf(tmp, sizeof(tmp), "\"%s\": [%lld, %.6f]", kv.first.c_str(), (long long)kv.second.first,
+                          kv.second.second);
+            js += tmp;
+        }
+        js += "}";
+        *needed = (int64_t)js.size() + 1;
+        if (buf && len > 0) {
+            const size_t m = std::min((size_t)len - 1, js.size());
+            std::memcpy(buf, js.data(), m);
+            buf[m] = 0;
+        }
     });
 }
 

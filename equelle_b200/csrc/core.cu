@@ -55,10 +55,12 @@ Core::~Core()
     cell_centroids.reset();
     red_partials.reset();
     red_counter.reset();
+    releasing = true;
+    release_cached();
     for (auto& m : marks) cudaEventDestroy(m.ev);
     for (auto& pr : timer_pairs) {
-        cudaEventDestroy(pr.first);
-        cudaEventDestroy(pr.second);
+        cudaEventDestroy(pr.a);
+        cudaEventDestroy(pr.b);
     }
     residual_clock.clear();
     factor_clock.clear();
@@ -70,29 +72,72 @@ Core::~Core()
     if (pinned) cudaFreeHost(pinned);
 }
 
+// Size classes of the caching allocator: multiples of 256 B up to 64 KiB,
+// then four classes per power of two (at most 25% slack).
+size_t Core::size_class(size_t bytes)
+{
+    if (bytes <= 65536) return (bytes + 255) & ~(size_t)255;
+    size_t p = 65536;
+    while (p * 2 < bytes) p *= 2;
+    const size_t step = p / 4;
+    return ((bytes + step - 1) / step) * step;
+}
+
+// Every buffer of a runtime is used on its one stream only, so a freed
+// block can serve the next request at once: work that still reads it was
+// enqueued earlier on the same stream.  Blocks return to per-class free
+// lists and go back to the pool only when the runtime ends (or when an
+// allocation fails), so time steps allocate without driver calls.
 Buf Core::alloc(size_t bytes)
 {
     if (bytes == 0) bytes = 16;
+    const size_t cls = size_class(bytes);
     void* p = nullptr;
-    cudaError_t e = cudaMallocAsync(&p, bytes, stream);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        fail(e == cudaErrorMemoryAllocation ? EQG_ERR_MEMORY : EQG_ERR_DEVICE,
-             std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+    auto it = free_blocks.find(cls);
+    if (it != free_blocks.end() && !it->second.empty()) {
+        p = it->second.back();
+        it->second.pop_back();
+        cached_bytes -= (int64_t)cls;
+    } else {
+        cudaError_t e = cudaMallocAsync(&p, cls, stream);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            release_cached();
+            e = cudaMallocAsync(&p, cls, stream);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            fail(e == cudaErrorMemoryAllocation ? EQG_ERR_MEMORY : EQG_ERR_DEVICE,
+                 std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " +
+                     cudaGetErrorString(e));
+        }
     }
-    bytes_in_use += (int64_t)bytes;
+    bytes_in_use += (int64_t)cls;
     if (bytes_in_use > bytes_peak) bytes_peak = bytes_in_use;
     auto b = std::make_shared<DevBuf>();
     b->core = this;
     b->ptr = p;
-    b->bytes = bytes;
+    b->bytes = cls;
     return b;
 }
 
 void Core::free(void* p, size_t bytes)
 {
-    cudaFreeAsync(p, stream);
     bytes_in_use -= (int64_t)bytes;
+    if (releasing) {
+        cudaFreeAsync(p, stream);
+        return;
+    }
+    free_blocks[bytes].push_back(p);
+    cached_bytes += (int64_t)bytes;
+}
+
+void Core::release_cached()
+{
+    for (auto& kv : free_blocks)
+        for (void* q : kv.second) cudaFreeAsync(q, stream);
+    free_blocks.clear();
+    cached_bytes = 0;
 }
 
 void Core::sync() { EQG_CUDA(cudaStreamSynchronize(stream)); }
@@ -388,17 +433,15 @@ void build_grid(Core& c, eqg_set** builtin)
     c.face_areas = c.allocN<double>(nf64);
     c.face_centroids = c.allocN<double>(c.dim * nf64);
     Buf face_interior = c.allocN<uint8_t>(nf64);
-    faces_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(d, c.face_cells->as<int32_t>(), c.face_areas->as<double>(),
+    launch(c, "grid_faces", [&] { faces_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(d, c.face_cells->as<int32_t>(), c.face_areas->as<double>(),
                                                              c.face_centroids->as<double>(),
-                                                             face_interior->as<uint8_t>());
-    c.checkLaunch("grid_faces");
+                                                             face_interior->as<uint8_t>()); });
     c.cell_volumes = c.allocN<double>(nc64);
     c.cell_centroids = c.allocN<double>(c.dim * nc64);
     Buf cell_boundary = c.allocN<uint8_t>(nc64);
-    cells_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, c.cell_volumes->as<double>(),
+    launch(c, "grid_cells", [&] { cells_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, c.cell_volumes->as<double>(),
                                                              c.cell_centroids->as<double>(),
-                                                             cell_boundary->as<uint8_t>());
-    c.checkLaunch("grid_cells");
+                                                             cell_boundary->as<uint8_t>()); });
 
     // index sets
     auto make = [&](int entity, Buf idx, int64_t n, bool identity) {
@@ -411,21 +454,17 @@ void build_grid(Core& c, eqg_set** builtin)
         return s;
     };
     Buf all_c = c.allocN<int32_t>(nc64), all_f = c.allocN<int32_t>(nf64);
-    iota_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(all_c->as<int32_t>(), nc64);
-    c.checkLaunch("iota");
-    iota_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(all_f->as<int32_t>(), nf64);
-    c.checkLaunch("iota");
+    launch(c, "iota", [&] { iota_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(all_c->as<int32_t>(), nc64); });
+    launch(c, "iota", [&] { iota_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(all_f->as<int32_t>(), nf64); });
     int64_t n_bc = 0, n_ic = 0, n_bf = 0, n_if = 0;
     Buf bc = compact_indices(c, cell_boundary->as<uint8_t>(), nc64, n_bc);
     Buf not_b = c.allocN<uint8_t>(nc64 > nf64 ? nc64 : nf64);
-    negate_u8_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(cell_boundary->as<uint8_t>(), not_b->as<uint8_t>(),
-                                                                 nc64);
-    c.checkLaunch("negate");
+    launch(c, "negate", [&] { negate_u8_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(cell_boundary->as<uint8_t>(), not_b->as<uint8_t>(),
+                                                                 nc64); });
     Buf ic = compact_indices(c, not_b->as<uint8_t>(), nc64, n_ic);
     Buf iff = compact_indices(c, face_interior->as<uint8_t>(), nf64, n_if);
-    negate_u8_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(face_interior->as<uint8_t>(), not_b->as<uint8_t>(),
-                                                                 nf64);
-    c.checkLaunch("negate");
+    launch(c, "negate", [&] { negate_u8_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(face_interior->as<uint8_t>(), not_b->as<uint8_t>(),
+                                                                 nf64); });
     Buf bf = compact_indices(c, not_b->as<uint8_t>(), nf64, n_bf);
     c.nif = (int)n_if;
     builtin[EQG_ALL_CELLS] = make(EQG_CELLS, all_c, nc64, true);
@@ -450,29 +489,25 @@ void build_grid(Core& c, eqg_set** builtin)
     c.grad = opm(c.nif, c.nc, 2, 2 * n_if);
     c.ngrad = opm(c.nif, c.nc, 2, 2 * n_if);
     if (c.nif > 0) {
-        grad_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(c.nif, iff->as<int32_t>(), c.face_cells->as<int32_t>(),
+        launch(c, "grad_op", [&] { grad_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(c.nif, iff->as<int32_t>(), c.face_cells->as<int32_t>(),
                                                                 -1.0, c.grad->ptr->as<int32_t>(),
-                                                                c.grad->src->as<int32_t>(), c.grad->w->as<double>());
-        c.checkLaunch("grad_op");
-        grad_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(c.nif, iff->as<int32_t>(), c.face_cells->as<int32_t>(),
+                                                                c.grad->src->as<int32_t>(), c.grad->w->as<double>()); });
+        launch(c, "ngrad_op", [&] { grad_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(c.nif, iff->as<int32_t>(), c.face_cells->as<int32_t>(),
                                                                 1.0, c.ngrad->ptr->as<int32_t>(),
-                                                                c.ngrad->src->as<int32_t>(), c.ngrad->w->as<double>());
-        c.checkLaunch("ngrad_op");
+                                                                c.ngrad->src->as<int32_t>(), c.ngrad->w->as<double>()); });
     } else {
         k_fill_i32(c, c.grad->ptr->as<int32_t>(), 0, 1);
         k_fill_i32(c, c.ngrad->ptr->as<int32_t>(), 0, 1);
     }
     c.div_full = opm(c.nc, c.nf, 2 * c.dim, (int64_t)2 * c.dim * nc64);
-    div_full_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, c.div_full->ptr->as<int32_t>(),
+    launch(c, "div_full_op", [&] { div_full_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, c.div_full->ptr->as<int32_t>(),
                                                                 c.div_full->src->as<int32_t>(),
-                                                                c.div_full->w->as<double>());
-    c.checkLaunch("div_full_op");
+                                                                c.div_full->w->as<double>()); });
 
     Buf ipos = c.allocN<int32_t>(nf64);
     k_fill_i32(c, ipos->as<int32_t>(), -1, nf64);
     if (n_if > 0) {
-        scatter_pos_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(iff->as<int32_t>(), n_if, ipos->as<int32_t>());
-        c.checkLaunch("interior_pos");
+        launch(c, "interior_pos", [&] { scatter_pos_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(iff->as<int32_t>(), n_if, ipos->as<int32_t>()); });
     }
     {
         auto m = std::make_shared<OpMatrix>();
@@ -481,18 +516,16 @@ void build_grid(Core& c, eqg_set** builtin)
         m->n_src = c.nif;
         m->max_row = 2 * c.dim;
         Buf cnt = c.allocN<int64_t>(nc64);
-        div_interior_kernel<false><<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, ipos->as<int32_t>(),
+        launch(c, "div_interior_count", [&] { div_interior_kernel<false><<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, ipos->as<int32_t>(),
                                                                                cnt->as<int64_t>(), nullptr, nullptr,
-                                                                               nullptr);
-        c.checkLaunch("div_interior_count");
+                                                                               nullptr); });
         const int64_t nnz = counts_to_rowptr(c, cnt, c.nc, m->ptr);
         m->src = c.allocN<int32_t>(nnz > 0 ? nnz : 1);
         m->w = c.allocN<double>(nnz > 0 ? nnz : 1);
-        div_interior_kernel<true><<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, ipos->as<int32_t>(), nullptr,
+        launch(c, "div_interior_fill", [&] { div_interior_kernel<true><<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, ipos->as<int32_t>(), nullptr,
                                                                               m->ptr->as<int32_t>(),
                                                                               m->src->as<int32_t>(),
-                                                                              m->w->as<double>());
-        c.checkLaunch("div_interior_fill");
+                                                                              m->w->as<double>()); });
         c.div_interior = m;
     }
     c.sync();

@@ -177,12 +177,23 @@ struct Core {
     std::vector<Mark> marks;
     std::vector<eqg_solve_info> solves;
     // device timing of one named kernel (parameter time_kernel)
-    std::string timed_kernel;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timer_pairs;
+    std::string timed_kernel;  // a kernel name, or "*" for all of them
+    struct TimedLaunch {
+        const char* name;
+        cudaEvent_t a, b;
+    };
+    std::vector<TimedLaunch> timer_pairs;
     PhaseClock residual_clock, factor_clock, krylov_clock;
 
     Core();
     ~Core();
+
+    // caching allocator (see core.cu)
+    std::unordered_map<size_t, std::vector<void*>> free_blocks;
+    int64_t cached_bytes = 0;
+    bool releasing = false;
+    static size_t size_class(size_t bytes);
+    void release_cached();
 
     uint64_t newId() { return next_id++; }
     Buf alloc(size_t bytes);
@@ -203,7 +214,7 @@ using CoreP = std::shared_ptr<Core>;
 template <class F>
 inline void launch(Core& c, const char* name, F&& f)
 {
-    const bool timed = !c.timed_kernel.empty() && c.timed_kernel == name;
+    const bool timed = !c.timed_kernel.empty() && (c.timed_kernel == name || c.timed_kernel == "*");
     cudaEvent_t a = nullptr, b = nullptr;
     if (timed) {
         cudaEventCreate(&a);
@@ -214,12 +225,12 @@ inline void launch(Core& c, const char* name, F&& f)
     c.checkLaunch(name);
     if (timed) {
         cudaEventRecord(b, c.stream);
-        c.timer_pairs.emplace_back(a, b);
+        c.timer_pairs.push_back({name, a, b});
     }
 }
 
 constexpr int kThreads = 256;
-constexpr int kRedBlocks = 592;  // 4 x 148 SMs
+constexpr int kRedBlocks = 2368;  // 16 x 148 SMs: grid cap of kernels that reduce through block partials
 
 inline int blocksFor(int64_t n, int threads = kThreads, int cap = 148 * 32)
 {

@@ -274,10 +274,8 @@ double run_reduce(Core& c, const double* a, int64_t n)
 {
     double* partials = c.red_partials->as<double>();
     const int nb = blocksFor(n, kThreads, kRedBlocks);
-    reduce_partials_kernel<OP, SQUARE><<<nb, kThreads, 0, c.stream>>>(a, n, partials);
-    c.checkLaunch("reduce_partials");
-    reduce_final_kernel<OP, SQUARE><<<1, kThreads, 0, c.stream>>>(partials, nb, partials + kRedBlocks);
-    c.checkLaunch("reduce_final");
+    launch(c, "reduce_partials", [&] { reduce_partials_kernel<OP, SQUARE><<<nb, kThreads, 0, c.stream>>>(a, n, partials); });
+    launch(c, "reduce_final", [&] { reduce_final_kernel<OP, SQUARE><<<1, kThreads, 0, c.stream>>>(partials, nb, partials + kRedBlocks); });
     EQG_CUDA(cudaMemcpyAsync(c.pinned, partials + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
     return c.pinned[0];
@@ -288,15 +286,13 @@ double run_reduce(Core& c, const double* a, int64_t n)
 void k_fill(Core& c, double* out, double v, int64_t n)
 {
     if (n <= 0) return;
-    fill_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(out, v, n);
-    c.checkLaunch("fill");
+    launch(c, "fill", [&] { fill_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(out, v, n); });
 }
 
 void k_fill_i32(Core& c, int32_t* out, int32_t v, int64_t n)
 {
     if (n <= 0) return;
-    fill_i32_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(out, v, n);
-    c.checkLaunch("fill_i32");
+    launch(c, "fill_i32", [&] { fill_i32_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(out, v, n); });
 }
 
 void k_binary(Core& c, int op, const double* a, const double* b, double* out, int64_t n)
@@ -304,92 +300,80 @@ void k_binary(Core& c, int op, const double* a, const double* b, double* out, in
     if (n <= 0) return;
     const int nb = blocksFor(n);
     switch (op) {
-    case EW_ADD: binary_kernel<EW_ADD><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); break;
-    case EW_SUB: binary_kernel<EW_SUB><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); break;
-    case EW_MUL: binary_kernel<EW_MUL><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); break;
-    case EW_DIV: binary_kernel<EW_DIV><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); break;
+    case EW_ADD: launch(c, "binary", [&] { binary_kernel<EW_ADD><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }); break;
+    case EW_SUB: launch(c, "binary", [&] { binary_kernel<EW_SUB><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }); break;
+    case EW_MUL: launch(c, "binary", [&] { binary_kernel<EW_MUL><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }); break;
+    case EW_DIV: launch(c, "binary", [&] { binary_kernel<EW_DIV><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }); break;
     default: fail(EQG_ERR_ARG, "unknown binary operator");
     }
-    c.checkLaunch("binary");
 }
 
 void k_binary_scalar(Core& c, int op, const double* a, double s, int scalar_left, double* out, int64_t n)
 {
     if (n <= 0) return;
-    binary_scalar_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, s, scalar_left, out, n);
-    c.checkLaunch("binary_scalar");
+    launch(c, "binary_scalar", [&] { binary_scalar_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, s, scalar_left, out, n); });
 }
 
 void k_unary_value(Core& c, int op, const double* a, double* out, int64_t n)
 {
     if (n <= 0) return;
-    unary_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, out, n);
-    c.checkLaunch("unary");
+    launch(c, "unary", [&] { unary_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, out, n); });
 }
 
 void k_compare(Core& c, int op, const double* a, const double* b, uint8_t* out, int64_t n)
 {
     if (n <= 0) return;
-    compare_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, b, out, n);
-    c.checkLaunch("compare");
+    launch(c, "compare", [&] { compare_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, b, out, n); });
 }
 
 void k_compare_scalar(Core& c, int op, const double* a, double s, int scalar_left, uint8_t* out, int64_t n)
 {
     if (n <= 0) return;
-    compare_scalar_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, s, scalar_left, out, n);
-    c.checkLaunch("compare_scalar");
+    launch(c, "compare_scalar", [&] { compare_scalar_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, s, scalar_left, out, n); });
 }
 
 void k_select_value(Core& c, const uint8_t* m, const double* a, const double* b, double* out, int64_t n)
 {
     if (n <= 0) return;
-    select_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(m, a, b, out, n);
-    c.checkLaunch("select");
+    launch(c, "select", [&] { select_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(m, a, b, out, n); });
 }
 
 void k_mask_logic(Core& c, int op, const uint8_t* a, const uint8_t* b, uint8_t* out, int64_t n)
 {
     if (n <= 0) return;
-    mask_logic_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, b, out, n);
-    c.checkLaunch("mask_logic");
+    launch(c, "mask_logic", [&] { mask_logic_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, b, out, n); });
 }
 
 void k_set_select(Core& c, const uint8_t* m, const int32_t* a, const int32_t* b, int32_t* out, int64_t n)
 {
     if (n <= 0) return;
-    set_select_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(m, a, b, out, n);
-    c.checkLaunch("set_select");
+    launch(c, "set_select", [&] { set_select_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(m, a, b, out, n); });
 }
 
 void k_is_empty(Core& c, const int32_t* s, uint8_t* out, int64_t n)
 {
     if (n <= 0) return;
-    is_empty_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(s, out, n);
-    c.checkLaunch("is_empty");
+    launch(c, "is_empty", [&] { is_empty_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(s, out, n); });
 }
 
 void k_face_neighbour(Core& c, const int32_t* faces, int side, int32_t* out, int64_t n, int32_t* err)
 {
     if (n <= 0) return;
-    face_neighbour_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(c.face_cells->as<int32_t>(), faces, side, out, n,
-                                                                   c.nf, err);
-    c.checkLaunch("face_neighbour");
+    launch(c, "face_neighbour", [&] { face_neighbour_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(c.face_cells->as<int32_t>(), faces, side, out, n,
+                                                                   c.nf, err); });
 }
 
 void k_gather_i32(Core& c, const int32_t* data, const int32_t* map, int32_t* out, int64_t n, int32_t fill)
 {
     if (n <= 0) return;
-    gather_i32_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(data, map, out, n, fill);
-    c.checkLaunch("gather_i32");
+    launch(c, "gather_i32", [&] { gather_i32_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(data, map, out, n, fill); });
 }
 
 void k_gather_f64(Core& c, const double* data, const int32_t* idx, int stride, int comp, double* out, int64_t n,
                   int32_t* err)
 {
     if (n <= 0) return;
-    gather_f64_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(data, idx, stride, comp, out, n, err);
-    c.checkLaunch("gather_f64");
+    launch(c, "gather_f64", [&] { gather_f64_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(data, idx, stride, comp, out, n, err); });
 }
 
 void k_normal(Core& c, const int32_t* faces, double* out, int comp, int64_t n, int32_t* err)
@@ -397,31 +381,27 @@ void k_normal(Core& c, const int32_t* faces, double* out, int comp, int64_t n, i
     if (n <= 0) return;
     const int fx = (c.nx + 1) * c.ny * c.nz;
     const int fy = c.nx * (c.ny + 1) * c.nz;
-    normal_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(faces, c.face_areas->as<double>(), out, comp, c.dim, c.nf,
-                                                           fx, fy, n, err);
-    c.checkLaunch("normal");
+    launch(c, "normal", [&] { normal_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(faces, c.face_areas->as<double>(), out, comp, c.dim, c.nf,
+                                                           fx, fy, n, err); });
 }
 
 void k_locate(Core& c, const int32_t* sorted, int64_t n_sorted, const int32_t* keys, int32_t* pos, int64_t n_keys,
               int identity_n, int32_t* err)
 {
     if (n_keys <= 0) return;
-    locate_kernel<<<blocksFor(n_keys), kThreads, 0, c.stream>>>(sorted, n_sorted, keys, pos, n_keys, identity_n, err);
-    c.checkLaunch("locate");
+    launch(c, "locate", [&] { locate_kernel<<<blocksFor(n_keys), kThreads, 0, c.stream>>>(sorted, n_sorted, keys, pos, n_keys, identity_n, err); });
 }
 
 void k_scatter_inverse(Core& c, const int32_t* pos, int64_t n, int32_t* inv, int32_t* err)
 {
     if (n <= 0) return;
-    scatter_inverse_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(pos, n, inv, err);
-    c.checkLaunch("scatter_inverse");
+    launch(c, "scatter_inverse", [&] { scatter_inverse_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(pos, n, inv, err); });
 }
 
 void k_is_strictly_sorted(Core& c, const int32_t* a, int64_t n, int32_t* flag)
 {
     if (n <= 1) return;
-    strictly_sorted_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(a, n, flag);
-    c.checkLaunch("strictly_sorted");
+    launch(c, "strictly_sorted", [&] { strictly_sorted_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(a, n, flag); });
 }
 
 double k_reduce(Core& c, int op, const double* a, int64_t n)
@@ -439,10 +419,8 @@ double k_two_norm(Core& c, const double* a, int64_t n)
 {
     double* partials = c.red_partials->as<double>();
     const int nb = blocksFor(n, kThreads, kRedBlocks);
-    reduce_partials_kernel<EQG_SUM, true><<<nb, kThreads, 0, c.stream>>>(a, n, partials);
-    c.checkLaunch("norm_partials");
-    reduce_final_kernel<EQG_SUM, true><<<1, kThreads, 0, c.stream>>>(partials, nb, partials + kRedBlocks);
-    c.checkLaunch("norm_final");
+    launch(c, "norm_partials", [&] { reduce_partials_kernel<EQG_SUM, true><<<nb, kThreads, 0, c.stream>>>(a, n, partials); });
+    launch(c, "norm_final", [&] { reduce_final_kernel<EQG_SUM, true><<<1, kThreads, 0, c.stream>>>(partials, nb, partials + kRedBlocks); });
     EQG_CUDA(cudaMemcpyAsync(c.pinned, partials + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
     return c.pinned[0];

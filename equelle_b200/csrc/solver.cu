@@ -80,8 +80,8 @@ __device__ __forceinline__ void block_sum(double (&v)[NV])
     }
 }
 
-// Writes block partials; returns true in exactly one thread of the last
-// block to finish, after which `partials` holds all blocks' sums.
+// Writes this block's sums to `partials`; returns true, in every thread of
+// the block, for the last block to finish.
 template <int NV>
 __device__ __forceinline__ bool publish_partials(double (&v)[NV], double* partials, unsigned int* counter)
 {
@@ -95,31 +95,103 @@ __device__ __forceinline__ bool publish_partials(double (&v)[NV], double* partia
         last = (done == gridDim.x - 1);
     }
     __syncthreads();
-    return last && threadIdx.x == 0;
+    return last;
 }
 
+// Grid-wide sums of NV values, deterministic: block sums in fixed slots, the
+// last block to finish adds them up in a fixed order with all its threads.
+// Returns true in thread 0 of that block, with the sums in `out`.
 template <int NV>
-__device__ __forceinline__ void final_sums(const double* partials, int nblocks, double (&out)[NV],
-                                           unsigned int* counter)
+__device__ __forceinline__ bool grid_sum(double (&v)[NV], double* partials, unsigned int* counter, double (&out)[NV])
 {
+    if (!publish_partials<NV>(v, partials, counter)) return false;
     __threadfence();
+    double acc[NV];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) out[k] = 0.0;
-    for (int b = 0; b < nblocks; ++b)
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
 #pragma unroll
-        for (int k = 0; k < NV; ++k) out[k] += ((volatile double*)partials)[b * NV + k];
+        for (int k = 0; k < NV; ++k) acc[k] += ((volatile double*)partials)[b * NV + k];
+    __syncthreads();
+    block_sum<NV>(acc);
+    if (threadIdx.x != 0) return false;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = acc[k];
     *counter = 0u;
+    return true;
 }
 
 // ---- matrix kernels ---------------------------------------------------------
-template <class T>
-__device__ __forceinline__ double row_dot(int r, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                          const T* __restrict__ a, const T* __restrict__ x)
+// Level matrices used by the sweeps are in a sliced ELL layout: rows in
+// slices of 32 (one warp), each slice stored column-major and padded to its
+// longest row, so that a warp's k-th loads of its 32 rows are one contiguous
+// 256-byte (FP64) segment.  Within a row, entries are in ascending column
+// order, so the ILU(0) lower part is k < dk[r] and the upper part k > dk[r].
+struct SellView {
+    const int* __restrict__ slice_ptr;  // first slot of each slice
+    const int* __restrict__ col;        // column of each slot
+    const int* __restrict__ len;        // entries of each row
+    const int* __restrict__ dk;         // position of the diagonal in each row
+};
+
+__device__ __forceinline__ int sell_base(const SellView& m, int r) { return m.slice_ptr[r >> 5] + (r & 31); }
+
+// sum_{k0 <= k < k1} a[row, k] x[col[row, k]], added in ascending k.  With
+// KM > 0 (rows of at most KM entries) the loop is unrolled so that a thread
+// issues all its column and value loads before the dependent gathers of x:
+// the kernels using it are bound by the latency of that load chain.
+template <int KM, class T>
+__device__ __forceinline__ double sell_dot(const SellView& m, int base, int k0, int k1, const T* __restrict__ a,
+                                           const T* __restrict__ x)
 {
     double acc = 0.0;
-    const int e1 = rowptr[r + 1];
-    for (int e = rowptr[r]; e < e1; ++e) acc += (double)a[e] * (double)x[col[e]];
+    if (KM == 0) {
+        for (int k = k0; k < k1; ++k) {
+            const int idx = base + (k << 5);
+            acc += (double)a[idx] * (double)x[m.col[idx]];
+        }
+        return acc;
+    }
+    int ci[KM > 0 ? KM : 1];
+    T av[KM > 0 ? KM : 1];
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+        const bool on = k >= k0 && k < k1;
+        const int idx = base + (k << 5);
+        ci[k] = on ? m.col[idx] : 0;
+        av[k] = on ? a[idx] : (T)0;
+    }
+#pragma unroll
+    for (int k = 0; k < KM; ++k)
+        if (k >= k0 && k < k1) acc += (double)av[k] * (double)x[ci[k]];
     return acc;
+}
+
+// Dispatches on a level's longest row as KK (4, 8, 16; 0 = plain loop).
+#define WITH_KMAX(kmax, ...)                        \
+    if ((kmax) <= 4) {                              \
+        constexpr int KK = 4;                       \
+        __VA_ARGS__;                                \
+    } else if ((kmax) <= 8) {                       \
+        constexpr int KK = 8;                       \
+        __VA_ARGS__;                                \
+    } else if ((kmax) <= 16) {                      \
+        constexpr int KK = 16;                      \
+        __VA_ARGS__;                                \
+    } else {                                        \
+        constexpr int KK = 0;                       \
+        __VA_ARGS__;                                \
+    }
+
+// dst (sliced ELL) <- src (CSR) through the slot map; padding slots get 0.
+__global__ void sell_scatter_kernel(int64_t size, const int* __restrict__ map, const double* __restrict__ src,
+                                    double* __restrict__ dst)
+{
+    GRID_STRIDE(i, size)
+    {
+        const int e = map[i];
+        dst[i] = e >= 0 ? src[e] : 0.0;
+    }
 }
 
 __global__ void gather_values_kernel(const double* __restrict__ src, const int* __restrict__ vmap,
@@ -176,36 +248,31 @@ __global__ void ilu0_factor_stage_kernel(int r0, int r1, const int* __restrict__
     }
 }
 
-template <class T>
-__global__ void ilu0_lower_stage_kernel(int r0, int r1, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                        const int* __restrict__ diag, const T* __restrict__ lu,
+template <int KM, class T>
+__global__ void ilu0_lower_stage_kernel(int r0, int r1, SellView m, const T* __restrict__ lu,
                                         const T* __restrict__ b, T* __restrict__ y, const KScal* sc, int skip_if_s)
 {
     if (stopped(sc) || (skip_if_s && sc->s_conv)) return;
     for (int64_t rr = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; rr < r1;
          rr += (int64_t)gridDim.x * blockDim.x) {
         const int r = (int)rr;
-        double s = (double)b[r];
-        const int dpos = diag[r];
-        for (int e = rowptr[r]; e < dpos; ++e) s -= (double)lu[e] * (double)y[col[e]];
-        y[r] = (T)s;
+        const double s = sell_dot<KM, T>(m, sell_base(m, r), 0, m.dk[r], lu, y);
+        y[r] = (T)((double)b[r] - s);
     }
 }
 
-template <class T>
-__global__ void ilu0_upper_stage_kernel(int r0, int r1, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                        const int* __restrict__ diag, const T* __restrict__ lu, T* __restrict__ x,
+template <int KM, class T>
+__global__ void ilu0_upper_stage_kernel(int r0, int r1, SellView m, const T* __restrict__ lu, T* __restrict__ x,
                                         const KScal* sc, int skip_if_s)
 {
     if (stopped(sc) || (skip_if_s && sc->s_conv)) return;
     for (int64_t rr = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; rr < r1;
          rr += (int64_t)gridDim.x * blockDim.x) {
         const int r = (int)rr;
-        const int dpos = diag[r];
-        double s = (double)x[r];
-        const int e1 = rowptr[r + 1];
-        for (int e = dpos + 1; e < e1; ++e) s -= (double)lu[e] * (double)x[col[e]];
-        x[r] = (T)(s / (double)lu[dpos]);
+        const int base = sell_base(m, r);
+        const int d = m.dk[r];
+        const double s = sell_dot<KM, T>(m, base, d + 1, m.len[r], lu, x);
+        x[r] = (T)(((double)x[r] - s) / (double)lu[base + (d << 5)]);
     }
 }
 
@@ -240,9 +307,8 @@ __global__ void bicg_init_kernel(const T* __restrict__ b, T* r, T* rhat, T* p, T
         d[0] += (double)bi * (double)bi;
         d[1] += (double)hi * (double)bi;
     }
-    if (publish_partials<2>(d, partials, counter)) {
-        double s[2];
-        final_sums<2>(partials, gridDim.x, s, counter);
+    double s[2];
+    if (grid_sum<2>(d, partials, counter, s)) {
         sc->rho = 1.0;
         sc->alpha = 1.0;
         sc->omega = 1.0;
@@ -266,22 +332,21 @@ __global__ void bicg_p_kernel(const T* __restrict__ r, const T* __restrict__ v, 
 }
 
 // v = A ph ; alpha = rho_new / (rhat . v)
-template <class T>
-__global__ void bicg_spmv_alpha_kernel(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                       const T* __restrict__ a, const T* __restrict__ ph, const T* __restrict__ rhat,
-                                       T* __restrict__ v, int n, double* partials, unsigned int* counter, KScal* sc)
+template <int KM, class T>
+__global__ void bicg_spmv_alpha_kernel(SellView m, const T* __restrict__ a, const T* __restrict__ ph,
+                                       const T* __restrict__ rhat, T* __restrict__ v, int n, double* partials,
+                                       unsigned int* counter, KScal* sc)
 {
     if (stopped(sc)) return;
     double d[1] = {0.0};
     GRID_STRIDE(i, n)
     {
-        const double vi = row_dot<T>((int)i, rowptr, col, a, ph);
+        const double vi = sell_dot<KM, T>(m, sell_base(m, (int)i), 0, m.len[i], a, ph);
         v[i] = (T)vi;
         d[0] += (double)rhat[i] * (double)(T)vi;
     }
-    if (publish_partials<1>(d, partials, counter)) {
-        double s[1];
-        final_sums<1>(partials, gridDim.x, s, counter);
+    double s[1];
+    if (grid_sum<1>(d, partials, counter, s)) {
         sc->rv = s[0];
         if (s[0] == 0.0 || !isfinite(s[0])) sc->status = ST_BREAK;
         else sc->alpha = sc->rho_new / s[0];
@@ -302,32 +367,30 @@ __global__ void bicg_s_kernel(const T* __restrict__ r, const T* __restrict__ v, 
         s[i] = si;
         d[0] += (double)si * (double)si;
     }
-    if (publish_partials<1>(d, partials, counter)) {
-        double t[1];
-        final_sums<1>(partials, gridDim.x, t, counter);
+    double t[1];
+    if (grid_sum<1>(d, partials, counter, t)) {
         sc->ss = t[0];
         sc->s_conv = t[0] <= sc->thr ? 1 : 0;
     }
 }
 
 // t = A sh ; omega = (t . s) / (t . t)
-template <class T>
-__global__ void bicg_spmv_omega_kernel(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                       const T* __restrict__ a, const T* __restrict__ sh, const T* __restrict__ s,
-                                       T* __restrict__ t, int n, double* partials, unsigned int* counter, KScal* sc)
+template <int KM, class T>
+__global__ void bicg_spmv_omega_kernel(SellView m, const T* __restrict__ a, const T* __restrict__ sh,
+                                       const T* __restrict__ s, T* __restrict__ t, int n, double* partials,
+                                       unsigned int* counter, KScal* sc)
 {
     if (stopped(sc) || sc->s_conv) return;
     double d[2] = {0.0, 0.0};
     GRID_STRIDE(i, n)
     {
-        const T ti = (T)row_dot<T>((int)i, rowptr, col, a, sh);
+        const T ti = (T)sell_dot<KM, T>(m, sell_base(m, (int)i), 0, m.len[i], a, sh);
         t[i] = ti;
         d[0] += (double)ti * (double)s[i];
         d[1] += (double)ti * (double)ti;
     }
-    if (publish_partials<2>(d, partials, counter)) {
-        double u[2];
-        final_sums<2>(partials, gridDim.x, u, counter);
+    double u[2];
+    if (grid_sum<2>(d, partials, counter, u)) {
         sc->ts = u[0];
         sc->tt = u[1];
         if (u[1] == 0.0 || !isfinite(u[1])) sc->status = ST_BREAK;
@@ -358,9 +421,8 @@ __global__ void bicg_xr_kernel(const T* __restrict__ ph, const T* __restrict__ s
             d[1] += (double)rhat[i] * (double)ri;
         }
     }
-    if (publish_partials<2>(d, partials, counter)) {
-        double u[2];
-        final_sums<2>(partials, gridDim.x, u, counter);
+    double u[2];
+    if (grid_sum<2>(d, partials, counter, u)) {
         sc->iterations += 1;
         if (half) {
             sc->rr = sc->ss;
@@ -377,22 +439,21 @@ __global__ void bicg_xr_kernel(const T* __restrict__ ph, const T* __restrict__ s
 }
 
 // Refinement: r = b - A x (FP64) with rr = r.r ; also r32 = float(r).
-__global__ void residual_kernel(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                const double* __restrict__ a, const double* __restrict__ x,
+template <int KM>
+__global__ void residual_kernel(SellView m, const double* __restrict__ a, const double* __restrict__ x,
                                 const double* __restrict__ b, double* __restrict__ r, float* __restrict__ r32, int n,
                                 double* partials, unsigned int* counter, double* out_rr)
 {
     double d[1] = {0.0};
     GRID_STRIDE(i, n)
     {
-        const double ri = b[i] - row_dot<double>((int)i, rowptr, col, a, x);
+        const double ri = b[i] - sell_dot<KM, double>(m, sell_base(m, (int)i), 0, m.len[i], a, x);
         r[i] = ri;
         r32[i] = (float)ri;
         d[0] += ri * ri;
     }
-    if (publish_partials<1>(d, partials, counter)) {
-        double u[1];
-        final_sums<1>(partials, gridDim.x, u, counter);
+    double u[1];
+    if (grid_sum<1>(d, partials, counter, u)) {
         *out_rr = u[0];
     }
 }
@@ -407,9 +468,8 @@ __global__ void sumsq_kernel(const double* __restrict__ a, int n, double* partia
 {
     double d[1] = {0.0};
     GRID_STRIDE(i, n) d[0] += a[i] * a[i];
-    if (publish_partials<1>(d, partials, counter)) {
-        double u[1];
-        final_sums<1>(partials, gridDim.x, u, counter);
+    double u[1];
+    if (grid_sum<1>(d, partials, counter, u)) {
         *out = u[0];
     }
 }
@@ -436,13 +496,12 @@ __device__ __forceinline__ bool mg_skip(const KScal* sc, int skip_if_s)
 }
 
 // out = b - A x
-template <class T>
-__global__ void mg_residual_kernel(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                   const T* __restrict__ a, const T* __restrict__ x, const T* __restrict__ b,
-                                   T* __restrict__ out, const KScal* sc, int skip_if_s)
+template <int KM, class T>
+__global__ void mg_residual_kernel(int n, SellView m, const T* __restrict__ a, const T* __restrict__ x,
+                                   const T* __restrict__ b, T* __restrict__ out, const KScal* sc, int skip_if_s)
 {
     if (mg_skip(sc, skip_if_s)) return;
-    GRID_STRIDE(i, n) out[i] = (T)((double)b[i] - row_dot<T>((int)i, rowptr, col, a, x));
+    GRID_STRIDE(i, n) out[i] = (T)((double)b[i] - sell_dot<KM, T>(m, sell_base(m, (int)i), 0, m.len[i], a, x));
 }
 
 // rc[P] = sum of t over the members of aggregate P
@@ -574,8 +633,16 @@ struct Level {
     Buf perm, rowptr, col, diag;   // permuted pattern
     Buf gptr, gidx;                // Galerkin gather from the finer level (levels > 0)
     Buf agg, mptr, midx;           // to the next coarser level
-    Buf a64, lu64, a32, lu32;
+    Buf a64, lu64;                 // CSR values: matrix, ILU(0) factors
+    int64_t sell_size = 0;         // sliced ELL copies used by the sweeps
+    int kmax = 0;                  // longest row
+    Buf sell_ptr, sell_col, sell_len, sell_dk, sell_map;
+    Buf as64, lus64, as32, lus32;
     Buf v64, v32;                  // 4 work vectors: r, z, t, w
+    SellView view() const
+    {
+        return SellView{sell_ptr->as<int>(), sell_col->as<int>(), sell_len->as<int>(), sell_dk->as<int>()};
+    }
     Buf work64, inv64, inv32;      // coarsest level
 };
 
@@ -588,6 +655,17 @@ struct SolverAnalysis {
     std::vector<Level> levels;
     Buf vmap;        // level-0 permuted entry <- Jacobian entry
     Buf vec64, vec32, scal, partials, counter, factor_status;
+    // CUDA graphs of `chunk` BiCGStab iterations, [0] FP64 and [1] FP32
+    struct IterGraph {
+        cudaGraphExec_t exec = nullptr;
+        int chunk = 0;
+        int64_t kernels = 0;
+    } graph[2];
+    ~SolverAnalysis()
+    {
+        for (auto& g : graph)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+    }
 };
 
 namespace {
@@ -689,6 +767,43 @@ void order_level(Core& c, const HostCsr& A, bool natural, Level& L, std::vector<
     }
     L.n = n;
     L.nnz = nnz;
+    {
+        // sliced ELL, 32 rows per slice (one thread per row)
+        const int nsl = (n + 31) / 32;
+        std::vector<int> sp(nsl + 1, 0), len(n), dk(n);
+        for (int sl = 0; sl < nsl; ++sl) {
+            int w = 0;
+            for (int r = sl * 32; r < std::min(n, sl * 32 + 32); ++r) w = std::max(w, pcsr_ptr[r + 1] - pcsr_ptr[r]);
+            sp[sl + 1] = sp[sl] + 32 * w;
+        }
+        const int64_t size = sp[nsl];
+        std::vector<int> scol(size > 0 ? size : 1, 0), smap(size > 0 ? size : 1, -1);
+        for (int r = 0; r < n; ++r) {
+            const int base = sp[r / 32] + (r % 32);
+            len[r] = pcsr_ptr[r + 1] - pcsr_ptr[r];
+            dk[r] = diag[r] - pcsr_ptr[r];
+            const int w = (sp[r / 32 + 1] - sp[r / 32]) / 32;
+            for (int k = 0; k < w; ++k) {
+                const int idx = base + 32 * k;
+                if (k < len[r]) {
+                    scol[idx] = pcsr_col[pcsr_ptr[r] + k];
+                    smap[idx] = pcsr_ptr[r] + k;
+                } else {
+                    scol[idx] = r;  // padding: a valid column, value 0, never read by the sweeps
+                }
+            }
+        }
+        L.sell_size = size;
+        L.kmax = 0;
+        for (int r = 0; r < n; ++r) L.kmax = std::max(L.kmax, len[r]);
+        L.sell_ptr = upload_ints(c, sp);
+        L.sell_col = upload_ints(c, scol);
+        L.sell_len = upload_ints(c, len);
+        L.sell_dk = upload_ints(c, dk);
+        L.sell_map = upload_ints(c, smap);
+        L.as64 = c.allocN<double>((size_t)(size > 0 ? size : 1));
+        L.lus64 = c.allocN<double>((size_t)(size > 0 ? size : 1));
+    }
     L.perm = upload_ints(c, perm);
     L.rowptr = upload_ints(c, pcsr_ptr);
     L.col = upload_ints(c, pcsr_col);
@@ -876,15 +991,15 @@ Vecs<T> vecs(T* base, int n)
 template <class T>
 const T* level_a(const Level& L);
 template <>
-const double* level_a<double>(const Level& L) { return L.a64->as<double>(); }
+const double* level_a<double>(const Level& L) { return L.as64->as<double>(); }
 template <>
-const float* level_a<float>(const Level& L) { return L.a32->as<float>(); }
+const float* level_a<float>(const Level& L) { return L.as32->as<float>(); }
 template <class T>
 const T* level_lu(const Level& L);
 template <>
-const double* level_lu<double>(const Level& L) { return L.lu64->as<double>(); }
+const double* level_lu<double>(const Level& L) { return L.lus64->as<double>(); }
 template <>
-const float* level_lu<float>(const Level& L) { return L.lu32->as<float>(); }
+const float* level_lu<float>(const Level& L) { return L.lus32->as<float>(); }
 template <class T>
 T* level_vec(const Level& L, int k);
 template <>
@@ -906,17 +1021,17 @@ void ilu_apply(Core& c, const Level& L, const T* in, T* out, const KScal* sc, in
     const int ns = (int)L.stage_ptr.size() - 1;
     for (int s = 0; s < ns; ++s) {
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
-        launch(c, "ilu0_lower", [&] {
-            ilu0_lower_stage_kernel<T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
-                r0, r1, L.rowptr->as<int>(), L.col->as<int>(), L.diag->as<int>(), lu, in, out, sc, skip_if_s);
-        });
+        WITH_KMAX(L.kmax, launch(c, "ilu0_lower", [&] {
+            ilu0_lower_stage_kernel<KK, T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(r0, r1, L.view(), lu, in,
+                                                                                          out, sc, skip_if_s);
+        }));
     }
     for (int s = ns - 1; s >= 0; --s) {
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
-        launch(c, "ilu0_upper", [&] {
-            ilu0_upper_stage_kernel<T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
-                r0, r1, L.rowptr->as<int>(), L.col->as<int>(), L.diag->as<int>(), lu, out, sc, skip_if_s);
-        });
+        WITH_KMAX(L.kmax, launch(c, "ilu0_upper", [&] {
+            ilu0_upper_stage_kernel<KK, T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(r0, r1, L.view(), lu, out,
+                                                                                          sc, skip_if_s);
+        }));
     }
 }
 
@@ -938,10 +1053,9 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     T* zc = level_vec<T>(C, 1);
     const T* a = level_a<T>(L);
     ilu_apply<T>(c, L, r, z, sc, skip);
-    launch(c, "mg_residual", [&] {
-        mg_residual_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.rowptr->as<int>(), L.col->as<int>(), a, z,
-                                                                        r, t, sc, skip);
-    });
+    WITH_KMAX(L.kmax, launch(c, "mg_residual", [&] {
+        mg_residual_kernel<KK, T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.view(), a, z, r, t, sc, skip);
+    }));
     launch(c, "mg_restrict", [&] {
         mg_restrict_kernel<T><<<blocksFor(C.n), kThreads, 0, c.stream>>>(C.n, L.mptr->as<int>(), L.midx->as<int>(), t,
                                                                           rc, sc, skip);
@@ -950,10 +1064,9 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     launch(c, "mg_prolong", [&] {
         mg_prolong_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.agg->as<int>(), zc, z, sc, skip);
     });
-    launch(c, "mg_residual", [&] {
-        mg_residual_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.rowptr->as<int>(), L.col->as<int>(), a, z,
-                                                                        r, t, sc, skip);
-    });
+    WITH_KMAX(L.kmax, launch(c, "mg_residual", [&] {
+        mg_residual_kernel<KK, T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.view(), a, z, r, t, sc, skip);
+    }));
     ilu_apply<T>(c, L, t, w, sc, skip);
     launch(c, "mg_add", [&] { mg_add_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, w, z, sc, skip); });
 }
@@ -979,29 +1092,62 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double 
     launch(c, "bicg_init", [&] {
         bicg_init_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.b, v.r, v.rhat, v.p, v.v, v.x, n, part, cnt, sc, tol * tol);
     });
+    auto iteration = [&] {
+        launch(c, "bicg_p", [&] { bicg_p_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(v.r, v.v, v.p, n, sc); });
+        precondition<T>(c, an, v.p, v.ph, sc, 0);
+        WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_alpha", [&] {
+            bicg_spmv_alpha_kernel<KK, T><<<nb, kThreads, 0, c.stream>>>(L0.view(), a, v.ph, v.rhat, v.v, n, part, cnt,
+                                                                        sc);
+        }));
+        launch(c, "bicg_s", [&] { bicg_s_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.r, v.v, v.s, n, part, cnt, sc); });
+        precondition<T>(c, an, v.s, v.sh, sc, 1);
+        WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_omega", [&] {
+            bicg_spmv_omega_kernel<KK, T><<<nb, kThreads, 0, c.stream>>>(L0.view(), a, v.sh, v.s, v.t, n, part, cnt,
+                                                                        sc);
+        }));
+        launch(c, "bicg_xr", [&] {
+            bicg_xr_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.ph, v.sh, v.s, v.t, v.rhat, v.x, v.r, n, part, cnt, sc);
+        });
+    };
+    // Graph of `check_every` iterations, captured once per analysis and
+    // precision; kernel arguments are fixed (buffers of the analysis,
+    // scalars in device memory).  Kernel timing (time_kernel) needs one
+    // event pair per launch, so timed runs launch eagerly.
+    const bool graphs = c.timed_kernel.empty() && c.param_i("linsolver_graphs", 1) != 0;
+    SolverAnalysis::IterGraph& g = an.graph[sizeof(T) == sizeof(double) ? 0 : 1];
+    if (graphs && (!g.exec || g.chunk != check_every)) {
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+        const int64_t before = c.launches.load();
+        cudaGraph_t graph = nullptr;
+        EQG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            for (int k = 0; k < check_every; ++k) iteration();
+        } catch (...) {
+            cudaStreamEndCapture(c.stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        EQG_CUDA(cudaStreamEndCapture(c.stream, &graph));
+        const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) fail(EQG_ERR_DEVICE, std::string("graph instantiation failed: ") + cudaGetErrorString(ie));
+        g.kernels = c.launches.load() - before;
+        c.launches -= g.kernels;  // captured, not executed
+        g.chunk = check_every;
+    }
     SolveResult res;
     KScal h{};
     int enq = 0;
     for (;;) {
         const int chunk = std::min(check_every, max_iter - enq);
-        for (int k = 0; k < chunk; ++k) {
-            launch(c, "bicg_p", [&] { bicg_p_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(v.r, v.v, v.p, n, sc); });
-            precondition<T>(c, an, v.p, v.ph, sc, 0);
-            launch(c, "bicg_spmv_alpha", [&] {
-                bicg_spmv_alpha_kernel<T><<<nb, kThreads, 0, c.stream>>>(L0.rowptr->as<int>(), L0.col->as<int>(), a,
-                                                                        v.ph, v.rhat, v.v, n, part, cnt, sc);
-            });
-            launch(c, "bicg_s",
-                   [&] { bicg_s_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.r, v.v, v.s, n, part, cnt, sc); });
-            precondition<T>(c, an, v.s, v.sh, sc, 1);
-            launch(c, "bicg_spmv_omega", [&] {
-                bicg_spmv_omega_kernel<T><<<nb, kThreads, 0, c.stream>>>(L0.rowptr->as<int>(), L0.col->as<int>(), a,
-                                                                        v.sh, v.s, v.t, n, part, cnt, sc);
-            });
-            launch(c, "bicg_xr", [&] {
-                bicg_xr_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.ph, v.sh, v.s, v.t, v.rhat, v.x, v.r, n, part, cnt,
-                                                                sc);
-            });
+        if (graphs && chunk == g.chunk) {
+            EQG_CUDA(cudaGraphLaunch(g.exec, c.stream));
+            c.launches += g.kernels;
+        } else {
+            for (int k = 0; k < chunk; ++k) iteration();
         }
         enq += chunk;
         EQG_CUDA(cudaMemcpyAsync(c.pinned, sc, sizeof(KScal), cudaMemcpyDeviceToHost, c.stream));
@@ -1077,6 +1223,10 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     }
     EQG_CUDA(cudaMemsetAsync(an.factor_status->ptr, 0, sizeof(int), c.stream));
     for (auto& L : an.levels) {
+        launch(c, "sell_scatter", [&] {
+            sell_scatter_kernel<<<blocksFor(L.sell_size), kThreads, 0, c.stream>>>(
+                L.sell_size, L.sell_map->as<int>(), L.a64->as<double>(), L.as64->as<double>());
+        });
         if (L.coarsest) {
             launch(c, "mg_dense_inverse", [&] {
                 dense_inverse_kernel<<<1, 1024, 0, c.stream>>>(L.n, L.rowptr->as<int>(), L.col->as<int>(),
@@ -1085,6 +1235,10 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
             });
         } else {
             factor_level(c, L, an.factor_status->as<int>());
+            launch(c, "sell_scatter", [&] {
+                sell_scatter_kernel<<<blocksFor(L.sell_size), kThreads, 0, c.stream>>>(
+                    L.sell_size, L.sell_map->as<int>(), L.lu64->as<double>(), L.lus64->as<double>());
+            });
         }
     }
     Vecs<double> v = vecs<double>(an.vec64->as<double>(), n);
@@ -1092,9 +1246,9 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
            [&] { permute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(rhs, L0.perm->as<int>(), v.b, n); });
     if (mixed) {
         for (auto& L : an.levels) {
-            to_float(c, L.a64, L.a32, L.nnz);
+            to_float(c, L.as64, L.as32, L.sell_size);
             if (L.coarsest) to_float(c, L.inv64, L.inv32, (int64_t)L.n * L.n);
-            else to_float(c, L.lu64, L.lu32, L.nnz);
+            else to_float(c, L.lus64, L.lus32, L.sell_size);
             if (!L.v32) L.v32 = c.allocN<float>((size_t)4 * (L.n > 0 ? L.n : 1));
         }
         if (!an.vec32) an.vec32 = c.allocN<float>((size_t)10 * n);
@@ -1108,7 +1262,7 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     c.krylov_clock.start(c.stream);
 
     if (!mixed) {
-        res = bicgstab<double>(c, an, L0.a64->as<double>(), v, tol, max_iter, check_every);
+        res = bicgstab<double>(c, an, L0.as64->as<double>(), v, tol, max_iter, check_every);
         res.sweeps = 1;
     } else {
         Vecs<float> w = vecs<float>(an.vec32->as<float>(), n);
@@ -1121,11 +1275,10 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         Buf rr_dev = c.allocN<double>(2);
         launch(c, "sumsq",
                [&] { sumsq_kernel<<<nb, kThreads, 0, c.stream>>>(v.b, n, part, cnt, rr_dev->as<double>()); });
-        launch(c, "residual", [&] {
-            residual_kernel<<<nb, kThreads, 0, c.stream>>>(L0.rowptr->as<int>(), L0.col->as<int>(),
-                                                           L0.a64->as<double>(), v.x, v.b, v.r, w.b, n, part, cnt,
-                                                           rr_dev->as<double>() + 1);
-        });
+        WITH_KMAX(L0.kmax, launch(c, "residual", [&] {
+            residual_kernel<KK><<<nb, kThreads, 0, c.stream>>>(L0.view(), L0.as64->as<double>(), v.x, v.b, v.r, w.b, n,
+                                                               part, cnt, rr_dev->as<double>() + 1);
+        }));
         EQG_CUDA(cudaMemcpyAsync(c.pinned, rr_dev->ptr, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
         c.sync();
         const double bb = c.pinned[0];
@@ -1133,17 +1286,16 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         int total_iter = 0, sweeps = 0;
         bool conv = bb == 0.0 || rr <= tol * tol * bb;
         while (!conv && sweeps < max_sweeps && total_iter < max_iter) {
-            SolveResult inner = bicgstab<float>(c, an, L0.a32->as<float>(), w, inner_tol, max_iter - total_iter,
+            SolveResult inner = bicgstab<float>(c, an, L0.as32->as<float>(), w, inner_tol, max_iter - total_iter,
                                                 check_every);
             total_iter += inner.iterations;
             ++sweeps;
             launch(c, "add_float",
                    [&] { add_float_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, w.x, n); });
-            launch(c, "residual", [&] {
-                residual_kernel<<<nb, kThreads, 0, c.stream>>>(L0.rowptr->as<int>(), L0.col->as<int>(),
-                                                               L0.a64->as<double>(), v.x, v.b, v.r, w.b, n, part, cnt,
-                                                               rr_dev->as<double>() + 1);
-            });
+            WITH_KMAX(L0.kmax, launch(c, "residual", [&] {
+                residual_kernel<KK><<<nb, kThreads, 0, c.stream>>>(L0.view(), L0.as64->as<double>(), v.x, v.b, v.r,
+                                                                   w.b, n, part, cnt, rr_dev->as<double>() + 1);
+            }));
             EQG_CUDA(cudaMemcpyAsync(c.pinned, rr_dev->as<double>() + 1, sizeof(double), cudaMemcpyDeviceToHost,
                                      c.stream));
             c.sync();

@@ -17,6 +17,7 @@ class SimReport(C.Structure):
         ("total_ms", C.c_double),
         ("stats", capi.Stats),
         ("error", C.c_char * 512),
+        ("profile", C.c_char * 16384),
     ]
 
 

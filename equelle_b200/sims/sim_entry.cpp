@@ -25,6 +25,7 @@ struct eqg_sim_report {
     double total_ms;            // first solve start to last solve end
     eqg_stats stats;
     char error[512];
+    char profile[16384];        // eqg_runtime_kernel_profile JSON
 };
 
 int eqg_sim_main(int argc, char** argv, eqg_sim_report* report)
@@ -72,6 +73,8 @@ int eqg_sim_main(int argc, char** argv, eqg_sim_report* report)
         report->solves = k;
         if (first_start >= 0) equelle::detail::check(eqg_runtime_elapsed_ms(rt, first_start, last_end, &report->total_ms));
         equelle::detail::check(eqg_runtime_stats(rt, &report->stats));
+        int64_t need = 0;
+        equelle::detail::check(eqg_runtime_kernel_profile(rt, report->profile, sizeof(report->profile), &need));
         note("done");
         return 0;
     } catch (const std::exception& e) {

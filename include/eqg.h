@@ -113,7 +113,7 @@ const char* eqg_backend_name(void);
  * ilu0), linsolver_ordering (multicolor | natural),
  * linsolver_precision (double | mixed), linsolver_inner_tolerance (1e-4),
  * linsolver_max_sweeps (60), linsolver_check_every (8), time_kernel
- * (name of one kernel to time with CUDA events) and device (CUDA device
+ * (a kernel name, or "*", to time with CUDA events) and device (CUDA device
  * index; default: the calling thread's current device).  grid_filename is
  * rejected with EQG_ERR_UNSUPPORTED.
  * Replaces EquelleRuntimeCPU::EquelleRuntimeCPU(const ParameterGroup&)
@@ -125,6 +125,11 @@ int eqg_runtime_grid_info(const eqg_runtime* rt, eqg_grid_info* out);
 int eqg_runtime_synchronize(eqg_runtime* rt);
 int eqg_runtime_stats(const eqg_runtime* rt, eqg_stats* out);
 int eqg_runtime_reset_stats(eqg_runtime* rt);
+/* Device time per kernel name, as JSON {"name": [launches, ms], ...}, of
+ * the launches timed under the parameter time_kernel (a name, or "*" for
+ * every kernel).  Writes at most len bytes (NUL terminated) and the size
+ * needed to *needed. */
+int eqg_runtime_kernel_profile(const eqg_runtime* rt, char* buf, int64_t len, int64_t* needed);
 /* Timing marks: records an event on the runtime's stream (device clock for
  * the product, host steady clock for the oracle) and returns its id. */
 int eqg_runtime_mark(eqg_runtime* rt, int* mark_id);

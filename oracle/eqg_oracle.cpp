@@ -842,6 +842,15 @@ int eqg_runtime_reset_stats(eqg_runtime* rt)
     });
 }
 
+int eqg_runtime_kernel_profile(const eqg_runtime* rt, char* buf, int64_t len, int64_t* needed)
+{
+    return guarded([&] {
+        need(rt, "runtime");
+        *needed = 3;  // the oracle launches no kernels: "{}"
+        if (buf && len > 0) std::snprintf(buf, (size_t)len, "{}");
+    });
+}
+
 int eqg_runtime_mark(eqg_runtime* rt, int* mark_id)
 {
     return guarded([&] {
