@@ -370,7 +370,7 @@ def reference_counts(a):
         with open(path) as f:
             d = json.load(f)
         if a.workload in d:
-            return d[a.workload]
+            return {k: float(v) for k, v in d[a.workload].items()}
     return {"residuals": 5.0, "solves": 4.0, "krylov": 400.0}
 
 
