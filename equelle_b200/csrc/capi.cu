@@ -17,6 +17,7 @@
 
 namespace eqg {
 void build_grid(Core& c, eqg_set** builtin);
+void set_last_error(const std::string& msg);
 }
 
 using namespace eqg;
@@ -310,6 +311,9 @@ int mark(Core& c)
 }
 
 }  // namespace
+
+// Lets the library's other C entry points report through eqg_last_error().
+void eqg::set_last_error(const std::string& msg) { g_last_error = msg; }
 
 extern "C" {
 
