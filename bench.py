@@ -9,7 +9,7 @@ generated-style C++ simulator equelle_b200/sims/twophase.cpp linked to
 libeqg.so and called in this process.
 
     python bench.py [--gpus N] [--steps K] [--warmup W]
-                    [--impl ours|reference] [--precision double|mixed]
+                    [--impl ours|reference] [--precision double|mixed|refine]
                     [--workload twophase3d|twophase2d|heat] [--nx --ny --nz]
 
 `value` (time steps/s) is timed on the device clock between the runtime's
@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["double", "mixed"], default="double")
+    ap.add_argument("--precision", choices=["double", "mixed", "refine"], default="double")
     ap.add_argument("--ordering", choices=["multicolor", "natural"], default="multicolor")
     ap.add_argument("--workload", choices=["twophase3d", "twophase2d", "heat"], default="twophase3d")
     ap.add_argument("--nx", type=int)
@@ -271,7 +271,7 @@ def main():
     # algorithmic bytes per launch; its launches are timed with CUDA events
     # in a second, short run of the same workload (timing every launch with
     # events disables the CUDA graphs of the timed run)
-    if a.precision == "double":
+    if a.precision != "refine":  # FP64 BiCGStab (mixed: only the preconditioner is FP32)
         kbytes = 12 * nnz + 4 * (n_rows + 1) + 3 * 8 * n_rows
     else:
         kbytes = 8 * nnz + 4 * (n_rows + 1) + 3 * 4 * n_rows

@@ -24,7 +24,9 @@
 // keeps the iteration count of the elliptic pressure part from growing with
 // the grid; "ilu0": the staged ILU(0) alone.
 //
-// Precision "mixed": the inner BiCGStab and the preconditioner run in FP32,
+// Precision "mixed": BiCGStab in FP64, the preconditioner (V-cycle or ILU
+// sweeps, with FP32 copies of the factors and level matrices) in FP32.
+// Precision "refine": the inner BiCGStab and the preconditioner in FP32,
 // inside FP64 iterative refinement (r = b - A x in FP64 with FP64 A).
 //
 // Every kernel of an iteration reads a device-side status word first and
@@ -606,6 +608,21 @@ __global__ void dense_apply_kernel(int n, const T* __restrict__ inv, const T* __
     }
 }
 
+// FP64 <-> FP32 copies around an FP32 preconditioner.
+__global__ void pc_to_f32_kernel(const double* __restrict__ a, float* __restrict__ b, int n, const KScal* sc,
+                                 int skip_if_s)
+{
+    if (mg_skip(sc, skip_if_s)) return;
+    GRID_STRIDE(i, n) b[i] = (float)a[i];
+}
+
+__global__ void pc_to_f64_kernel(const float* __restrict__ a, double* __restrict__ b, int n, const KScal* sc,
+                                 int skip_if_s)
+{
+    if (mg_skip(sc, skip_if_s)) return;
+    GRID_STRIDE(i, n) b[i] = (double)a[i];
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -655,12 +672,14 @@ struct SolverAnalysis {
     std::vector<Level> levels;
     Buf vmap;        // level-0 permuted entry <- Jacobian entry
     Buf vec64, vec32, scal, partials, counter, factor_status;
-    // CUDA graphs of `chunk` BiCGStab iterations, [0] FP64 and [1] FP32
+    Buf pc32;        // FP32 input and output of an FP32 preconditioner
+    // CUDA graphs of `chunk` BiCGStab iterations: [0] FP64, [1] FP32, [2] FP64
+    // with an FP32 preconditioner
     struct IterGraph {
         cudaGraphExec_t exec = nullptr;
         int chunk = 0;
         int64_t kernels = 0;
-    } graph[2];
+    } graph[3];
     ~SolverAnalysis()
     {
         for (auto& g : graph)
@@ -1078,10 +1097,36 @@ void precondition(Core& c, const SolverAnalysis& an, const T* in, T* out, const 
     else ilu_apply<T>(c, an.levels[0], in, out, sc, skip_if_s);
 }
 
+// out = M^{-1} in with the FP32 copy of the preconditioner, for FP64 vectors.
+void precondition_f32(Core& c, const SolverAnalysis& an, const double* in, double* out, const KScal* sc, int skip_if_s)
+{
+    const int n = an.n;
+    float* in32 = an.pc32->as<float>();
+    float* out32 = in32 + n;
+    launch(c, "pc_to_f32",
+           [&] { pc_to_f32_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(in, in32, n, sc, skip_if_s); });
+    precondition<float>(c, an, in32, out32, sc, skip_if_s);
+    launch(c, "pc_to_f64",
+           [&] { pc_to_f64_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(out32, out, n, sc, skip_if_s); });
+}
+
+template <class T>
+void apply_pc(Core& c, const SolverAnalysis& an, const T* in, T* out, const KScal* sc, int skip_if_s, bool pc32)
+{
+    if constexpr (sizeof(T) == sizeof(double)) {
+        if (pc32) {
+            precondition_f32(c, an, in, out, sc, skip_if_s);
+            return;
+        }
+    }
+    precondition<T>(c, an, in, out, sc, skip_if_s);
+}
+
 // BiCGStab on the permuted system with values a; v.b holds the right-hand
 // side.
 template <class T>
-SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double tol, int max_iter, int check_every)
+SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double tol, int max_iter, int check_every,
+                     bool pc32 = false)
 {
     const int n = an.n;
     const Level& L0 = an.levels[0];
@@ -1094,13 +1139,13 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double 
     });
     auto iteration = [&] {
         launch(c, "bicg_p", [&] { bicg_p_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(v.r, v.v, v.p, n, sc); });
-        precondition<T>(c, an, v.p, v.ph, sc, 0);
+        apply_pc<T>(c, an, v.p, v.ph, sc, 0, pc32);
         WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_alpha", [&] {
             bicg_spmv_alpha_kernel<KK, T><<<nb, kThreads, 0, c.stream>>>(L0.view(), a, v.ph, v.rhat, v.v, n, part, cnt,
                                                                         sc);
         }));
         launch(c, "bicg_s", [&] { bicg_s_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.r, v.v, v.s, n, part, cnt, sc); });
-        precondition<T>(c, an, v.s, v.sh, sc, 1);
+        apply_pc<T>(c, an, v.s, v.sh, sc, 1, pc32);
         WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_omega", [&] {
             bicg_spmv_omega_kernel<KK, T><<<nb, kThreads, 0, c.stream>>>(L0.view(), a, v.sh, v.s, v.t, n, part, cnt,
                                                                         sc);
@@ -1114,7 +1159,7 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double 
     // scalars in device memory).  Kernel timing (time_kernel) needs one
     // event pair per launch, so timed runs launch eagerly.
     const bool graphs = c.timed_kernel.empty() && c.param_i("linsolver_graphs", 1) != 0;
-    SolverAnalysis::IterGraph& g = an.graph[sizeof(T) == sizeof(double) ? 0 : 1];
+    SolverAnalysis::IterGraph& g = an.graph[sizeof(T) == sizeof(double) ? (pc32 ? 2 : 0) : 1];
     if (graphs && (!g.exec || g.chunk != check_every)) {
         if (g.exec) {
             cudaGraphExecDestroy(g.exec);
@@ -1192,7 +1237,9 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     if (!natural && ordering != "multicolor") fail(EQG_ERR_ARG, "linsolver_ordering must be natural or multicolor");
     const std::string precision = c.param_s("linsolver_precision", "double");
     const bool mixed = precision == "mixed";
-    if (!mixed && precision != "double") fail(EQG_ERR_ARG, "linsolver_precision must be double or mixed");
+    const bool refine = precision == "refine";
+    if (!mixed && !refine && precision != "double")
+        fail(EQG_ERR_ARG, "linsolver_precision must be double, mixed or refine");
     const double tol = c.param_d("linsolver_residual_tolerance", 1e-8);
     const int max_iter = c.param_i("linsolver_max_iterations", 1000);
     const int check_every = std::max(1, c.param_i("linsolver_check_every", 8));
@@ -1244,14 +1291,15 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     Vecs<double> v = vecs<double>(an.vec64->as<double>(), n);
     launch(c, "permute",
            [&] { permute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(rhs, L0.perm->as<int>(), v.b, n); });
-    if (mixed) {
+    if (mixed || refine) {
         for (auto& L : an.levels) {
             to_float(c, L.as64, L.as32, L.sell_size);
             if (L.coarsest) to_float(c, L.inv64, L.inv32, (int64_t)L.n * L.n);
             else to_float(c, L.lus64, L.lus32, L.sell_size);
             if (!L.v32) L.v32 = c.allocN<float>((size_t)4 * (L.n > 0 ? L.n : 1));
         }
-        if (!an.vec32) an.vec32 = c.allocN<float>((size_t)10 * n);
+        if (refine && !an.vec32) an.vec32 = c.allocN<float>((size_t)10 * n);
+        if (mixed && !an.pc32) an.pc32 = c.allocN<float>((size_t)2 * n);
     }
     c.factor_clock.stop(c.stream);
     int fstat = 0;
@@ -1261,8 +1309,8 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     if (fstat) return res;  // zero pivot
     c.krylov_clock.start(c.stream);
 
-    if (!mixed) {
-        res = bicgstab<double>(c, an, L0.as64->as<double>(), v, tol, max_iter, check_every);
+    if (!refine) {
+        res = bicgstab<double>(c, an, L0.as64->as<double>(), v, tol, max_iter, check_every, mixed);
         res.sweeps = 1;
     } else {
         Vecs<float> w = vecs<float>(an.vec32->as<float>(), n);

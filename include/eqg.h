@@ -111,8 +111,9 @@ const char* eqg_backend_name(void);
  * linsolver_residual_tolerance (1e-8), linsolver_max_iterations (1000).
  * The device library also reads linsolver_preconditioner (multigrid |
  * ilu0), linsolver_ordering (multicolor | natural),
- * linsolver_precision (double | mixed), linsolver_inner_tolerance (1e-4),
- * linsolver_max_sweeps (60), linsolver_check_every (8), time_kernel
+ * linsolver_precision (double | mixed: FP32 preconditioner | refine: FP32
+ * BiCGStab inside FP64 refinement), linsolver_inner_tolerance (1e-4) and
+ * linsolver_max_sweeps (60) for refine, linsolver_check_every (8), time_kernel
  * (a kernel name, or "*", to time with CUDA events) and device (CUDA device
  * index; default: the calling thread's current device).  grid_filename is
  * rejected with EQG_ERR_UNSUPPORTED.

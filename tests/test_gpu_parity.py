@@ -77,13 +77,16 @@ def test_heat_64x64_parity(gpu_lib, oracle_lib, ordering, precond):
 
 @pytest.mark.parametrize("shape,precision,precond", [((16, 16, None), "double", "multigrid"),
                                                      ((16, 16, None), "mixed", "multigrid"),
+                                                     ((16, 16, None), "refine", "multigrid"),
                                                      ((8, 8, 4), "double", "multigrid"),
                                                      ((8, 8, 4), "mixed", "multigrid"),
                                                      ((16, 16, 8), "double", "multigrid"),
-                                                     ((16, 16, 8), "mixed", "ilu0")])
+                                                     ((16, 16, 8), "mixed", "ilu0"),
+                                                     ((16, 16, 8), "refine", "ilu0")])
 def test_two_phase_parity(gpu_lib, oracle_lib, shape, precision, precond):
     """Fully implicit two-phase flow: saturation within 1e-8 relative of the
-    FP64 oracle after every step, in plain FP64 and in mixed precision."""
+    FP64 oracle after every step, in plain FP64, with the FP32 preconditioner
+    (mixed) and with FP32 BiCGStab inside FP64 refinement (refine)."""
     grid, case = programs.two_phase_case(*shape, steps=3)
     params = dict(grid, abs_res_tol=1e-11, linsolver_residual_tolerance=1e-12, linsolver_max_iterations=5000)
     eg = Runtime(gpu_lib, dict(params, linsolver_precision=precision, linsolver_preconditioner=precond))
@@ -92,5 +95,7 @@ def test_two_phase_parity(gpu_lib, oracle_lib, shape, precision, precond):
     for step, ((pg, sg), (po, so)) in enumerate(zip(og, oo)):
         assert np.max(np.abs(sg - so) / np.abs(so)) <= 1e-8, "Sw step %d" % step
         assert np.max(np.abs(pg - po)) <= 1e-8 * np.max(np.abs(po)), "p step %d" % step
-    if precision == "mixed":
-        assert eg.stats()["refinement_sweeps"] > 0
+    st = eg.stats()
+    if precision == "refine":
+        assert st["refinement_sweeps"] >= st["linear_solves"] > 0
+
