@@ -266,15 +266,17 @@ def main():
     value = world * K / (ms / 1000.0)
     st = rep.stats
     n_rows, nnz = st.last_matrix_rows, st.last_matrix_nnz
+    bsz, nblk = max(st.last_block_size, 1), st.last_matrix_blocks or st.last_matrix_nnz
 
     # roofline of the BiCGStab SpMV t = A s fused with the (t,s), (t,t) dots:
-    # algorithmic bytes per launch; its launches are timed with CUDA events
-    # in a second, short run of the same workload (timing every launch with
-    # events disables the CUDA graphs of the timed run)
-    if a.precision != "refine":  # FP64 BiCGStab (mixed: only the preconditioner is FP32)
-        kbytes = 12 * nnz + 4 * (n_rows + 1) + 3 * 8 * n_rows
-    else:
-        kbytes = 8 * nnz + 4 * (n_rows + 1) + 3 * 4 * n_rows
+    # algorithmic bytes per launch = the block values (bsz^2 per block), one
+    # 4-byte column index per block, one 4-byte length per block row, and
+    # the vectors sh (gathered), s (dotted) and t (written);
+    # its launches are timed with CUDA events in a second, short run of the
+    # same workload (timing every launch with events disables the CUDA
+    # graphs of the timed run)
+    esize = 4 if a.precision == "refine" else 8  # mixed: only the preconditioner is FP32
+    kbytes = esize * bsz * bsz * nblk + 4 * nblk + 4 * (n_rows // bsz) + 3 * esize * n_rows
     prof = json.loads(rep.profile.decode() or "{}")
     if SPMV_KERNEL not in prof:
         d3 = input_dir(key, 2, rank)
@@ -299,7 +301,7 @@ def main():
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if a.precision == "double" else "f64+f32",
         "data": "synthetic (seeded Gaussian-random-field log-permeability, corner wells)",
-        "config": config(a, desc, cells),
+        "config": dict(config(a, desc, cells), ilu_blocks="%dx%d" % (bsz, bsz)),
         "newton_iterations_per_step": infos["newton"] / K,
         "krylov_iterations_per_step": infos["krylov"] / K,
         "cell_updates_per_s": world * K * cells / (ms / 1000.0),
@@ -348,7 +350,7 @@ def main():
 
 def config(a, desc, cells):
     return {"workload": desc, "cells": cells, "precision": a.precision, "ordering": a.ordering,
-            "dt": "1 day" if a.workload != "heat" else "0.5", "solver": "Newton + BiCGStab/ILU(0)",
+            "dt": "1 day" if a.workload != "heat" else "0.5", "solver": "Newton + BiCGStab, V-cycle with block ILU(0) smoothers",
             "l2": "working set larger than L2 (126 MB), no flush", "parallelism": "replicas"}
 
 

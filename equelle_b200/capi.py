@@ -52,6 +52,7 @@ class Stats(C.Structure):
         ("timed_kernel_launches", C.c_int64), ("timed_kernel_ms", C.c_double),
         ("residual_evaluations", C.c_int64), ("residual_ms", C.c_double),
         ("factor_ms", C.c_double), ("krylov_ms", C.c_double),
+        ("last_block_size", C.c_int64), ("last_matrix_blocks", C.c_int64),
     ]
 
     def as_dict(self):

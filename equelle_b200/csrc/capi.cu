@@ -423,6 +423,8 @@ int eqg_runtime_stats(const eqg_runtime* rt, eqg_stats* out)
         out->last_linear_residual = c.solver.last_residual;
         out->last_matrix_rows = c.solver.last_rows;
         out->last_matrix_nnz = c.solver.last_nnz;
+        out->last_block_size = c.solver.last_block_size;
+        out->last_matrix_blocks = c.solver.last_blocks;
         out->timed_kernel_launches = (int64_t)c.timer_pairs.size();
         double ms = 0.0;
         for (auto& pr : c.timer_pairs) {
@@ -1186,6 +1188,8 @@ int eqg_solve_for_update(eqg_runtime* rt, const eqg_coll* residual, eqg_coll** d
         c.solver.last_residual = r.rel_residual;
         c.solver.last_rows = residual->pat->rows;
         c.solver.last_nnz = residual->pat->nnz;
+        c.solver.last_block_size = r.block_size;
+        c.solver.last_blocks = r.blocks;
         if (c.verbose > 2)
             std::printf("        solveForUpdate: BiCGStab+ILU0 %d iterations (%d sweeps), rel. residual %g\n",
                         r.iterations, r.sweeps, r.rel_residual);

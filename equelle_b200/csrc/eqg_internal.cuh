@@ -84,6 +84,7 @@ struct SolverStats {
     int64_t linear_solves = 0, krylov_iterations = 0, refinement_sweeps = 0;
     double last_residual = 0.0;
     int64_t last_rows = 0, last_nnz = 0;
+    int64_t last_block_size = 0, last_blocks = 0;
 };
 
 struct Mark {
@@ -313,6 +314,8 @@ struct SolveResult {
     int iterations = 0;
     int sweeps = 0;
     double rel_residual = 0.0;
+    int block_size = 1;   // layout of the system in the preconditioner
+    int64_t blocks = 0;   // block entries of the matrix pattern
 };
 SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const double* rhs, double* x);
 

@@ -2,27 +2,37 @@
 // Opm::LinearSolverFactory::solve from solveForUpdate,
 // EquelleRuntimeCPU.cpp:413-440).
 //
-// Method: BiCGStab (van der Vorst 1992) right-preconditioned with ILU(0)
-// (Saad, Iterative Methods for Sparse Linear Systems, Alg. 10.4), from x = 0,
+// Method: BiCGStab (van der Vorst 1992) right-preconditioned, from x = 0,
 // converged when ||b - A x|| <= tol * ||b||, with a fixed pseudo-random
 // shadow residual (shadow_entry).
 //
-// Parallel ILU(0): rows are reordered symmetrically so that each "stage" is a
-// contiguous block of rows with no couplings inside it; factorization and
-// both triangular solves then run one kernel per stage, a thread per row.
-//   - ordering "natural": stages are the wavefront levels of the natural
-//     order (symmetrised pattern), which reproduces natural-order ILU(0)
-//     exactly (the oracle's preconditioner), at the price of many stages;
-//   - ordering "multicolor" (default): greedy colouring of the symmetrised
-//     pattern; a 7-point stencil gives 2 colours per unknown block, so a
-//     handful of stages of ~n/colors rows each.
-// The analysis (ordering, permuted pattern, value map) is computed on the
-// host once per Jacobian pattern and cached with it.
+// Block structure: Equelle's newtonSolveSystem stacks its unknowns as
+// `ncomp` collections over all cells, so unknown comp * ncells + cell belongs
+// to grid cell `cell`.  For ncomp = 2 or 3 the solver works on ncomp x ncomp
+// blocks, one block row per cell (all unknowns of a cell together); with
+// ncomp = 1, with the natural ordering, or when the unknowns do not cover
+// every cell, the blocks are 1 x 1 (one block row per unknown).
+//
+// Preconditioner: block ILU(0) (Saad, Iterative Methods for Sparse Linear
+// Systems, sec. 10.3, in its block form, as in OPM's BILU0), with the block
+// rows reordered symmetrically so that each "stage" is a contiguous range of
+// block rows with no couplings inside it:
+//   - ordering "multicolor" (default): greedy colouring of the block graph;
+//     the 7-point (5-point) cell graph takes two colours, so a sweep is two
+//     stages;
+//   - ordering "natural" (1 x 1 blocks): wavefront levels of the natural
+//     order, which reproduces natural-order ILU(0), the oracle's
+//     preconditioner, at the price of many stages.
+// Factorization and both triangular sweeps run one kernel per stage, one
+// thread per block row.  Rows of the first stage have no lower part (their
+// forward-sweep value is the right-hand side itself) and rows of the last
+// stage have no upper part (the forward sweep finishes them), so a sweep
+// over S stages takes S kernels.
 //
 // Preconditioner "multigrid" (default; see the analysis section below):
-// geometric-aggregation V-cycle with these ILU(0) sweeps as smoothers, which
-// keeps the iteration count of the elliptic pressure part from growing with
-// the grid; "ilu0": the staged ILU(0) alone.
+// geometric-aggregation V-cycle with these block ILU(0) sweeps as smoothers,
+// which keeps the iteration count of the elliptic pressure part from growing
+// with the grid; "ilu0": the staged block ILU(0) alone.
 //
 // Precision "mixed": BiCGStab in FP64, the preconditioner (V-cycle or ILU
 // sweeps, with FP32 copies of the factors and level matrices) in FP32.
@@ -35,6 +45,7 @@
 #include "eqg_internal.cuh"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -123,58 +134,187 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NV], double* partials, unsi
     return true;
 }
 
-// ---- matrix kernels ---------------------------------------------------------
-// Level matrices used by the sweeps are in a sliced ELL layout: rows in
-// slices of 32 (one warp), each slice stored column-major and padded to its
-// longest row, so that a warp's k-th loads of its 32 rows are one contiguous
-// 256-byte (FP64) segment.  Within a row, entries are in ascending column
-// order, so the ILU(0) lower part is k < dk[r] and the upper part k > dk[r].
+// ---- block matrices -----------------------------------------------------------
+// Level matrices are in a block sliced ELL layout: block rows in slices of
+// 32 (one warp), each slice stored by position k in the row and padded to
+// its longest row.  Slot q = slice_ptr[R / 32] + 32 k + R % 32 holds the
+// block column col[q] of the k-th block of block row R; the B x B values of
+// that block (row-major, e = i B + j) are at
+//     (slice_ptr[R / 32] + 32 k) B^2 + 32 e + R % 32,
+// so that a warp's loads of value e at position k are one contiguous
+// segment.  Within a row, blocks are in ascending column order, so the
+// ILU(0) lower part is k < dk[R] and the upper part k > dk[R].  Vectors are
+// in block-row order: unknown c of block row R is at R B + c.
 struct SellView {
     const int* __restrict__ slice_ptr;  // first slot of each slice
-    const int* __restrict__ col;        // column of each slot
-    const int* __restrict__ len;        // entries of each row
-    const int* __restrict__ dk;         // position of the diagonal in each row
+    const int* __restrict__ col;        // block column of each slot
+    const int* __restrict__ len;        // blocks of each block row
+    const int* __restrict__ dk;         // position of the diagonal block in each row
 };
 
-__device__ __forceinline__ int sell_base(const SellView& m, int r) { return m.slice_ptr[r >> 5] + (r & 31); }
-
-// sum_{k0 <= k < k1} a[row, k] x[col[row, k]], added in ascending k.  With
-// KM > 0 (rows of at most KM entries) the loop is unrolled so that a thread
-// issues all its column and value loads before the dependent gathers of x:
-// the kernels using it are bound by the latency of that load chain.
-template <int KM, class T>
-__device__ __forceinline__ double sell_dot(const SellView& m, int base, int k0, int k1, const T* __restrict__ a,
-                                           const T* __restrict__ x)
+template <int B, class T>
+__device__ __forceinline__ void load_bvec(const T* __restrict__ x, int J, double (&v)[B])
 {
-    double acc = 0.0;
-    if (KM == 0) {
-        for (int k = k0; k < k1; ++k) {
-            const int idx = base + (k << 5);
-            acc += (double)a[idx] * (double)x[m.col[idx]];
-        }
-        return acc;
-    }
-    int ci[KM > 0 ? KM : 1];
-    T av[KM > 0 ? KM : 1];
+    if constexpr (B == 2 && sizeof(T) == 8) {
+        const double2 t = reinterpret_cast<const double2*>(x)[J];
+        v[0] = t.x;
+        v[1] = t.y;
+    } else if constexpr (B == 2 && sizeof(T) == 4) {
+        const float2 t = reinterpret_cast<const float2*>(x)[J];
+        v[0] = (double)t.x;
+        v[1] = (double)t.y;
+    } else {
 #pragma unroll
-    for (int k = 0; k < KM; ++k) {
-        const bool on = k >= k0 && k < k1;
-        const int idx = base + (k << 5);
-        ci[k] = on ? m.col[idx] : 0;
-        av[k] = on ? a[idx] : (T)0;
+        for (int c = 0; c < B; ++c) v[c] = (double)x[J * B + c];
     }
-#pragma unroll
-    for (int k = 0; k < KM; ++k)
-        if (k >= k0 && k < k1) acc += (double)av[k] * (double)x[ci[k]];
-    return acc;
 }
 
-// Dispatches on a level's longest row as KK (4, 8, 16; 0 = plain loop).
+template <int B, class T>
+__device__ __forceinline__ void store_bvec(T* __restrict__ x, int R, const double (&v)[B])
+{
+#pragma unroll
+    for (int c = 0; c < B; ++c) x[R * B + c] = (T)v[c];
+}
+
+// acc += sum_{k0 <= k < k1} A_{R,k} x_{col(R,k)}, blocks in ascending k and
+// within a block in ascending j.  x_J is read from `x` when J < split and
+// from `x2` otherwise.  With KM > 0 (rows of at most KM blocks) the loop is
+// unrolled so that a thread issues its column loads before the dependent
+// gathers of x: the kernels using it are bound by the latency of that chain.
+template <int B, int KM, class T>
+__device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int k0, int k1, const T* __restrict__ a,
+                                     const T* __restrict__ x, const T* __restrict__ x2, int split, double (&acc)[B])
+{
+    constexpr int BB = B * B;
+    if constexpr (KM == 0) {
+        for (int k = k0; k < k1; ++k) {
+            const int q = sbase + (k << 5);
+            const int J = m.col[q + lane];
+            double xv[B];
+            load_bvec<B, T>(J < split ? x : x2, J, xv);
+            const T* av = a + (size_t)q * BB + lane;
+#pragma unroll
+            for (int i = 0; i < B; ++i)
+#pragma unroll
+                for (int j = 0; j < B; ++j) acc[i] += (double)av[(i * B + j) << 5] * xv[j];
+        }
+    } else if constexpr (KM * BB <= 32) {
+        // columns and values of the whole row first (predicated loads), then
+        // the gathers of x
+        int ci[KM];
+        T av[KM][BB];
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            const bool on = k >= k0 && k < k1;
+            const int q = sbase + (k << 5);
+            ci[k] = on ? m.col[q + lane] : 0;
+#pragma unroll
+            for (int e = 0; e < BB; ++e) av[k][e] = on ? a[(size_t)q * BB + (e << 5) + lane] : (T)0;
+        }
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            if (k >= k0 && k < k1) {
+                double xv[B];
+                load_bvec<B, T>(ci[k] < split ? x : x2, ci[k], xv);
+#pragma unroll
+                for (int i = 0; i < B; ++i)
+#pragma unroll
+                    for (int j = 0; j < B; ++j) acc[i] += (double)av[k][i * B + j] * xv[j];
+            }
+        }
+    } else {
+        int ci[KM];
+#pragma unroll
+        for (int k = 0; k < KM; ++k) ci[k] = (k >= k0 && k < k1) ? m.col[sbase + (k << 5) + lane] : 0;
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            if (k >= k0 && k < k1) {
+                const int q = sbase + (k << 5);
+                double xv[B];
+                load_bvec<B, T>(ci[k] < split ? x : x2, ci[k], xv);
+                const T* av = a + (size_t)q * BB + lane;
+#pragma unroll
+                for (int i = 0; i < B; ++i)
+#pragma unroll
+                    for (int j = 0; j < B; ++j) acc[i] += (double)av[(i * B + j) << 5] * xv[j];
+            }
+        }
+    }
+}
+
+// y = D x for the block at slot position `q` (its first value at
+// a[q B^2 + lane], values 32 apart).
+template <int B, class T>
+__device__ __forceinline__ void bmatvec(const T* __restrict__ a, int q, int lane, const double (&x)[B], double (&y)[B])
+{
+    const T* av = a + (size_t)q * (B * B) + lane;
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < B; ++j) s += (double)av[(i * B + j) << 5] * x[j];
+        y[i] = s;
+    }
+}
+
+// In-place inverse of a B x B block by Gauss-Jordan elimination with
+// partial pivoting; false when a pivot is zero or not finite.
+template <int B>
+__device__ __forceinline__ bool invert_block(double (&a)[B * B])
+{
+    double v[B * B];
+#pragma unroll
+    for (int i = 0; i < B; ++i)
+#pragma unroll
+        for (int j = 0; j < B; ++j) v[i * B + j] = i == j ? 1.0 : 0.0;
+#pragma unroll
+    for (int c = 0; c < B; ++c) {
+        int p = c;
+        double best = fabs(a[c * B + c]);
+#pragma unroll
+        for (int r = c + 1; r < B; ++r)
+            if (fabs(a[r * B + c]) > best) {
+                best = fabs(a[r * B + c]);
+                p = r;
+            }
+        if (!(best > 0.0) || !isfinite(best)) return false;
+#pragma unroll
+        for (int r = c + 1; r < B; ++r)
+            if (r == p)
+#pragma unroll
+                for (int j = 0; j < B; ++j) {
+                    const double t = a[c * B + j];
+                    a[c * B + j] = a[r * B + j];
+                    a[r * B + j] = t;
+                    const double u = v[c * B + j];
+                    v[c * B + j] = v[r * B + j];
+                    v[r * B + j] = u;
+                }
+        const double piv = a[c * B + c];
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            a[c * B + j] /= piv;
+            v[c * B + j] /= piv;
+        }
+#pragma unroll
+        for (int r = 0; r < B; ++r)
+            if (r != c) {
+                const double f = a[r * B + c];
+#pragma unroll
+                for (int j = 0; j < B; ++j) {
+                    a[r * B + j] -= f * a[c * B + j];
+                    v[r * B + j] -= f * v[c * B + j];
+                }
+            }
+    }
+#pragma unroll
+    for (int e = 0; e < B * B; ++e) a[e] = v[e];
+    return true;
+}
+
+// Dispatches on a level's longest block row as KK (8, 16; 0 = plain loop).
 #define WITH_KMAX(kmax, ...)                        \
-    if ((kmax) <= 4) {                              \
-        constexpr int KK = 4;                       \
-        __VA_ARGS__;                                \
-    } else if ((kmax) <= 8) {                       \
+    if ((kmax) <= 8) {                              \
         constexpr int KK = 8;                       \
         __VA_ARGS__;                                \
     } else if ((kmax) <= 16) {                      \
@@ -185,21 +325,29 @@ __device__ __forceinline__ double sell_dot(const SellView& m, int base, int k0, 
         __VA_ARGS__;                                \
     }
 
-// dst (sliced ELL) <- src (CSR) through the slot map; padding slots get 0.
-__global__ void sell_scatter_kernel(int64_t size, const int* __restrict__ map, const double* __restrict__ src,
-                                    double* __restrict__ dst)
-{
-    GRID_STRIDE(i, size)
-    {
-        const int e = map[i];
-        dst[i] = e >= 0 ? src[e] : 0.0;
+// Dispatches on the block size as BS (1, 2, 3).
+#define WITH_BS(bs, ...)                            \
+    if ((bs) == 1) {                                \
+        constexpr int BS = 1;                       \
+        __VA_ARGS__;                                \
+    } else if ((bs) == 2) {                         \
+        constexpr int BS = 2;                       \
+        __VA_ARGS__;                                \
+    } else {                                        \
+        constexpr int BS = 3;                       \
+        __VA_ARGS__;                                \
     }
-}
 
-__global__ void gather_values_kernel(const double* __restrict__ src, const int* __restrict__ vmap,
-                                     double* __restrict__ dst, int64_t nnz)
+// dst[p] = src[map[p]], or 0 where map[p] < 0 (padding, or an entry of a
+// block that the Jacobian does not have).
+__global__ void gather_values_kernel(const double* __restrict__ src, const int* __restrict__ map,
+                                     double* __restrict__ dst, int64_t size)
 {
-    GRID_STRIDE(e, nnz) dst[e] = src[vmap[e]];
+    GRID_STRIDE(p, size)
+    {
+        const int e = map[p];
+        dst[p] = e >= 0 ? src[e] : 0.0;
+    }
 }
 
 __global__ void to_float_kernel(const double* __restrict__ a, float* __restrict__ b, int64_t n)
@@ -219,62 +367,145 @@ __global__ void unpermute_kernel(const double* __restrict__ src, const int* __re
     GRID_STRIDE(i, n) dst[perm[i]] = src[i];
 }
 
-// ILU(0) of the rows [r0, r1) of one stage (their L parts reference only
-// finished rows of earlier stages).
-__global__ void ilu0_factor_stage_kernel(int r0, int r1, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                         const int* __restrict__ diag, double* lu, int* status)
+// Block ILU(0) of the block rows [r0, r1) of one stage, in place in `lu`
+// (the block values of the matrix on entry).  For each lower block (R, K),
+// in ascending K: L_RK = A_RK D_K^{-1}, then A_RJ -= L_RK U_KJ for every
+// upper block (K, J) of row K whose position (R, J) is in row R's pattern.
+// The diagonal block is stored inverted (D_R^{-1}); rows of earlier stages
+// are finished.  A singular diagonal block sets *status.
+template <int B>
+__global__ void bilu_factor_stage_kernel(int r0, int r1, SellView m, double* lu, int* status)
 {
+    constexpr int BB = B * B;
     for (int64_t rr = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; rr < r1;
          rr += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)rr;
-        const int dpos = diag[r];
-        const int end = rowptr[r + 1];
-        for (int e = rowptr[r]; e < dpos; ++e) {
-            const int k = col[e];
-            const double piv = lu[diag[k]];
-            if (piv == 0.0) {
-                *status = 1;
-                return;
-            }
-            const double lik = lu[e] / piv;
-            lu[e] = lik;
-            int p = e + 1;
-            const int q1 = rowptr[k + 1];
-            for (int q = diag[k] + 1; q < q1; ++q) {
-                const int cq = col[q];
-                while (p < end && col[p] < cq) ++p;
-                if (p < end && col[p] == cq) lu[p] -= lik * lu[q];
+        const int R = (int)rr;
+        const int lane = R & 31, sb = m.slice_ptr[R >> 5], len = m.len[R], d = m.dk[R];
+        auto at = [&](int sbase, int ln, int k, int e) -> double& {
+            return lu[(size_t)(sbase + (k << 5)) * BB + (e << 5) + ln];
+        };
+        for (int k = 0; k < d; ++k) {
+            const int K = m.col[sb + (k << 5) + lane];
+            const int lk = K & 31, sk = m.slice_ptr[K >> 5], lenk = m.len[K], dkk = m.dk[K];
+            double l[BB];
+#pragma unroll
+            for (int i = 0; i < B; ++i)
+#pragma unroll
+                for (int j = 0; j < B; ++j) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int t = 0; t < B; ++t) s += at(sb, lane, k, i * B + t) * at(sk, lk, dkk, t * B + j);
+                    l[i * B + j] = s;
+                }
+#pragma unroll
+            for (int e = 0; e < BB; ++e) at(sb, lane, k, e) = l[e];
+            int p = k + 1;
+            for (int kk = dkk + 1; kk < lenk; ++kk) {
+                const int J = m.col[sk + (kk << 5) + lk];
+                while (p < len && m.col[sb + (p << 5) + lane] < J) ++p;
+                if (p < len && m.col[sb + (p << 5) + lane] == J) {
+#pragma unroll
+                    for (int i = 0; i < B; ++i)
+#pragma unroll
+                        for (int j = 0; j < B; ++j) {
+                            double s = 0.0;
+#pragma unroll
+                            for (int t = 0; t < B; ++t) s += l[i * B + t] * at(sk, lk, kk, t * B + j);
+                            at(sb, lane, p, i * B + j) -= s;
+                        }
+                }
             }
         }
-        if (lu[dpos] == 0.0) *status = 1;
+        double dg[BB];
+#pragma unroll
+        for (int e = 0; e < BB; ++e) dg[e] = at(sb, lane, d, e);
+        if (!invert_block<B>(dg)) *status = 1;
+#pragma unroll
+        for (int e = 0; e < BB; ++e) at(sb, lane, d, e) = dg[e];
     }
 }
 
-template <int KM, class T>
-__global__ void ilu0_lower_stage_kernel(int r0, int r1, SellView m, const T* __restrict__ lu,
-                                        const T* __restrict__ b, T* __restrict__ y, const KScal* sc, int skip_if_s)
+__device__ __forceinline__ bool mg_skip(const KScal* sc, int skip_if_s)
 {
-    if (stopped(sc) || (skip_if_s && sc->s_conv)) return;
+    return stopped(sc) || (skip_if_s && sc->s_conv);
+}
+
+// Forward sweep of stage [r0, r1), a stage after the first:
+//   y_R = b_R - sum_{k < dk} L_Rk y_K,
+// with y_K = b_K for rows of the first stage (K < r_first) and out_K
+// otherwise.  The last stage has no upper part: there the row is finished,
+// out_R = D_R^{-1} y_R (and zadd_R += out_R when zadd is given).
+template <int B, int KM, class T>
+__global__ void bilu_lower_kernel(int r0, int r1, int r_first, int last, SellView m, const T* __restrict__ lu,
+                                  const T* __restrict__ b, T* __restrict__ out, T* __restrict__ zadd,
+                                  const KScal* sc, int skip_if_s)
+{
+    if (mg_skip(sc, skip_if_s)) return;
     for (int64_t rr = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; rr < r1;
          rr += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)rr;
-        const double s = sell_dot<KM, T>(m, sell_base(m, r), 0, m.dk[r], lu, y);
-        y[r] = (T)((double)b[r] - s);
+        const int R = (int)rr;
+        const int lane = R & 31, sb = m.slice_ptr[R >> 5], d = m.dk[R];
+        double acc[B];
+#pragma unroll
+        for (int c = 0; c < B; ++c) acc[c] = 0.0;
+        bdot<B, KM, T>(m, sb, lane, 0, d, lu, b, out, r_first, acc);
+        double y[B];
+        load_bvec<B, T>(b, R, y);
+#pragma unroll
+        for (int c = 0; c < B; ++c) y[c] = (double)(T)(y[c] - acc[c]);
+        if (last) {
+            double z[B];
+            bmatvec<B, T>(lu, sb + (d << 5), lane, y, z);
+#pragma unroll
+            for (int c = 0; c < B; ++c) z[c] = (double)(T)z[c];
+            store_bvec<B, T>(out, R, z);
+            if (zadd) {
+                double w[B];
+                load_bvec<B, T>(zadd, R, w);
+#pragma unroll
+                for (int c = 0; c < B; ++c) w[c] += z[c];
+                store_bvec<B, T>(zadd, R, w);
+            }
+        } else {
+            store_bvec<B, T>(out, R, y);
+        }
     }
 }
 
-template <int KM, class T>
-__global__ void ilu0_upper_stage_kernel(int r0, int r1, SellView m, const T* __restrict__ lu, T* __restrict__ x,
-                                        const KScal* sc, int skip_if_s)
+// Backward sweep of stage [r0, r1), a stage before the last:
+//   out_R = D_R^{-1} (y_R - sum_{k > dk} U_Rk out_K),
+// with y_R = b_R in the first stage and the forward-sweep value out_R
+// otherwise; zadd_R += out_R when zadd is given.
+template <int B, int KM, class T>
+__global__ void bilu_upper_kernel(int r0, int r1, int first, SellView m, const T* __restrict__ lu,
+                                  const T* __restrict__ b, T* __restrict__ out, T* __restrict__ zadd,
+                                  const KScal* sc, int skip_if_s)
 {
-    if (stopped(sc) || (skip_if_s && sc->s_conv)) return;
+    if (mg_skip(sc, skip_if_s)) return;
     for (int64_t rr = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; rr < r1;
          rr += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)rr;
-        const int base = sell_base(m, r);
-        const int d = m.dk[r];
-        const double s = sell_dot<KM, T>(m, base, d + 1, m.len[r], lu, x);
-        x[r] = (T)(((double)x[r] - s) / (double)lu[base + (d << 5)]);
+        const int R = (int)rr;
+        const int lane = R & 31, sb = m.slice_ptr[R >> 5], d = m.dk[R];
+        double acc[B];
+#pragma unroll
+        for (int c = 0; c < B; ++c) acc[c] = 0.0;
+        bdot<B, KM, T>(m, sb, lane, d + 1, m.len[R], lu, out, out, INT_MAX, acc);
+        double y[B];
+        load_bvec<B, T>(first ? b : out, R, y);
+#pragma unroll
+        for (int c = 0; c < B; ++c) y[c] -= acc[c];
+        double z[B];
+        bmatvec<B, T>(lu, sb + (d << 5), lane, y, z);
+#pragma unroll
+        for (int c = 0; c < B; ++c) z[c] = (double)(T)z[c];
+        store_bvec<B, T>(out, R, z);
+        if (zadd) {
+            double w[B];
+            load_bvec<B, T>(zadd, R, w);
+#pragma unroll
+            for (int c = 0; c < B; ++c) w[c] += z[c];
+            store_bvec<B, T>(zadd, R, w);
+        }
     }
 }
 
@@ -334,18 +565,28 @@ __global__ void bicg_p_kernel(const T* __restrict__ r, const T* __restrict__ v, 
 }
 
 // v = A ph ; alpha = rho_new / (rhat . v)
-template <int KM, class T>
+template <int B, int KM, class T>
 __global__ void bicg_spmv_alpha_kernel(SellView m, const T* __restrict__ a, const T* __restrict__ ph,
-                                       const T* __restrict__ rhat, T* __restrict__ v, int n, double* partials,
+                                       const T* __restrict__ rhat, T* __restrict__ v, int nb, double* partials,
                                        unsigned int* counter, KScal* sc)
 {
     if (stopped(sc)) return;
     double d[1] = {0.0};
-    GRID_STRIDE(i, n)
+    GRID_STRIDE(rr, nb)
     {
-        const double vi = sell_dot<KM, T>(m, sell_base(m, (int)i), 0, m.len[i], a, ph);
-        v[i] = (T)vi;
-        d[0] += (double)rhat[i] * (double)(T)vi;
+        const int R = (int)rr;
+        double acc[B];
+#pragma unroll
+        for (int c = 0; c < B; ++c) acc[c] = 0.0;
+        bdot<B, KM, T>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, ph, ph, INT_MAX, acc);
+        double h[B];
+        load_bvec<B, T>(rhat, R, h);
+#pragma unroll
+        for (int c = 0; c < B; ++c) {
+            const T vi = (T)acc[c];
+            v[R * B + c] = vi;
+            d[0] += h[c] * (double)vi;
+        }
     }
     double s[1];
     if (grid_sum<1>(d, partials, counter, s)) {
@@ -377,19 +618,29 @@ __global__ void bicg_s_kernel(const T* __restrict__ r, const T* __restrict__ v, 
 }
 
 // t = A sh ; omega = (t . s) / (t . t)
-template <int KM, class T>
+template <int B, int KM, class T>
 __global__ void bicg_spmv_omega_kernel(SellView m, const T* __restrict__ a, const T* __restrict__ sh,
-                                       const T* __restrict__ s, T* __restrict__ t, int n, double* partials,
+                                       const T* __restrict__ s, T* __restrict__ t, int nb, double* partials,
                                        unsigned int* counter, KScal* sc)
 {
     if (stopped(sc) || sc->s_conv) return;
     double d[2] = {0.0, 0.0};
-    GRID_STRIDE(i, n)
+    GRID_STRIDE(rr, nb)
     {
-        const T ti = (T)sell_dot<KM, T>(m, sell_base(m, (int)i), 0, m.len[i], a, sh);
-        t[i] = ti;
-        d[0] += (double)ti * (double)s[i];
-        d[1] += (double)ti * (double)ti;
+        const int R = (int)rr;
+        double acc[B];
+#pragma unroll
+        for (int c = 0; c < B; ++c) acc[c] = 0.0;
+        bdot<B, KM, T>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, sh, sh, INT_MAX, acc);
+        double sv[B];
+        load_bvec<B, T>(s, R, sv);
+#pragma unroll
+        for (int c = 0; c < B; ++c) {
+            const T ti = (T)acc[c];
+            t[R * B + c] = ti;
+            d[0] += (double)ti * sv[c];
+            d[1] += (double)ti * (double)ti;
+        }
     }
     double u[2];
     if (grid_sum<2>(d, partials, counter, u)) {
@@ -441,18 +692,26 @@ __global__ void bicg_xr_kernel(const T* __restrict__ ph, const T* __restrict__ s
 }
 
 // Refinement: r = b - A x (FP64) with rr = r.r ; also r32 = float(r).
-template <int KM>
+template <int B, int KM>
 __global__ void residual_kernel(SellView m, const double* __restrict__ a, const double* __restrict__ x,
-                                const double* __restrict__ b, double* __restrict__ r, float* __restrict__ r32, int n,
+                                const double* __restrict__ b, double* __restrict__ r, float* __restrict__ r32, int nb,
                                 double* partials, unsigned int* counter, double* out_rr)
 {
     double d[1] = {0.0};
-    GRID_STRIDE(i, n)
+    GRID_STRIDE(rr, nb)
     {
-        const double ri = b[i] - sell_dot<KM, double>(m, sell_base(m, (int)i), 0, m.len[i], a, x);
-        r[i] = ri;
-        r32[i] = (float)ri;
-        d[0] += ri * ri;
+        const int R = (int)rr;
+        double acc[B];
+#pragma unroll
+        for (int c = 0; c < B; ++c) acc[c] = 0.0;
+        bdot<B, KM, double>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, x, x, INT_MAX, acc);
+#pragma unroll
+        for (int c = 0; c < B; ++c) {
+            const double ri = b[R * B + c] - acc[c];
+            r[R * B + c] = ri;
+            r32[R * B + c] = (float)ri;
+            d[0] += ri * ri;
+        }
     }
     double u[1];
     if (grid_sum<1>(d, partials, counter, u)) {
@@ -477,13 +736,13 @@ __global__ void sumsq_kernel(const double* __restrict__ a, int n, double* partia
 }
 
 // ---- multilevel preconditioner kernels -------------------------------------
-// Coarse-level values: each coarse entry is the sum of the finer level's
-// entries that aggregate onto it (Galerkin product R A R^T with a 0/1
-// aggregation R), gathered in a fixed order.
-__global__ void galerkin_kernel(int64_t nnz_c, const int* __restrict__ gptr, const int* __restrict__ gidx,
+// Coarse-level values: each coarse value is the sum of the finer level's
+// values that aggregate onto it (Galerkin product R A R^T with a 0/1
+// aggregation R), gathered in a fixed order; an empty list gives 0.
+__global__ void galerkin_kernel(int64_t size_c, const int* __restrict__ gptr, const int* __restrict__ gidx,
                                 const double* __restrict__ fine, double* __restrict__ coarse)
 {
-    GRID_STRIDE(c, nnz_c)
+    GRID_STRIDE(c, size_c)
     {
         double s = 0.0;
         const int k1 = gptr[c + 1];
@@ -492,18 +751,25 @@ __global__ void galerkin_kernel(int64_t nnz_c, const int* __restrict__ gptr, con
     }
 }
 
-__device__ __forceinline__ bool mg_skip(const KScal* sc, int skip_if_s)
-{
-    return stopped(sc) || (skip_if_s && sc->s_conv);
-}
-
 // out = b - A x
-template <int KM, class T>
-__global__ void mg_residual_kernel(int n, SellView m, const T* __restrict__ a, const T* __restrict__ x,
+template <int B, int KM, class T>
+__global__ void mg_residual_kernel(int nb, SellView m, const T* __restrict__ a, const T* __restrict__ x,
                                    const T* __restrict__ b, T* __restrict__ out, const KScal* sc, int skip_if_s)
 {
     if (mg_skip(sc, skip_if_s)) return;
-    GRID_STRIDE(i, n) out[i] = (T)((double)b[i] - sell_dot<KM, T>(m, sell_base(m, (int)i), 0, m.len[i], a, x));
+    GRID_STRIDE(rr, nb)
+    {
+        const int R = (int)rr;
+        double acc[B];
+#pragma unroll
+        for (int c = 0; c < B; ++c) acc[c] = 0.0;
+        bdot<B, KM, T>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, x, x, INT_MAX, acc);
+        double y[B];
+        load_bvec<B, T>(b, R, y);
+#pragma unroll
+        for (int c = 0; c < B; ++c) y[c] -= acc[c];
+        store_bvec<B, T>(out, R, y);
+    }
 }
 
 // rc[P] = sum of t over the members of aggregate P
@@ -530,30 +796,32 @@ __global__ void mg_prolong_kernel(int n, const int* __restrict__ agg, const T* _
     GRID_STRIDE(i, n) z[i] = (T)((double)z[i] + (double)ec[agg[i]]);
 }
 
-template <class T>
-__global__ void mg_add_kernel(int n, const T* __restrict__ w, T* __restrict__ z, const KScal* sc, int skip_if_s)
-{
-    if (mg_skip(sc, skip_if_s)) return;
-    GRID_STRIDE(i, n) z[i] = (T)((double)z[i] + (double)w[i]);
-}
-
-// Inverse of the coarsest matrix (n <= kCoarsest) by Gauss-Jordan with
-// partial pivoting on [A | I], one block.
+// Inverse of the coarsest matrix (n <= kCoarsest unknowns) by Gauss-Jordan
+// with partial pivoting on [A | I], one thread block; A is expanded from its
+// block sliced ELL values.
 constexpr int kCoarsest = 128;
 
-__global__ void dense_inverse_kernel(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                     const double* __restrict__ a, double* __restrict__ work,
+template <int B>
+__global__ void dense_inverse_kernel(int nb, SellView m, const double* __restrict__ a, double* __restrict__ work,
                                      double* __restrict__ inv, int* status)
 {
+    constexpr int BB = B * B;
     __shared__ double factor[kCoarsest];
     __shared__ int piv;
     __shared__ double pval;
+    const int n = nb * B;
     const int w2 = 2 * n;
     for (int idx = threadIdx.x; idx < n * w2; idx += blockDim.x) work[idx] = 0.0;
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) work[i * w2 + col[e]] = a[e];
-        work[i * w2 + n + i] = 1.0;
+    for (int R = threadIdx.x; R < nb; R += blockDim.x) {
+        const int lane = R & 31, sb = m.slice_ptr[R >> 5];
+        for (int k = 0; k < m.len[R]; ++k) {
+            const int J = m.col[sb + (k << 5) + lane];
+            for (int i = 0; i < B; ++i)
+                for (int j = 0; j < B; ++j)
+                    work[(R * B + i) * w2 + J * B + j] = a[(size_t)(sb + (k << 5)) * BB + ((i * B + j) << 5) + lane];
+        }
+        for (int i = 0; i < B; ++i) work[(R * B + i) * w2 + n + R * B + i] = 1.0;
     }
     __syncthreads();
     for (int k = 0; k < n; ++k) {
@@ -632,9 +900,9 @@ __global__ void pc_to_f64_kernel(const float* __restrict__ a, double* __restrict
 // `ncomp` blocks of one unknown per grid cell, as newtonSolve and
 // newtonSolveSystem stack them): geometric aggregation of 2x2x2 cells per
 // unknown block, Galerkin coarse matrices R A R^T, a V(1,1) cycle with one
-// ILU(0) sweep before and after the coarse correction on every level, and a
-// dense inverse on the coarsest level (<= 128 unknowns).  Otherwise plain
-// ILU(0).
+// block ILU(0) sweep before and after the coarse correction on every level,
+// and a dense inverse on the coarsest level (<= 128 unknowns).  Otherwise
+// plain block ILU(0).
 // ---------------------------------------------------------------------------
 struct HostCsr {
     int n = 0;
@@ -642,19 +910,22 @@ struct HostCsr {
 };
 
 struct Level {
-    int n = 0;
-    int64_t nnz = 0;
+    int n = 0;                     // unknowns
+    int nb = 0;                    // block rows
+    int bs = 1;                    // block size
+    int64_t nnz = 0;               // scalar entries of the matrix pattern
     int cx = 1, cy = 1, cz = 1;    // cells of this level's grid
     bool coarsest = false;
-    std::vector<int> stage_ptr;    // stages (colours or wavefronts) in the permuted order
-    Buf perm, rowptr, col, diag;   // permuted pattern
-    Buf gptr, gidx;                // Galerkin gather from the finer level (levels > 0)
-    Buf agg, mptr, midx;           // to the next coarser level
-    Buf a64, lu64;                 // CSR values: matrix, ILU(0) factors
-    int64_t sell_size = 0;         // sliced ELL copies used by the sweeps
-    int kmax = 0;                  // longest row
-    Buf sell_ptr, sell_col, sell_len, sell_dk, sell_map;
-    Buf as64, lus64, as32, lus32;
+    std::vector<int> stage_ptr;    // stages (colours or wavefronts) of block rows, permuted order
+    Buf perm;                      // permuted unknown position -> natural unknown
+    Buf gptr, gidx;                // Galerkin gather from the finer level's values (levels > 0)
+    Buf agg, mptr, midx;           // to the next coarser level (unknown positions)
+    int64_t sell_size = 0;         // slots of the block sliced ELL layout
+    int64_t vals = 0;              // sell_size * bs^2
+    int64_t blocks = 0;            // block entries of the pattern (without padding)
+    int kmax = 0;                  // longest block row
+    Buf sell_ptr, sell_col, sell_len, sell_dk;
+    Buf as64, lus64, as32, lus32;  // matrix, block ILU(0) factors (inverted diagonal blocks)
     Buf v64, v32;                  // 4 work vectors: r, z, t, w
     SellView view() const
     {
@@ -667,10 +938,10 @@ struct SolverAnalysis {
     int n = 0;
     int64_t nnz = 0;
     bool natural = false;
-    bool ok = true;  // every row has a diagonal entry
+    bool ok = true;  // every row has a diagonal entry (1 x 1 blocks)
     bool multigrid = false;
     std::vector<Level> levels;
-    Buf vmap;        // level-0 permuted entry <- Jacobian entry
+    Buf vmap;        // level-0 value <- Jacobian entry (-1: zero)
     Buf vec64, vec32, scal, partials, counter, factor_status;
     Buf pc32;        // FP32 input and output of an FP32 preconditioner
     // CUDA graphs of `chunk` BiCGStab iterations: [0] FP64, [1] FP32, [2] FP64
@@ -740,96 +1011,126 @@ Buf upload_ints(Core& c, const std::vector<int>& v)
     return b;
 }
 
-// Orders the rows of `A` by stage, builds the permuted pattern with
-// ascending columns, and returns the host permutation (new -> old), its
-// inverse and, for every permuted entry, its entry index in `A`.
-void order_level(Core& c, const HostCsr& A, bool natural, Level& L, std::vector<int>& perm, std::vector<int>& iperm,
-                 std::vector<int>& pcsr_ptr, std::vector<int>& pcsr_col, std::vector<int>& emap, bool& ok)
+// Lays out the matrix with pattern `A` (natural unknown numbering) in blocks
+// of `bs` unknowns: block row of unknown u is u % nb and its component u / nb
+// (nb = n / bs).  Orders the block rows by stage and builds the block sliced
+// ELL pattern (each row with its diagonal block).  Returns the unknown
+// permutation (position -> natural unknown), its inverse, and for every
+// entry of `A` its position in the level's value array.
+void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std::vector<int>& perm,
+                 std::vector<int>& iperm, std::vector<int>& vpos, bool& ok)
 {
     const int n = A.n;
+    const int nb = n / bs;
+    const int bb = bs * bs;
     const int64_t nnz = A.ptr[n];
-    const std::vector<int> key = stage_keys(A, natural);
-    const int nst = n > 0 ? *std::max_element(key.begin(), key.end()) + 1 : 0;
+    // block graph (natural block numbering), sorted, with the diagonal
+    HostCsr G;
+    G.n = nb;
+    G.ptr.assign(nb + 1, 0);
+    {
+        std::vector<std::vector<int>> rows(nb);
+        for (int u = 0; u < n; ++u)
+            for (int e = A.ptr[u]; e < A.ptr[u + 1]; ++e) rows[u % nb].push_back(A.col[e] % nb);
+        for (int R = 0; R < nb; ++R) {
+            auto& r = rows[R];
+            r.push_back(R);
+            std::sort(r.begin(), r.end());
+            r.erase(std::unique(r.begin(), r.end()), r.end());
+            G.ptr[R + 1] = G.ptr[R] + (int)r.size();
+        }
+        G.col.resize(G.ptr[nb] > 0 ? G.ptr[nb] : 1);
+        for (int R = 0; R < nb; ++R) std::copy(rows[R].begin(), rows[R].end(), G.col.begin() + G.ptr[R]);
+    }
+    if (bs == 1)
+        for (int u = 0; u < n; ++u) {
+            bool has = false;
+            for (int e = A.ptr[u]; e < A.ptr[u + 1]; ++e) has = has || A.col[e] == u;
+            if (!has) ok = false;
+        }
+    const std::vector<int> key = stage_keys(G, natural);
+    const int nst = nb > 0 ? *std::max_element(key.begin(), key.end()) + 1 : 0;
     L.stage_ptr.assign(nst + 1, 0);
-    for (int i = 0; i < n; ++i) L.stage_ptr[key[i] + 1]++;
+    for (int R = 0; R < nb; ++R) L.stage_ptr[key[R] + 1]++;
     for (int s = 0; s < nst; ++s) L.stage_ptr[s + 1] += L.stage_ptr[s];
-    perm.assign(n, 0);
-    iperm.assign(n, 0);
+    std::vector<int> pb(nb), ipb(nb);
     {
         std::vector<int> pos(L.stage_ptr.begin(), L.stage_ptr.end() - 1);
-        for (int i = 0; i < n; ++i) perm[pos[key[i]]++] = i;
+        for (int R = 0; R < nb; ++R) pb[pos[key[R]]++] = R;
     }
-    for (int r = 0; r < n; ++r) iperm[perm[r]] = r;
-    pcsr_ptr.assign(n + 1, 0);
-    pcsr_col.assign(nnz > 0 ? nnz : 1, 0);
-    emap.assign(nnz > 0 ? nnz : 1, 0);
-    std::vector<int> diag(n, 0);
-    std::vector<std::pair<int, int>> row;
-    for (int r = 0; r < n; ++r) {
-        const int i = perm[r];
-        row.clear();
-        for (int e = A.ptr[i]; e < A.ptr[i + 1]; ++e) row.emplace_back(iperm[A.col[e]], e);
-        std::sort(row.begin(), row.end());
-        pcsr_ptr[r + 1] = pcsr_ptr[r] + (int)row.size();
-        int o = pcsr_ptr[r];
-        bool has = false;
-        for (auto& ce : row) {
-            if (ce.first == r) {
-                diag[r] = o;
-                has = true;
-            }
-            pcsr_col[o] = ce.first;
-            emap[o] = ce.second;
-            ++o;
+    for (int R = 0; R < nb; ++R) ipb[pb[R]] = R;
+    perm.assign(n, 0);
+    iperm.assign(n, 0);
+    for (int R = 0; R < nb; ++R)
+        for (int cc = 0; cc < bs; ++cc) {
+            perm[R * bs + cc] = cc * nb + pb[R];
+            iperm[cc * nb + pb[R]] = R * bs + cc;
         }
-        if (!has) ok = false;
+    // permuted block rows: sorted permuted columns
+    std::vector<int> pptr(nb + 1, 0), pcol(G.ptr[nb] > 0 ? G.ptr[nb] : 1);
+    for (int R = 0; R < nb; ++R) {
+        const int o = pb[R];
+        pptr[R + 1] = pptr[R] + (G.ptr[o + 1] - G.ptr[o]);
+        int w = pptr[R];
+        for (int e = G.ptr[o]; e < G.ptr[o + 1]; ++e) pcol[w++] = ipb[G.col[e]];
+        std::sort(pcol.begin() + pptr[R], pcol.begin() + pptr[R + 1]);
+    }
+    // block sliced ELL, 32 block rows per slice
+    const int nsl = (nb + 31) / 32;
+    std::vector<int> sp(nsl + 1, 0), len(nb > 0 ? nb : 1), dk(nb > 0 ? nb : 1);
+    for (int sl = 0; sl < nsl; ++sl) {
+        int w = 0;
+        for (int R = sl * 32; R < std::min(nb, sl * 32 + 32); ++R) w = std::max(w, pptr[R + 1] - pptr[R]);
+        sp[sl + 1] = sp[sl] + 32 * w;
+    }
+    const int64_t size = sp[nsl];
+    if (size * bb >= (int64_t)INT_MAX) fail(EQG_ERR_UNSUPPORTED, "linear system too large for 32-bit value offsets");
+    std::vector<int> scol(size > 0 ? size : 1, 0);
+    L.kmax = 0;
+    for (int R = 0; R < nb; ++R) {
+        const int base = sp[R / 32] + (R % 32);
+        len[R] = pptr[R + 1] - pptr[R];
+        L.kmax = std::max(L.kmax, len[R]);
+        const int w = (sp[R / 32 + 1] - sp[R / 32]) / 32;
+        dk[R] = -1;
+        for (int k = 0; k < w; ++k) {
+            if (k < len[R]) {
+                scol[base + 32 * k] = pcol[pptr[R] + k];
+                if (pcol[pptr[R] + k] == R) dk[R] = k;
+            } else {
+                scol[base + 32 * k] = R;  // padding: a valid column, values 0, never read by the kernels
+            }
+        }
+    }
+    // value position of every scalar entry of A
+    vpos.assign(nnz > 0 ? nnz : 1, -1);
+    for (int u = 0; u < n; ++u) {
+        const int R = ipb[u % nb], cu = u / nb;
+        for (int e = A.ptr[u]; e < A.ptr[u + 1]; ++e) {
+            const int v = A.col[e];
+            const int J = ipb[v % nb], cv = v / nb;
+            const int* lo = pcol.data() + pptr[R];
+            const int* hi = pcol.data() + pptr[R + 1];
+            const int k = (int)(std::lower_bound(lo, hi, J) - lo);
+            const int64_t slot0 = sp[R / 32] + 32 * k;
+            vpos[e] = (int)(slot0 * bb + 32 * (cu * bs + cv) + (R % 32));
+        }
     }
     L.n = n;
+    L.nb = nb;
+    L.bs = bs;
     L.nnz = nnz;
-    {
-        // sliced ELL, 32 rows per slice (one thread per row)
-        const int nsl = (n + 31) / 32;
-        std::vector<int> sp(nsl + 1, 0), len(n), dk(n);
-        for (int sl = 0; sl < nsl; ++sl) {
-            int w = 0;
-            for (int r = sl * 32; r < std::min(n, sl * 32 + 32); ++r) w = std::max(w, pcsr_ptr[r + 1] - pcsr_ptr[r]);
-            sp[sl + 1] = sp[sl] + 32 * w;
-        }
-        const int64_t size = sp[nsl];
-        std::vector<int> scol(size > 0 ? size : 1, 0), smap(size > 0 ? size : 1, -1);
-        for (int r = 0; r < n; ++r) {
-            const int base = sp[r / 32] + (r % 32);
-            len[r] = pcsr_ptr[r + 1] - pcsr_ptr[r];
-            dk[r] = diag[r] - pcsr_ptr[r];
-            const int w = (sp[r / 32 + 1] - sp[r / 32]) / 32;
-            for (int k = 0; k < w; ++k) {
-                const int idx = base + 32 * k;
-                if (k < len[r]) {
-                    scol[idx] = pcsr_col[pcsr_ptr[r] + k];
-                    smap[idx] = pcsr_ptr[r] + k;
-                } else {
-                    scol[idx] = r;  // padding: a valid column, value 0, never read by the sweeps
-                }
-            }
-        }
-        L.sell_size = size;
-        L.kmax = 0;
-        for (int r = 0; r < n; ++r) L.kmax = std::max(L.kmax, len[r]);
-        L.sell_ptr = upload_ints(c, sp);
-        L.sell_col = upload_ints(c, scol);
-        L.sell_len = upload_ints(c, len);
-        L.sell_dk = upload_ints(c, dk);
-        L.sell_map = upload_ints(c, smap);
-        L.as64 = c.allocN<double>((size_t)(size > 0 ? size : 1));
-        L.lus64 = c.allocN<double>((size_t)(size > 0 ? size : 1));
-    }
+    L.sell_size = size;
+    L.vals = size * bb;
+    L.blocks = pptr[nb];
+    L.sell_ptr = upload_ints(c, sp);
+    L.sell_col = upload_ints(c, scol);
+    L.sell_len = upload_ints(c, len);
+    L.sell_dk = upload_ints(c, dk);
+    const size_t nv = (size_t)(L.vals > 0 ? L.vals : 1);
+    L.as64 = c.allocN<double>(nv);
+    L.lus64 = c.allocN<double>(nv);
     L.perm = upload_ints(c, perm);
-    L.rowptr = upload_ints(c, pcsr_ptr);
-    L.col = upload_ints(c, pcsr_col);
-    L.diag = upload_ints(c, diag);
-    const size_t nz = (size_t)(nnz > 0 ? nnz : 1);
-    L.a64 = c.allocN<double>(nz);
-    L.lu64 = c.allocN<double>(nz);
     L.v64 = c.allocN<double>((size_t)4 * (n > 0 ? n : 1));
 }
 
@@ -849,22 +1150,35 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
         EQG_CUDA(cudaMemcpyAsync(A.col.data(), p.colind->ptr, (size_t)p.nnz * 4, cudaMemcpyDeviceToHost, c.stream));
     c.sync();
 
-    std::vector<int> perm, iperm, pptr, pcol, emap;
-    an->levels.emplace_back();
-    order_level(c, A, natural, an->levels[0], perm, iperm, pptr, pcol, emap, an->ok);
-    an->vmap = upload_ints(c, emap);
-
     const std::string pre = c.param_s("linsolver_preconditioner", "multigrid");
     if (pre != "multigrid" && pre != "ilu0") fail(EQG_ERR_ARG, "linsolver_preconditioner must be multigrid or ilu0");
+    // unknowns stacked as ncomp collections over all cells
     const int ncomp = (c.nc > 0 && n % c.nc == 0) ? n / c.nc : 0;
-    an->multigrid = pre == "multigrid" && ncomp >= 1 && ncomp <= 8 && n > kCoarsest && an->ok;
+    const bool mg_wanted = pre == "multigrid" && ncomp >= 1 && ncomp <= 8 && n > kCoarsest;
+    // Block ILU(0) with FP32 factors (explicit FP32 inverses of the diagonal
+    // blocks) converges much more slowly than scalar ILU(0) in FP32 on the
+    // two-phase systems, alone and as the V-cycle smoother, so the FP32
+    // preconditioners keep 1 x 1 blocks.
+    const bool fp64_pc = c.param_s("linsolver_precision", "double") == "double";
+    const int bs =
+        (!natural && fp64_pc && (ncomp == 2 || ncomp == 3) && c.param_i("linsolver_block", 1) != 0) ? ncomp : 1;
+
+    std::vector<int> perm, iperm, vpos;
+    an->levels.emplace_back();
+    order_level(c, A, natural, bs, an->levels[0], perm, iperm, vpos, an->ok);
+    {
+        std::vector<int> vmap(an->levels[0].vals > 0 ? an->levels[0].vals : 1, -1);
+        for (int64_t e = 0; e < p.nnz; ++e) vmap[vpos[e]] = (int)e;
+        an->vmap = upload_ints(c, vmap);
+    }
+    an->multigrid = mg_wanted && an->ok;
     an->levels[0].cx = c.nx;
     an->levels[0].cy = c.ny;
     an->levels[0].cz = c.nz;
     if (an->multigrid) {
-        // the finer level in its natural ordering, with its permutation
+        // the finer level in its natural ordering, with its permutation and value positions
         HostCsr fine = A;
-        std::vector<int> fperm = perm, fiperm = iperm, fptr = pptr, fcol = pcol;
+        std::vector<int> fperm = perm, fvpos = vpos;
         for (;;) {
             Level& F = an->levels.back();
             const int fcx = F.cx, fcy = F.cy, fcz = F.cz;
@@ -879,7 +1193,7 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
                 const int i = cell % fcx, j = (cell / fcx) % fcy, k = cell / (fcx * fcy);
                 agg_nat[u] = comp * ccells + (i / 2) + ccx * ((j / 2) + ccy * (fcz > 1 ? k / 2 : 0));
             }
-            // coarse pattern (natural ordering)
+            // coarse pattern (natural ordering, sorted rows)
             HostCsr C;
             C.n = nc_unk;
             {
@@ -888,7 +1202,6 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
                 std::vector<std::vector<int>> members(nc_unk);
                 for (int u = 0; u < fine.n; ++u) members[agg_nat[u]].push_back(u);
                 C.ptr.assign(nc_unk + 1, 0);
-                std::vector<int> cols;
                 for (int U = 0; U < nc_unk; ++U) {
                     for (int u : members[U])
                         for (int e = fine.ptr[u]; e < fine.ptr[u + 1]; ++e) {
@@ -910,11 +1223,11 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             Lc.cx = ccx;
             Lc.cy = ccy;
             Lc.cz = ccz;
-            std::vector<int> cperm, ciperm, cptr, ccol, cemap;
+            std::vector<int> cperm, ciperm, cvpos;
             bool cok = true;
-            order_level(c, C, natural, Lc, cperm, ciperm, cptr, ccol, cemap, cok);
+            order_level(c, C, natural, bs, Lc, cperm, ciperm, cvpos, cok);
             if (!cok) fail(EQG_ERR_DEVICE, "coarse level without a diagonal entry");
-            // aggregation in permuted indices, and aggregate members
+            // aggregation in permuted positions, and aggregate members
             std::vector<int> aggp(fine.n);
             for (int pf = 0; pf < fine.n; ++pf) aggp[pf] = ciperm[agg_nat[fperm[pf]]];
             std::vector<int> mptr(nc_unk + 1, 0), midx(fine.n);
@@ -927,26 +1240,26 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             Lf.agg = upload_ints(c, aggp);
             Lf.mptr = upload_ints(c, mptr);
             Lf.midx = upload_ints(c, midx);
-            // Galerkin gather: coarse permuted entry <- fine permuted entries
-            const int64_t fnnz = fptr[fine.n];
+            // Galerkin gather: coarse value <- fine values, in ascending fine entry order
+            const int64_t fnnz = fine.ptr[fine.n];
+            const int64_t cvals = Lc.vals;
             std::vector<int> target(fnnz > 0 ? fnnz : 1);
-            for (int pf = 0; pf < fine.n; ++pf) {
-                const int P = aggp[pf];
-                for (int e = fptr[pf]; e < fptr[pf + 1]; ++e) {
-                    const int Q = aggp[fcol[e]];
-                    const int* lo = ccol.data() + cptr[P];
-                    const int* hi = ccol.data() + cptr[P + 1];
-                    const int* q = std::lower_bound(lo, hi, Q);
-                    target[e] = (int)(q - ccol.data());
+            for (int u = 0; u < fine.n; ++u) {
+                const int U = agg_nat[u];
+                for (int e = fine.ptr[u]; e < fine.ptr[u + 1]; ++e) {
+                    const int V = agg_nat[fine.col[e]];
+                    const int* lo = C.col.data() + C.ptr[U];
+                    const int* hi = C.col.data() + C.ptr[U + 1];
+                    const int* q = std::lower_bound(lo, hi, V);
+                    target[e] = cvpos[q - C.col.data()];
                 }
             }
-            const int64_t cnnz = cptr[nc_unk];
-            std::vector<int> gptr(cnnz + 1, 0), gidx(fnnz > 0 ? fnnz : 1);
+            std::vector<int> gptr(cvals + 1, 0), gidx(fnnz > 0 ? fnnz : 1);
             for (int64_t e = 0; e < fnnz; ++e) gptr[target[e] + 1]++;
-            for (int64_t k = 0; k < cnnz; ++k) gptr[k + 1] += gptr[k];
+            for (int64_t k = 0; k < cvals; ++k) gptr[k + 1] += gptr[k];
             {
                 std::vector<int> pos(gptr.begin(), gptr.end() - 1);
-                for (int64_t e = 0; e < fnnz; ++e) gidx[pos[target[e]]++] = (int)e;
+                for (int64_t e = 0; e < fnnz; ++e) gidx[pos[target[e]]++] = fvpos[e];
             }
             Lc.gptr = upload_ints(c, gptr);
             Lc.gidx = upload_ints(c, gidx);
@@ -963,9 +1276,7 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             }
             fine = std::move(C);
             fperm = std::move(cperm);
-            fiperm = std::move(ciperm);
-            fptr = std::move(cptr);
-            fcol = std::move(ccol);
+            fvpos = std::move(cvpos);
         }
     }
     an->vec64 = c.allocN<double>((size_t)10 * (n > 0 ? n : 1));
@@ -975,8 +1286,8 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     an->factor_status = c.allocN<int>(1);
     EQG_CUDA(cudaMemsetAsync(an->counter->ptr, 0, sizeof(unsigned int), c.stream));
     c.sync();
-    if (c.verbose > 2 && an->multigrid) {
-        std::printf("        multigrid levels:");
+    if (c.verbose > 2) {
+        std::printf("        linear solver: %dx%d blocks%s, levels:", bs, bs, an->multigrid ? ", multigrid" : "");
         for (auto& L : an->levels) std::printf(" %d(%zu stages)", L.n, L.stage_ptr.size() - 1);
         std::printf("\n");
     }
@@ -1032,26 +1343,41 @@ const double* level_inv<double>(const Level& L) { return L.inv64->as<double>(); 
 template <>
 const float* level_inv<float>(const Level& L) { return L.inv32->as<float>(); }
 
-// out = M^{-1} in for the ILU(0) factors of one level.
+// out = M^{-1} b for the block ILU(0) factors of one level; with zadd,
+// zadd += out as rows finish.  One kernel per stage: forward sweeps of
+// stages 1 .. S-1 (the last one finishing its rows), then backward sweeps
+// of stages S-2 .. 0.
 template <class T>
-void ilu_apply(Core& c, const Level& L, const T* in, T* out, const KScal* sc, int skip_if_s)
+void ilu_apply(Core& c, const Level& L, const T* b, T* out, T* zadd, const KScal* sc, int skip_if_s)
 {
     const T* lu = level_lu<T>(L);
     const int ns = (int)L.stage_ptr.size() - 1;
-    for (int s = 0; s < ns; ++s) {
+    if (ns <= 0) return;
+    const int r_first = L.stage_ptr[1];
+    for (int s = 1; s < ns; ++s) {
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
-        WITH_KMAX(L.kmax, launch(c, "ilu0_lower", [&] {
-            ilu0_lower_stage_kernel<KK, T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(r0, r1, L.view(), lu, in,
-                                                                                          out, sc, skip_if_s);
-        }));
+        const int last = s == ns - 1;
+        WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "bilu_lower", [&] {
+                    bilu_lower_kernel<BS, KK, T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
+                        r0, r1, r_first, last, L.view(), lu, b, out, last ? zadd : nullptr, sc, skip_if_s);
+                })));
     }
-    for (int s = ns - 1; s >= 0; --s) {
+    for (int s = ns >= 2 ? ns - 2 : 0; s >= 0; --s) {
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
-        WITH_KMAX(L.kmax, launch(c, "ilu0_upper", [&] {
-            ilu0_upper_stage_kernel<KK, T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(r0, r1, L.view(), lu, out,
-                                                                                          sc, skip_if_s);
-        }));
+        WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "bilu_upper", [&] {
+                    bilu_upper_kernel<BS, KK, T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
+                        r0, r1, s == 0, L.view(), lu, b, out, zadd, sc, skip_if_s);
+                })));
     }
+}
+
+template <class T>
+void level_residual(Core& c, const Level& L, const T* x, const T* b, T* out, const KScal* sc, int skip_if_s)
+{
+    WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "mg_residual", [&] {
+                mg_residual_kernel<BS, KK, T><<<blocksFor(L.nb), kThreads, 0, c.stream>>>(
+                    L.nb, L.view(), level_a<T>(L), x, b, out, sc, skip_if_s);
+            })));
 }
 
 // z = V-cycle(r) on level l.
@@ -1070,11 +1396,8 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     T* w = level_vec<T>(L, 3);
     T* rc = level_vec<T>(C, 0);
     T* zc = level_vec<T>(C, 1);
-    const T* a = level_a<T>(L);
-    ilu_apply<T>(c, L, r, z, sc, skip);
-    WITH_KMAX(L.kmax, launch(c, "mg_residual", [&] {
-        mg_residual_kernel<KK, T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.view(), a, z, r, t, sc, skip);
-    }));
+    ilu_apply<T>(c, L, r, z, nullptr, sc, skip);
+    level_residual<T>(c, L, z, r, t, sc, skip);
     launch(c, "mg_restrict", [&] {
         mg_restrict_kernel<T><<<blocksFor(C.n), kThreads, 0, c.stream>>>(C.n, L.mptr->as<int>(), L.midx->as<int>(), t,
                                                                           rc, sc, skip);
@@ -1083,18 +1406,15 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     launch(c, "mg_prolong", [&] {
         mg_prolong_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.agg->as<int>(), zc, z, sc, skip);
     });
-    WITH_KMAX(L.kmax, launch(c, "mg_residual", [&] {
-        mg_residual_kernel<KK, T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.view(), a, z, r, t, sc, skip);
-    }));
-    ilu_apply<T>(c, L, t, w, sc, skip);
-    launch(c, "mg_add", [&] { mg_add_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, w, z, sc, skip); });
+    level_residual<T>(c, L, z, r, t, sc, skip);
+    ilu_apply<T>(c, L, t, w, z, sc, skip);  // z += M^{-1} t
 }
 
 template <class T>
 void precondition(Core& c, const SolverAnalysis& an, const T* in, T* out, const KScal* sc, int skip_if_s)
 {
     if (an.multigrid) vcycle<T>(c, an, 0, in, out, sc, skip_if_s);
-    else ilu_apply<T>(c, an.levels[0], in, out, sc, skip_if_s);
+    else ilu_apply<T>(c, an.levels[0], in, out, nullptr, sc, skip_if_s);
 }
 
 // out = M^{-1} in with the FP32 copy of the preconditioner, for FP64 vectors.
@@ -1134,22 +1454,23 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double 
     double* part = an.partials->as<double>();
     unsigned int* cnt = an.counter->as<unsigned int>();
     const int nb = blocksFor(n, kThreads, kRedBlocks);
+    const int nbr = blocksFor(L0.nb, kThreads, kRedBlocks);
     launch(c, "bicg_init", [&] {
         bicg_init_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.b, v.r, v.rhat, v.p, v.v, v.x, n, part, cnt, sc, tol * tol);
     });
     auto iteration = [&] {
         launch(c, "bicg_p", [&] { bicg_p_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(v.r, v.v, v.p, n, sc); });
         apply_pc<T>(c, an, v.p, v.ph, sc, 0, pc32);
-        WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_alpha", [&] {
-            bicg_spmv_alpha_kernel<KK, T><<<nb, kThreads, 0, c.stream>>>(L0.view(), a, v.ph, v.rhat, v.v, n, part, cnt,
-                                                                        sc);
-        }));
+        WITH_BS(L0.bs, WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_alpha", [&] {
+                    bicg_spmv_alpha_kernel<BS, KK, T><<<nbr, kThreads, 0, c.stream>>>(L0.view(), a, v.ph, v.rhat, v.v,
+                                                                                       L0.nb, part, cnt, sc);
+                })));
         launch(c, "bicg_s", [&] { bicg_s_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.r, v.v, v.s, n, part, cnt, sc); });
         apply_pc<T>(c, an, v.s, v.sh, sc, 1, pc32);
-        WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_omega", [&] {
-            bicg_spmv_omega_kernel<KK, T><<<nb, kThreads, 0, c.stream>>>(L0.view(), a, v.sh, v.s, v.t, n, part, cnt,
-                                                                        sc);
-        }));
+        WITH_BS(L0.bs, WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_omega", [&] {
+                    bicg_spmv_omega_kernel<BS, KK, T><<<nbr, kThreads, 0, c.stream>>>(L0.view(), a, v.sh, v.s, v.t,
+                                                                                       L0.nb, part, cnt, sc);
+                })));
         launch(c, "bicg_xr", [&] {
             bicg_xr_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.ph, v.sh, v.s, v.t, v.rhat, v.x, v.r, n, part, cnt, sc);
         });
@@ -1209,14 +1530,14 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double 
 
 void factor_level(Core& c, const Level& L, int* status)
 {
-    EQG_CUDA(cudaMemcpyAsync(L.lu64->ptr, L.a64->ptr, (size_t)L.nnz * 8, cudaMemcpyDeviceToDevice, c.stream));
+    EQG_CUDA(cudaMemcpyAsync(L.lus64->ptr, L.as64->ptr, (size_t)L.vals * 8, cudaMemcpyDeviceToDevice, c.stream));
     const int ns = (int)L.stage_ptr.size() - 1;
     for (int s = 0; s < ns; ++s) {
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
-        launch(c, "ilu0_factor", [&] {
-            ilu0_factor_stage_kernel<<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
-                r0, r1, L.rowptr->as<int>(), L.col->as<int>(), L.diag->as<int>(), L.lu64->as<double>(), status);
-        });
+        WITH_BS(L.bs, launch(c, "bilu_factor", [&] {
+                    bilu_factor_stage_kernel<BS><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
+                        r0, r1, L.view(), L.lus64->as<double>(), status);
+                }));
     }
 }
 
@@ -1257,35 +1578,28 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     c.factor_clock.start(c.stream);
     const Level& L0 = an.levels[0];
     launch(c, "gather_values", [&] {
-        gather_values_kernel<<<blocksFor(an.nnz), kThreads, 0, c.stream>>>(jval, an.vmap->as<int>(),
-                                                                           L0.a64->as<double>(), an.nnz);
+        gather_values_kernel<<<blocksFor(L0.vals), kThreads, 0, c.stream>>>(jval, an.vmap->as<int>(),
+                                                                            L0.as64->as<double>(), L0.vals);
     });
     for (size_t l = 1; l < an.levels.size(); ++l) {
         const Level& F = an.levels[l - 1];
         const Level& C = an.levels[l];
         launch(c, "mg_galerkin", [&] {
-            galerkin_kernel<<<blocksFor(C.nnz), kThreads, 0, c.stream>>>(C.nnz, C.gptr->as<int>(), C.gidx->as<int>(),
-                                                                         F.a64->as<double>(), C.a64->as<double>());
+            galerkin_kernel<<<blocksFor(C.vals), kThreads, 0, c.stream>>>(C.vals, C.gptr->as<int>(), C.gidx->as<int>(),
+                                                                          F.as64->as<double>(), C.as64->as<double>());
         });
     }
     EQG_CUDA(cudaMemsetAsync(an.factor_status->ptr, 0, sizeof(int), c.stream));
     for (auto& L : an.levels) {
-        launch(c, "sell_scatter", [&] {
-            sell_scatter_kernel<<<blocksFor(L.sell_size), kThreads, 0, c.stream>>>(
-                L.sell_size, L.sell_map->as<int>(), L.a64->as<double>(), L.as64->as<double>());
-        });
         if (L.coarsest) {
-            launch(c, "mg_dense_inverse", [&] {
-                dense_inverse_kernel<<<1, 1024, 0, c.stream>>>(L.n, L.rowptr->as<int>(), L.col->as<int>(),
-                                                               L.a64->as<double>(), L.work64->as<double>(),
-                                                               L.inv64->as<double>(), an.factor_status->as<int>());
-            });
+            WITH_BS(L.bs, launch(c, "mg_dense_inverse", [&] {
+                        dense_inverse_kernel<BS><<<1, 1024, 0, c.stream>>>(L.nb, L.view(), L.as64->as<double>(),
+                                                                           L.work64->as<double>(),
+                                                                           L.inv64->as<double>(),
+                                                                           an.factor_status->as<int>());
+                    }));
         } else {
             factor_level(c, L, an.factor_status->as<int>());
-            launch(c, "sell_scatter", [&] {
-                sell_scatter_kernel<<<blocksFor(L.sell_size), kThreads, 0, c.stream>>>(
-                    L.sell_size, L.sell_map->as<int>(), L.lu64->as<double>(), L.lus64->as<double>());
-            });
         }
     }
     Vecs<double> v = vecs<double>(an.vec64->as<double>(), n);
@@ -1293,9 +1607,9 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
            [&] { permute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(rhs, L0.perm->as<int>(), v.b, n); });
     if (mixed || refine) {
         for (auto& L : an.levels) {
-            to_float(c, L.as64, L.as32, L.sell_size);
+            to_float(c, L.as64, L.as32, L.vals);
             if (L.coarsest) to_float(c, L.inv64, L.inv32, (int64_t)L.n * L.n);
-            else to_float(c, L.lus64, L.lus32, L.sell_size);
+            else to_float(c, L.lus64, L.lus32, L.vals);
             if (!L.v32) L.v32 = c.allocN<float>((size_t)4 * (L.n > 0 ? L.n : 1));
         }
         if (refine && !an.vec32) an.vec32 = c.allocN<float>((size_t)10 * n);
@@ -1319,14 +1633,19 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         double* part = an.partials->as<double>();
         unsigned int* cnt = an.counter->as<unsigned int>();
         const int nb = blocksFor(n, kThreads, kRedBlocks);
+        const int nbr = blocksFor(L0.nb, kThreads, kRedBlocks);
         k_fill(c, v.x, 0.0, n);
         Buf rr_dev = c.allocN<double>(2);
         launch(c, "sumsq",
                [&] { sumsq_kernel<<<nb, kThreads, 0, c.stream>>>(v.b, n, part, cnt, rr_dev->as<double>()); });
-        WITH_KMAX(L0.kmax, launch(c, "residual", [&] {
-            residual_kernel<KK><<<nb, kThreads, 0, c.stream>>>(L0.view(), L0.as64->as<double>(), v.x, v.b, v.r, w.b, n,
-                                                               part, cnt, rr_dev->as<double>() + 1);
-        }));
+        auto residual = [&] {
+            WITH_BS(L0.bs, WITH_KMAX(L0.kmax, launch(c, "residual", [&] {
+                        residual_kernel<BS, KK><<<nbr, kThreads, 0, c.stream>>>(
+                            L0.view(), L0.as64->as<double>(), v.x, v.b, v.r, w.b, L0.nb, part, cnt,
+                            rr_dev->as<double>() + 1);
+                    })));
+        };
+        residual();
         EQG_CUDA(cudaMemcpyAsync(c.pinned, rr_dev->ptr, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
         c.sync();
         const double bb = c.pinned[0];
@@ -1340,10 +1659,7 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
             ++sweeps;
             launch(c, "add_float",
                    [&] { add_float_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, w.x, n); });
-            WITH_KMAX(L0.kmax, launch(c, "residual", [&] {
-                residual_kernel<KK><<<nb, kThreads, 0, c.stream>>>(L0.view(), L0.as64->as<double>(), v.x, v.b, v.r,
-                                                                   w.b, n, part, cnt, rr_dev->as<double>() + 1);
-            }));
+            residual();
             EQG_CUDA(cudaMemcpyAsync(c.pinned, rr_dev->as<double>() + 1, sizeof(double), cudaMemcpyDeviceToHost,
                                      c.stream));
             c.sync();
@@ -1359,6 +1675,8 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     c.krylov_clock.stop(c.stream);
     launch(c, "unpermute",
            [&] { unpermute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, L0.perm->as<int>(), xout, n); });
+    res.block_size = L0.bs;
+    res.blocks = L0.blocks;
     return res;
 }
 

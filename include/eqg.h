@@ -97,6 +97,11 @@ typedef struct eqg_stats {
     double residual_ms;
     double factor_ms;
     double krylov_ms;
+    /* Layout of the last linear system in the preconditioner: block size
+     * (unknowns per block row) and stored blocks (1 and the nonzeros for a
+     * scalar layout; the oracle always reports a scalar layout). */
+    int64_t last_block_size;
+    int64_t last_matrix_blocks;
 } eqg_stats;
 
 /* ---- errors and identity -------------------------------------------- */
@@ -113,7 +118,9 @@ const char* eqg_backend_name(void);
  * ilu0), linsolver_ordering (multicolor | natural),
  * linsolver_precision (double | mixed: FP32 preconditioner | refine: FP32
  * BiCGStab inside FP64 refinement), linsolver_inner_tolerance (1e-4) and
- * linsolver_max_sweeps (60) for refine, linsolver_check_every (8), time_kernel
+ * linsolver_max_sweeps (60) for refine, linsolver_check_every (8),
+ * linsolver_block (1: ncomp x ncomp block ILU(0) for 2 or 3 unknowns per
+ * cell; 0: scalar ILU(0)), time_kernel
  * (a kernel name, or "*", to time with CUDA events) and device (CUDA device
  * index; default: the calling thread's current device).  grid_filename is
  * rejected with EQG_ERR_UNSUPPORTED.

@@ -1533,6 +1533,8 @@ int eqg_solve_for_update(eqg_runtime* rt, const eqg_coll* residual, eqg_coll** d
         rt->stats.krylov_ms += rep.krylov_ms;
         rt->stats.last_matrix_rows = r.jac.rows;
         rt->stats.last_matrix_nnz = r.jac.nnz();
+        rt->stats.last_block_size = 1;
+        rt->stats.last_matrix_blocks = r.jac.nnz();
         if (rt->verbose > 2)
             std::printf("        solveForUpdate: BiCGStab+ILU0 %d iterations, rel. residual %g\n", rep.iterations,
                         rep.rel_residual);

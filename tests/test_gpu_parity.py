@@ -81,6 +81,8 @@ def test_heat_64x64_parity(gpu_lib, oracle_lib, ordering, precond):
                                                      ((8, 8, 4), "double", "multigrid"),
                                                      ((8, 8, 4), "mixed", "multigrid"),
                                                      ((16, 16, 8), "double", "multigrid"),
+                                                     ((16, 16, 8), "mixed", "multigrid"),
+                                                     ((16, 16, 8), "double", "ilu0"),
                                                      ((16, 16, 8), "mixed", "ilu0"),
                                                      ((16, 16, 8), "refine", "ilu0")])
 def test_two_phase_parity(gpu_lib, oracle_lib, shape, precision, precond):
@@ -99,3 +101,68 @@ def test_two_phase_parity(gpu_lib, oracle_lib, shape, precision, precond):
     if precision == "refine":
         assert st["refinement_sweeps"] >= st["linear_solves"] > 0
 
+
+
+def reaction_diffusion3(er, fields, rates, timesteps):
+    """Three species on all cells, implicit in time: diffusion with no-flow
+    boundaries and a nonlinear exchange a <-> b <-> c, solved together with
+    newtonSolveSystem (3 x 3 blocks per cell).  Returns (a, b, c) per step."""
+    ifaces = er.interiorFaces()
+    first = er.firstCell(ifaces)
+    second = er.secondCell(ifaces)
+    trans = er.norm(ifaces) / er.norm(er.centroid(first) - er.centroid(second))
+    vol = er.norm(er.allCells())
+    k1, k2, d = rates
+
+    def div_flux(x, diff):
+        return er.divergence(er.operatorExtend(-(diff * trans) * er.gradient(x), er.interiorFaces(), er.allFaces()))
+
+    olds = [er.collection(f) for f in fields]
+    out = []
+    for dt in timesteps:
+        a0, b0, c0 = olds
+
+        def ra(a, b, c):
+            return (a - a0) + (dt / vol) * div_flux(a, d[0]) + dt * (k1 * a * b - k2 * c)
+
+        def rb(a, b, c):
+            return (b - b0) + (dt / vol) * div_flux(b, d[1]) + dt * (k1 * a * b - k2 * c)
+
+        def rc(a, b, c):
+            return (c - c0) + (dt / vol) * div_flux(c, d[2]) - dt * (k1 * a * b - k2 * c)
+
+        olds = list(er.newtonSolveSystem([ra, rb, rc], olds))
+        out.append(tuple(x.value() for x in olds))
+    return out
+
+
+@pytest.mark.parametrize("shape,precond", [((12, 10, 6), "multigrid"), ((12, 10, 6), "ilu0"), ((40, 30, None), "multigrid")])
+def test_three_species_blocks_parity(gpu_lib, oracle_lib, shape, precond):
+    """A 3-unknowns-per-cell system (3 x 3 block ILU(0)): every species
+    within 1e-9 relative of the FP64 oracle after every step."""
+    nx, ny, nz = shape
+    grid = dict(grid_dim=2 if nz is None else 3, nx=nx, ny=ny, nz=nz or 1, dx=1.0, dy=1.0, dz=1.0)
+    n = nx * ny * (nz or 1)
+    rng = np.random.RandomState(3)
+    fields = [1.0 + rng.rand(n), 0.5 + rng.rand(n), 0.1 * rng.rand(n)]
+    args = (fields, (2.0, 0.5, (1.0, 0.3, 0.05)), [0.1, 0.2, 0.2])
+    params = dict(grid, abs_res_tol=1e-12, linsolver_residual_tolerance=1e-12, linsolver_max_iterations=5000)
+    og = reaction_diffusion3(Runtime(gpu_lib, dict(params, linsolver_preconditioner=precond)), *args)
+    oo = reaction_diffusion3(Runtime(oracle_lib, params), *args)
+    for step, (g, o) in enumerate(zip(og, oo)):
+        for k in range(3):
+            assert np.max(np.abs(g[k] - o[k]) / np.abs(o[k])) <= 1e-9, "species %d step %d" % (k, step)
+
+
+@pytest.mark.parametrize("block,ordering", [(0, "multicolor"), (0, "natural"), (1, "multicolor")])
+def test_two_phase_block_layouts(gpu_lib, oracle_lib, block, ordering):
+    """The same two-phase case with 2 x 2 blocks per cell and with 1 x 1
+    blocks (scalar ILU(0), multicolour or natural order): saturation within
+    1e-8 relative of the oracle."""
+    grid, case = programs.two_phase_case(8, 8, 4, steps=2)
+    params = dict(grid, abs_res_tol=1e-11, linsolver_residual_tolerance=1e-12, linsolver_max_iterations=5000)
+    eg = Runtime(gpu_lib, dict(params, linsolver_block=block, linsolver_ordering=ordering))
+    og = programs.two_phase(eg, **case)
+    oo = programs.two_phase(Runtime(oracle_lib, params), **case)
+    for step, ((pg, sg), (po, so)) in enumerate(zip(og, oo)):
+        assert np.max(np.abs(sg - so) / np.abs(so)) <= 1e-8, "Sw step %d" % step
