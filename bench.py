@@ -306,7 +306,7 @@ def main():
         "krylov_iterations_per_step": infos["krylov"] / K,
         "cell_updates_per_s": world * K * cells / (ms / 1000.0),
         "gpu_launches": infos["launches"],
-        "phase_ms_total": {"residual": st.residual_ms, "factor": st.factor_ms, "krylov": st.krylov_ms},
+        "phase_ms_per_step": {k: infos[k + "_ms"] / K for k in ("residual", "factor", "krylov")},
         "roofline": roofline,
         "clocks": clk.summary(),
     }
@@ -360,6 +360,8 @@ def window_counts(rep, w, k):
     newton = sum(s.newton_iterations for s in sel)
     return {"newton": newton, "krylov": sum(s.krylov_iterations for s in sel),
             "launches": sum(s.kernel_launches for s in sel),
+            "residual_ms": sum(s.residual_ms for s in sel), "factor_ms": sum(s.factor_ms for s in sel),
+            "krylov_ms": sum(s.krylov_ms for s in sel),
             "residuals": newton + k, "solves": newton,
             "unconverged_steps": sum(1 for s in sel if not s.converged)}
 

@@ -63,6 +63,7 @@ class SolveInfo(C.Structure):
     _fields_ = [
         ("start_mark", C.c_int), ("end_mark", C.c_int), ("newton_iterations", C.c_int),
         ("converged", C.c_int), ("krylov_iterations", C.c_int64), ("kernel_launches", C.c_int64),
+        ("residual_ms", C.c_double), ("factor_ms", C.c_double), ("krylov_ms", C.c_double),
     ]
 
 

@@ -1209,6 +1209,8 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
         c.newton_solves++;
         const int64_t krylov0 = c.solver.krylov_iterations;
         const int64_t launches0 = c.launches.load();
+        const size_t rp0 = c.residual_clock.pairs.size(), fp0 = c.factor_clock.pairs.size(),
+                     kp0 = c.krylov_clock.pairs.size();
         struct Ref {
             eqg_coll* p = nullptr;
             ~Ref() { eqg_coll_release(p); }
@@ -1267,6 +1269,9 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
         info.converged = norm <= c.abs_res_tol ? 1 : 0;
         info.krylov_iterations = c.solver.krylov_iterations - krylov0;
         info.kernel_launches = c.launches.load() - launches0;
+        info.residual_ms = c.residual_clock.ms_from(rp0);
+        info.factor_ms = c.factor_clock.ms_from(fp0);
+        info.krylov_ms = c.krylov_clock.ms_from(kp0);
         info.end_mark = mark(c);
         c.solves.push_back(info);
     });

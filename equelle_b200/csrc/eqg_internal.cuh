@@ -110,13 +110,15 @@ struct PhaseClock {
         open = nullptr;
         ++count;
     }
-    double total_ms() const
+    double total_ms() const { return ms_from(0); }
+    // time of the intervals first .. end
+    double ms_from(size_t first) const
     {
         double ms = 0.0;
-        for (auto& p : pairs) {
+        for (size_t i = first; i < pairs.size(); ++i) {
             float f = 0.f;
-            cudaEventSynchronize(p.second);
-            cudaEventElapsedTime(&f, p.first, p.second);
+            cudaEventSynchronize(pairs[i].second);
+            cudaEventElapsedTime(&f, pairs[i].first, pairs[i].second);
             ms += f;
         }
         return ms;

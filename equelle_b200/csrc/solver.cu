@@ -34,8 +34,9 @@
 // which keeps the iteration count of the elliptic pressure part from growing
 // with the grid; "ilu0": the staged block ILU(0) alone.
 //
-// Precision "mixed": BiCGStab in FP64, the preconditioner (V-cycle or ILU
-// sweeps, with FP32 copies of the factors and level matrices) in FP32.
+// Precision "mixed": BiCGStab and every vector in FP64, the preconditioner's
+// matrices (level matrices, block ILU(0) factors, coarsest inverse) stored
+// in FP32: the V-cycle reads about half the bytes, in FP64 arithmetic.
 // Precision "refine": the inner BiCGStab and the preconditioner in FP32,
 // inside FP64 iterative refinement (r = b - A x in FP64 with FP64 A).
 //
@@ -152,20 +153,24 @@ struct SellView {
     const int* __restrict__ dk;         // position of the diagonal block in each row
 };
 
-template <int B, class T>
+// Block J of a vector.  With CG the loads bypass L1 (ld.global.cg): for
+// vectors that other thread blocks of the same kernel wrote.
+template <int B, class T, bool CG = false>
 __device__ __forceinline__ void load_bvec(const T* __restrict__ x, int J, double (&v)[B])
 {
     if constexpr (B == 2 && sizeof(T) == 8) {
-        const double2 t = reinterpret_cast<const double2*>(x)[J];
+        const double2* p = reinterpret_cast<const double2*>(x) + J;
+        const double2 t = CG ? __ldcg(p) : *p;
         v[0] = t.x;
         v[1] = t.y;
     } else if constexpr (B == 2 && sizeof(T) == 4) {
-        const float2 t = reinterpret_cast<const float2*>(x)[J];
+        const float2* p = reinterpret_cast<const float2*>(x) + J;
+        const float2 t = CG ? __ldcg(p) : *p;
         v[0] = (double)t.x;
         v[1] = (double)t.y;
     } else {
 #pragma unroll
-        for (int c = 0; c < B; ++c) v[c] = (double)x[J * B + c];
+        for (int c = 0; c < B; ++c) v[c] = (double)(CG ? __ldcg(x + J * B + c) : x[J * B + c]);
     }
 }
 
@@ -181,8 +186,8 @@ __device__ __forceinline__ void store_bvec(T* __restrict__ x, int R, const doubl
 // from `x2` otherwise.  With KM > 0 (rows of at most KM blocks) the loop is
 // unrolled so that a thread issues its column loads before the dependent
 // gathers of x: the kernels using it are bound by the latency of that chain.
-template <int B, int KM, class T>
-__device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int k0, int k1, const T* __restrict__ a,
+template <int B, int KM, class T, class M, bool CG = false>
+__device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int k0, int k1, const M* __restrict__ a,
                                      const T* __restrict__ x, const T* __restrict__ x2, int split, double (&acc)[B])
 {
     constexpr int BB = B * B;
@@ -191,8 +196,8 @@ __device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int
             const int q = sbase + (k << 5);
             const int J = m.col[q + lane];
             double xv[B];
-            load_bvec<B, T>(J < split ? x : x2, J, xv);
-            const T* av = a + (size_t)q * BB + lane;
+            load_bvec<B, T, CG>(J < split ? x : x2, J, xv);
+            const M* av = a + (size_t)q * BB + lane;
 #pragma unroll
             for (int i = 0; i < B; ++i)
 #pragma unroll
@@ -202,20 +207,20 @@ __device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int
         // columns and values of the whole row first (predicated loads), then
         // the gathers of x
         int ci[KM];
-        T av[KM][BB];
+        M av[KM][BB];
 #pragma unroll
         for (int k = 0; k < KM; ++k) {
             const bool on = k >= k0 && k < k1;
             const int q = sbase + (k << 5);
             ci[k] = on ? m.col[q + lane] : 0;
 #pragma unroll
-            for (int e = 0; e < BB; ++e) av[k][e] = on ? a[(size_t)q * BB + (e << 5) + lane] : (T)0;
+            for (int e = 0; e < BB; ++e) av[k][e] = on ? a[(size_t)q * BB + (e << 5) + lane] : (M)0;
         }
 #pragma unroll
         for (int k = 0; k < KM; ++k) {
             if (k >= k0 && k < k1) {
                 double xv[B];
-                load_bvec<B, T>(ci[k] < split ? x : x2, ci[k], xv);
+                load_bvec<B, T, CG>(ci[k] < split ? x : x2, ci[k], xv);
 #pragma unroll
                 for (int i = 0; i < B; ++i)
 #pragma unroll
@@ -231,8 +236,8 @@ __device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int
             if (k >= k0 && k < k1) {
                 const int q = sbase + (k << 5);
                 double xv[B];
-                load_bvec<B, T>(ci[k] < split ? x : x2, ci[k], xv);
-                const T* av = a + (size_t)q * BB + lane;
+                load_bvec<B, T, CG>(ci[k] < split ? x : x2, ci[k], xv);
+                const M* av = a + (size_t)q * BB + lane;
 #pragma unroll
                 for (int i = 0; i < B; ++i)
 #pragma unroll
@@ -244,10 +249,10 @@ __device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int
 
 // y = D x for the block at slot position `q` (its first value at
 // a[q B^2 + lane], values 32 apart).
-template <int B, class T>
-__device__ __forceinline__ void bmatvec(const T* __restrict__ a, int q, int lane, const double (&x)[B], double (&y)[B])
+template <int B, class M>
+__device__ __forceinline__ void bmatvec(const M* __restrict__ a, int q, int lane, const double (&x)[B], double (&y)[B])
 {
-    const T* av = a + (size_t)q * (B * B) + lane;
+    const M* av = a + (size_t)q * (B * B) + lane;
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         double s = 0.0;
@@ -430,42 +435,49 @@ __device__ __forceinline__ bool mg_skip(const KScal* sc, int skip_if_s)
     return stopped(sc) || (skip_if_s && sc->s_conv);
 }
 
+// zadd_R += z
+template <int B, class T, bool CG = false>
+__device__ __forceinline__ void update_z(T* __restrict__ zadd, int R, const double (&z)[B])
+{
+    double w[B];
+    load_bvec<B, T, CG>(zadd, R, w);
+#pragma unroll
+    for (int c = 0; c < B; ++c) w[c] += z[c];
+    store_bvec<B, T>(zadd, R, w);
+}
+
+// The multigrid steps below are written as loops over a row range for
+// thread `tid` of `nth`, shared by the one-step kernels (CG = false) and by
+// the fused coarse cycle (mg_tail_kernel, CG = true), so that both compute
+// every element with the same operations.
+
 // Forward sweep of stage [r0, r1), a stage after the first:
 //   y_R = b_R - sum_{k < dk} L_Rk y_K,
 // with y_K = b_K for rows of the first stage (K < r_first) and out_K
 // otherwise.  The last stage has no upper part: there the row is finished,
 // out_R = D_R^{-1} y_R (and zadd_R += out_R when zadd is given).
-template <int B, int KM, class T>
-__global__ void bilu_lower_kernel(int r0, int r1, int r_first, int last, SellView m, const T* __restrict__ lu,
-                                  const T* __restrict__ b, T* __restrict__ out, T* __restrict__ zadd,
-                                  const KScal* sc, int skip_if_s)
+template <int B, int KM, class T, class M, bool CG>
+__device__ __forceinline__ void lower_rows(int r0, int r1, int r_first, int last, const SellView& m,
+                                           const M* __restrict__ lu, const T* __restrict__ b, T* __restrict__ out,
+                                           T* __restrict__ zadd, int tid, int nth)
 {
-    if (mg_skip(sc, skip_if_s)) return;
-    for (int64_t rr = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; rr < r1;
-         rr += (int64_t)gridDim.x * blockDim.x) {
-        const int R = (int)rr;
+    for (int R = r0 + tid; R < r1; R += nth) {
         const int lane = R & 31, sb = m.slice_ptr[R >> 5], d = m.dk[R];
         double acc[B];
 #pragma unroll
         for (int c = 0; c < B; ++c) acc[c] = 0.0;
-        bdot<B, KM, T>(m, sb, lane, 0, d, lu, b, out, r_first, acc);
+        bdot<B, KM, T, M, CG>(m, sb, lane, 0, d, lu, b, out, r_first, acc);
         double y[B];
-        load_bvec<B, T>(b, R, y);
+        load_bvec<B, T, CG>(b, R, y);
 #pragma unroll
         for (int c = 0; c < B; ++c) y[c] = (double)(T)(y[c] - acc[c]);
         if (last) {
             double z[B];
-            bmatvec<B, T>(lu, sb + (d << 5), lane, y, z);
+            bmatvec<B, M>(lu, sb + (d << 5), lane, y, z);
 #pragma unroll
             for (int c = 0; c < B; ++c) z[c] = (double)(T)z[c];
             store_bvec<B, T>(out, R, z);
-            if (zadd) {
-                double w[B];
-                load_bvec<B, T>(zadd, R, w);
-#pragma unroll
-                for (int c = 0; c < B; ++c) w[c] += z[c];
-                store_bvec<B, T>(zadd, R, w);
-            }
+            if (zadd) update_z<B, T, CG>(zadd, R, z);
         } else {
             store_bvec<B, T>(out, R, y);
         }
@@ -476,37 +488,114 @@ __global__ void bilu_lower_kernel(int r0, int r1, int r_first, int last, SellVie
 //   out_R = D_R^{-1} (y_R - sum_{k > dk} U_Rk out_K),
 // with y_R = b_R in the first stage and the forward-sweep value out_R
 // otherwise; zadd_R += out_R when zadd is given.
-template <int B, int KM, class T>
-__global__ void bilu_upper_kernel(int r0, int r1, int first, SellView m, const T* __restrict__ lu,
-                                  const T* __restrict__ b, T* __restrict__ out, T* __restrict__ zadd,
-                                  const KScal* sc, int skip_if_s)
+template <int B, int KM, class T, class M, bool CG>
+__device__ __forceinline__ void upper_rows(int r0, int r1, int first, const SellView& m, const M* __restrict__ lu,
+                                           const T* __restrict__ b, T* __restrict__ out, T* __restrict__ zadd,
+                                           int tid, int nth)
 {
-    if (mg_skip(sc, skip_if_s)) return;
-    for (int64_t rr = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; rr < r1;
-         rr += (int64_t)gridDim.x * blockDim.x) {
-        const int R = (int)rr;
+    for (int R = r0 + tid; R < r1; R += nth) {
         const int lane = R & 31, sb = m.slice_ptr[R >> 5], d = m.dk[R];
         double acc[B];
 #pragma unroll
         for (int c = 0; c < B; ++c) acc[c] = 0.0;
-        bdot<B, KM, T>(m, sb, lane, d + 1, m.len[R], lu, out, out, INT_MAX, acc);
+        bdot<B, KM, T, M, CG>(m, sb, lane, d + 1, m.len[R], lu, out, out, INT_MAX, acc);
         double y[B];
-        load_bvec<B, T>(first ? b : out, R, y);
+        load_bvec<B, T, CG>(first ? b : out, R, y);
 #pragma unroll
         for (int c = 0; c < B; ++c) y[c] -= acc[c];
         double z[B];
-        bmatvec<B, T>(lu, sb + (d << 5), lane, y, z);
+        bmatvec<B, M>(lu, sb + (d << 5), lane, y, z);
 #pragma unroll
         for (int c = 0; c < B; ++c) z[c] = (double)(T)z[c];
         store_bvec<B, T>(out, R, z);
-        if (zadd) {
-            double w[B];
-            load_bvec<B, T>(zadd, R, w);
-#pragma unroll
-            for (int c = 0; c < B; ++c) w[c] += z[c];
-            store_bvec<B, T>(zadd, R, w);
-        }
+        if (zadd) update_z<B, T, CG>(zadd, R, z);
     }
+}
+
+// out = b - A x.  Block rows below r_zero get 0 without being computed:
+// after a full ILU(0) sweep their residual is zero (see vcycle).
+template <int B, int KM, class T, class M, bool CG>
+__device__ __forceinline__ void residual_rows(int nb, int r_zero, const SellView& m, const M* __restrict__ a,
+                                              const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ out,
+                                              int tid, int nth)
+{
+    for (int R = tid; R < nb; R += nth) {
+        if (R < r_zero) {
+#pragma unroll
+            for (int c = 0; c < B; ++c) out[R * B + c] = (T)0;
+            continue;
+        }
+        double acc[B];
+#pragma unroll
+        for (int c = 0; c < B; ++c) acc[c] = 0.0;
+        bdot<B, KM, T, M, CG>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, x, x, INT_MAX, acc);
+        double y[B];
+        load_bvec<B, T, CG>(b, R, y);
+#pragma unroll
+        for (int c = 0; c < B; ++c) y[c] -= acc[c];
+        store_bvec<B, T>(out, R, y);
+    }
+}
+
+// rc[P] = sum of t over the members of aggregate P
+template <class T, bool CG>
+__device__ __forceinline__ void restrict_rows(int nc, const int* __restrict__ mptr, const int* __restrict__ midx,
+                                              const T* __restrict__ t, T* __restrict__ rc, int tid, int nth)
+{
+    for (int P = tid; P < nc; P += nth) {
+        double s = 0.0;
+        const int k1 = mptr[P + 1];
+        for (int k = mptr[P]; k < k1; ++k) s += (double)(CG ? __ldcg(t + midx[k]) : t[midx[k]]);
+        rc[P] = (T)s;
+    }
+}
+
+// z_R += zc_{aggb[R]} (piecewise-constant prolongation, per block row)
+template <int B, class T, bool CG>
+__device__ __forceinline__ void prolong_rows(int nb, const int* __restrict__ aggb, const T* __restrict__ zc,
+                                             T* __restrict__ z, int tid, int nth)
+{
+    for (int R = tid; R < nb; R += nth) {
+        double e[B];
+        load_bvec<B, T, CG>(zc, aggb[R], e);
+        update_z<B, T, CG>(z, R, e);
+    }
+}
+
+// z = inv r with the dense inverse of the coarsest level
+template <class T, class M, bool CG>
+__device__ __forceinline__ void dense_rows(int n, const M* __restrict__ inv, const T* __restrict__ r,
+                                           T* __restrict__ z, int tid, int nth)
+{
+    for (int i = tid; i < n; i += nth) {
+        double s = 0.0;
+        for (int j = 0; j < n; ++j) s += (double)inv[i * n + j] * (double)(CG ? __ldcg(r + j) : r[j]);
+        z[i] = (T)s;
+    }
+}
+
+#define THREAD_RANGE                                                 \
+    const int tid = (int)(blockIdx.x * blockDim.x + threadIdx.x); \
+    const int nth = (int)(gridDim.x * blockDim.x)
+
+template <int B, int KM, class T, class M>
+__global__ void bilu_lower_kernel(int r0, int r1, int r_first, int last, SellView m, const M* __restrict__ lu,
+                                  const T* __restrict__ b, T* __restrict__ out, T* __restrict__ zadd,
+                                  const KScal* sc, int skip_if_s)
+{
+    if (mg_skip(sc, skip_if_s)) return;
+    THREAD_RANGE;
+    lower_rows<B, KM, T, M, false>(r0, r1, r_first, last, m, lu, b, out, zadd, tid, nth);
+}
+
+template <int B, int KM, class T, class M>
+__global__ void bilu_upper_kernel(int r0, int r1, int first, SellView m, const M* __restrict__ lu,
+                                  const T* __restrict__ b, T* __restrict__ out, T* __restrict__ zadd,
+                                  const KScal* sc, int skip_if_s)
+{
+    if (mg_skip(sc, skip_if_s)) return;
+    THREAD_RANGE;
+    upper_rows<B, KM, T, M, false>(r0, r1, first, m, lu, b, out, zadd, tid, nth);
 }
 
 // ---- BiCGStab steps -----------------------------------------------------------
@@ -578,7 +667,7 @@ __global__ void bicg_spmv_alpha_kernel(SellView m, const T* __restrict__ a, cons
         double acc[B];
 #pragma unroll
         for (int c = 0; c < B; ++c) acc[c] = 0.0;
-        bdot<B, KM, T>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, ph, ph, INT_MAX, acc);
+        bdot<B, KM, T, T>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, ph, ph, INT_MAX, acc);
         double h[B];
         load_bvec<B, T>(rhat, R, h);
 #pragma unroll
@@ -631,7 +720,7 @@ __global__ void bicg_spmv_omega_kernel(SellView m, const T* __restrict__ a, cons
         double acc[B];
 #pragma unroll
         for (int c = 0; c < B; ++c) acc[c] = 0.0;
-        bdot<B, KM, T>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, sh, sh, INT_MAX, acc);
+        bdot<B, KM, T, T>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, sh, sh, INT_MAX, acc);
         double sv[B];
         load_bvec<B, T>(s, R, sv);
 #pragma unroll
@@ -704,7 +793,7 @@ __global__ void residual_kernel(SellView m, const double* __restrict__ a, const 
         double acc[B];
 #pragma unroll
         for (int c = 0; c < B; ++c) acc[c] = 0.0;
-        bdot<B, KM, double>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, x, x, INT_MAX, acc);
+        bdot<B, KM, double, double>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, x, x, INT_MAX, acc);
 #pragma unroll
         for (int c = 0; c < B; ++c) {
             const double ri = b[R * B + c] - acc[c];
@@ -751,49 +840,31 @@ __global__ void galerkin_kernel(int64_t size_c, const int* __restrict__ gptr, co
     }
 }
 
-// out = b - A x
-template <int B, int KM, class T>
-__global__ void mg_residual_kernel(int nb, SellView m, const T* __restrict__ a, const T* __restrict__ x,
+template <int B, int KM, class T, class M>
+__global__ void mg_residual_kernel(int nb, int r_zero, SellView m, const M* __restrict__ a, const T* __restrict__ x,
                                    const T* __restrict__ b, T* __restrict__ out, const KScal* sc, int skip_if_s)
 {
     if (mg_skip(sc, skip_if_s)) return;
-    GRID_STRIDE(rr, nb)
-    {
-        const int R = (int)rr;
-        double acc[B];
-#pragma unroll
-        for (int c = 0; c < B; ++c) acc[c] = 0.0;
-        bdot<B, KM, T>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, x, x, INT_MAX, acc);
-        double y[B];
-        load_bvec<B, T>(b, R, y);
-#pragma unroll
-        for (int c = 0; c < B; ++c) y[c] -= acc[c];
-        store_bvec<B, T>(out, R, y);
-    }
+    THREAD_RANGE;
+    residual_rows<B, KM, T, M, false>(nb, r_zero, m, a, x, b, out, tid, nth);
 }
 
-// rc[P] = sum of t over the members of aggregate P
 template <class T>
 __global__ void mg_restrict_kernel(int nc, const int* __restrict__ mptr, const int* __restrict__ midx,
                                    const T* __restrict__ t, T* __restrict__ rc, const KScal* sc, int skip_if_s)
 {
     if (mg_skip(sc, skip_if_s)) return;
-    GRID_STRIDE(P, nc)
-    {
-        double s = 0.0;
-        const int k1 = mptr[P + 1];
-        for (int k = mptr[P]; k < k1; ++k) s += (double)t[midx[k]];
-        rc[P] = (T)s;
-    }
+    THREAD_RANGE;
+    restrict_rows<T, false>(nc, mptr, midx, t, rc, tid, nth);
 }
 
-// z[i] += ec[agg[i]] (piecewise-constant prolongation)
-template <class T>
-__global__ void mg_prolong_kernel(int n, const int* __restrict__ agg, const T* __restrict__ ec, T* __restrict__ z,
+template <int B, class T>
+__global__ void mg_prolong_kernel(int nb, const int* __restrict__ aggb, const T* __restrict__ zc, T* __restrict__ z,
                                   const KScal* sc, int skip_if_s)
 {
     if (mg_skip(sc, skip_if_s)) return;
-    GRID_STRIDE(i, n) z[i] = (T)((double)z[i] + (double)ec[agg[i]]);
+    THREAD_RANGE;
+    prolong_rows<B, T, false>(nb, aggb, zc, z, tid, nth);
 }
 
 // Inverse of the coarsest matrix (n <= kCoarsest unknowns) by Gauss-Jordan
@@ -864,31 +935,105 @@ __global__ void dense_inverse_kernel(int nb, SellView m, const double* __restric
     }
 }
 
-template <class T>
-__global__ void dense_apply_kernel(int n, const T* __restrict__ inv, const T* __restrict__ r, T* __restrict__ z,
+template <class T, class M>
+__global__ void dense_apply_kernel(int n, const M* __restrict__ inv, const T* __restrict__ r, T* __restrict__ z,
                                    const KScal* sc, int skip_if_s)
 {
     if (mg_skip(sc, skip_if_s)) return;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double s = 0.0;
-        for (int j = 0; j < n; ++j) s += (double)inv[i * n + j] * (double)r[j];
-        z[i] = (T)s;
+    dense_rows<T, M, false>(n, inv, r, z, (int)threadIdx.x, (int)blockDim.x);
+}
+
+// ---- the coarse end of the V-cycle in one kernel ------------------------------
+// Below a size threshold a level of the V-cycle is a few microseconds of
+// work spread over seven dependent launches.  mg_tail_kernel runs the whole
+// cycle from one level down to the dense coarsest solve and back on a single
+// thread-block cluster, with a cluster barrier (release/acquire at cluster
+// scope) where the launch-per-step cycle has a kernel boundary, through the
+// same row-range steps, so both give identical results.  Vectors written
+// inside the kernel are read with L2-only loads.  Every thread passes every
+// barrier: loop bounds are kernel parameters or device arrays that do not
+// change while it runs, and so is the early-exit flag (a converged solve).
+constexpr int kTailThreads = 512;
+constexpr int kMaxTail = 12;
+
+template <class T, class M>
+struct TailLevel {
+    int nb = 0, n = 0, coarsest = 0;
+    SellView m{};
+    const M* a = nullptr;
+    const M* lu = nullptr;
+    const M* inv = nullptr;      // coarsest level
+    const int* stage_ptr = nullptr;
+    int nstages = 0;
+    const int* aggb = nullptr;   // to the next coarser level
+    const int* mptr = nullptr;
+    const int* midx = nullptr;
+    T *r = nullptr, *z = nullptr, *t = nullptr, *w = nullptr;
+};
+
+template <class T, class M>
+struct TailParams {
+    TailLevel<T, M> lv[kMaxTail];
+    int nlev = 0;
+};
+
+__device__ __forceinline__ void cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+
+// out = M^{-1} b on one level (zadd += out when given), stage by stage.
+template <int B, int KM, class T, class M>
+__device__ __forceinline__ void tail_ilu(const TailLevel<T, M>& L, const T* b, T* out, T* zadd, int tid, int nth)
+{
+    const int ns = L.nstages;
+    if (ns <= 0) return;
+    const int r_first = L.stage_ptr[1];
+    for (int s = 1; s < ns; ++s) {
+        const int last = s == ns - 1;
+        lower_rows<B, KM, T, M, true>(L.stage_ptr[s], L.stage_ptr[s + 1], r_first, last, L.m, L.lu, b, out,
+                                   last ? zadd : nullptr, tid, nth);
+        cluster_barrier();
+    }
+    for (int s = ns >= 2 ? ns - 2 : 0; s >= 0; --s) {
+        upper_rows<B, KM, T, M, true>(L.stage_ptr[s], L.stage_ptr[s + 1], s == 0, L.m, L.lu, b, out, zadd, tid, nth);
+        cluster_barrier();
     }
 }
 
-// FP64 <-> FP32 copies around an FP32 preconditioner.
-__global__ void pc_to_f32_kernel(const double* __restrict__ a, float* __restrict__ b, int n, const KScal* sc,
-                                 int skip_if_s)
+// z = V-cycle(r) from level lv[0] down; r and z of lv[0] are r_top, z_top.
+template <int B, int KM, class T, class M>
+__global__ void __launch_bounds__(kTailThreads)
+    mg_tail_kernel(const __grid_constant__ TailParams<T, M> p, const T* r_top, T* z_top, const KScal* sc, int skip_if_s)
 {
     if (mg_skip(sc, skip_if_s)) return;
-    GRID_STRIDE(i, n) b[i] = (float)a[i];
-}
-
-__global__ void pc_to_f64_kernel(const float* __restrict__ a, double* __restrict__ b, int n, const KScal* sc,
-                                 int skip_if_s)
-{
-    if (mg_skip(sc, skip_if_s)) return;
-    GRID_STRIDE(i, n) b[i] = (double)a[i];
+    THREAD_RANGE;
+    int l = 0;
+    for (;; ++l) {
+        const TailLevel<T, M>& L = p.lv[l];
+        const T* r = l == 0 ? r_top : L.r;
+        T* z = l == 0 ? z_top : L.z;
+        if (L.coarsest || l == p.nlev - 1) {
+            dense_rows<T, M, true>(L.n, L.inv, r, z, tid, nth);
+            cluster_barrier();
+            break;
+        }
+        tail_ilu<B, KM, T, M>(L, r, z, nullptr, tid, nth);
+        residual_rows<B, KM, T, M, true>(L.nb, L.nstages >= 1 ? L.stage_ptr[1] : 0, L.m, L.a, z, r, L.t, tid, nth);
+        cluster_barrier();
+        restrict_rows<T, true>(p.lv[l + 1].n, L.mptr, L.midx, L.t, p.lv[l + 1].r, tid, nth);
+        cluster_barrier();
+    }
+    for (--l; l >= 0; --l) {
+        const TailLevel<T, M>& L = p.lv[l];
+        const T* r = l == 0 ? r_top : L.r;
+        T* z = l == 0 ? z_top : L.z;
+        prolong_rows<B, T, true>(L.nb, L.aggb, p.lv[l + 1].z, z, tid, nth);
+        cluster_barrier();
+        residual_rows<B, KM, T, M, true>(L.nb, 0, L.m, L.a, z, r, L.t, tid, nth);
+        cluster_barrier();
+        tail_ilu<B, KM, T, M>(L, L.t, L.w, z, tid, nth);
+    }
 }
 
 }  // namespace
@@ -917,9 +1062,11 @@ struct Level {
     int cx = 1, cy = 1, cz = 1;    // cells of this level's grid
     bool coarsest = false;
     std::vector<int> stage_ptr;    // stages (colours or wavefronts) of block rows, permuted order
+    Buf stage_dev;                 // the same on the device (fused coarse cycle)
     Buf perm;                      // permuted unknown position -> natural unknown
     Buf gptr, gidx;                // Galerkin gather from the finer level's values (levels > 0)
-    Buf agg, mptr, midx;           // to the next coarser level (unknown positions)
+    Buf aggb;                      // coarse block row of each block row (next coarser level)
+    Buf mptr, midx;                // aggregate members (unknown positions) of each coarse unknown
     int64_t sell_size = 0;         // slots of the block sliced ELL layout
     int64_t vals = 0;              // sell_size * bs^2
     int64_t blocks = 0;            // block entries of the pattern (without padding)
@@ -943,7 +1090,11 @@ struct SolverAnalysis {
     std::vector<Level> levels;
     Buf vmap;        // level-0 value <- Jacobian entry (-1: zero)
     Buf vec64, vec32, scal, partials, counter, factor_status;
-    Buf pc32;        // FP32 input and output of an FP32 preconditioner
+    // coarse levels fused into one kernel: levels[tail_first..] (-1: none),
+    // their longest block row, cluster size per precision (pc_mode)
+    int tail_first = -1;
+    int tail_kmax = 0;
+    int tail_cluster[3] = {0, 0, 0};
     // CUDA graphs of `chunk` BiCGStab iterations: [0] FP64, [1] FP32, [2] FP64
     // with an FP32 preconditioner
     struct IterGraph {
@@ -1123,6 +1274,7 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std:
     L.sell_size = size;
     L.vals = size * bb;
     L.blocks = pptr[nb];
+    L.stage_dev = upload_ints(c, L.stage_ptr);
     L.sell_ptr = upload_ints(c, sp);
     L.sell_col = upload_ints(c, scol);
     L.sell_len = upload_ints(c, len);
@@ -1155,13 +1307,14 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     // unknowns stacked as ncomp collections over all cells
     const int ncomp = (c.nc > 0 && n % c.nc == 0) ? n / c.nc : 0;
     const bool mg_wanted = pre == "multigrid" && ncomp >= 1 && ncomp <= 8 && n > kCoarsest;
-    // Block ILU(0) with FP32 factors (explicit FP32 inverses of the diagonal
-    // blocks) converges much more slowly than scalar ILU(0) in FP32 on the
-    // two-phase systems, alone and as the V-cycle smoother, so the FP32
-    // preconditioners keep 1 x 1 blocks.
-    const bool fp64_pc = c.param_s("linsolver_precision", "double") == "double";
+    // Block ILU(0) sweeps with FP32 vectors (precision "refine") converge much
+    // more slowly than scalar ones on the two-phase systems; with FP64
+    // vectors, FP32 matrix values ("mixed") do not change the iteration
+    // count.  So "refine" keeps 1 x 1 blocks.
+    const bool fp64_vectors = c.param_s("linsolver_precision", "double") != "refine";
     const int bs =
-        (!natural && fp64_pc && (ncomp == 2 || ncomp == 3) && c.param_i("linsolver_block", 1) != 0) ? ncomp : 1;
+        (!natural && fp64_vectors && (ncomp == 2 || ncomp == 3) && c.param_i("linsolver_block", 1) != 0) ? ncomp
+                                                                                                          : 1;
 
     std::vector<int> perm, iperm, vpos;
     an->levels.emplace_back();
@@ -1237,7 +1390,16 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
                 std::vector<int> pos(mptr.begin(), mptr.end() - 1);
                 for (int pf = 0; pf < fine.n; ++pf) midx[pos[aggp[pf]]++] = pf;
             }
-            Lf.agg = upload_ints(c, aggp);
+            {
+                // per block row: unknown R*bs + c aggregates onto coarse R'*bs + c
+                std::vector<int> aggb(Lf.nb);
+                for (int R = 0; R < Lf.nb; ++R) {
+                    aggb[R] = aggp[R * bs] / bs;
+                    for (int cc = 0; cc < bs; ++cc)
+                        if (aggp[R * bs + cc] != aggb[R] * bs + cc) fail(EQG_ERR_DEVICE, "aggregation splits a block");
+                }
+                Lf.aggb = upload_ints(c, aggb);
+            }
             Lf.mptr = upload_ints(c, mptr);
             Lf.midx = upload_ints(c, midx);
             // Galerkin gather: coarse value <- fine values, in ascending fine entry order
@@ -1278,6 +1440,19 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             fperm = std::move(cperm);
             fvpos = std::move(cvpos);
         }
+    }
+    if (an->multigrid) {
+        // fuse the levels of at most linsolver_mg_fuse_rows unknowns (0: none)
+        const int fuse_rows = c.param_i("linsolver_mg_fuse_rows", 40000);
+        const int nl = (int)an->levels.size();
+        for (int l = 0; l < nl; ++l)
+            if (an->levels[l].n <= fuse_rows && nl - l <= kMaxTail) {
+                an->tail_first = l;
+                break;
+            }
+        if (an->tail_first >= 0)
+            for (int l = an->tail_first; l < nl; ++l)
+                if (!an->levels[l].coarsest) an->tail_kmax = std::max(an->tail_kmax, an->levels[l].kmax);
     }
     an->vec64 = c.allocN<double>((size_t)10 * (n > 0 ? n : 1));
     an->scal = c.alloc(sizeof(KScal));
@@ -1343,14 +1518,107 @@ const double* level_inv<double>(const Level& L) { return L.inv64->as<double>(); 
 template <>
 const float* level_inv<float>(const Level& L) { return L.inv32->as<float>(); }
 
+// Precision of a preconditioner application: vectors T, matrix values M.
+// [0] FP64, [1] FP32 (inner solve of "refine"), [2] FP64 vectors with FP32
+// matrices ("mixed").
+template <class T, class M>
+constexpr int pc_mode()
+{
+    return sizeof(T) == sizeof(float) ? 1 : (sizeof(M) == sizeof(float) ? 2 : 0);
+}
+
+// Cluster size for mg_tail_kernel<B, KM, T, M>: linsolver_mg_cluster
+// (default 16, at most 16), reduced until the device reports that it can
+// schedule one cluster of that size.
+template <int B, int KM, class T, class M>
+int tail_cluster_size(Core& c)
+{
+    int want = std::min(16, std::max(1, c.param_i("linsolver_mg_cluster", 16)));
+    auto kern = mg_tail_kernel<B, KM, T, M>;
+    if (want > 8) EQG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    for (; want > 1; want /= 2) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        cfg.gridDim = dim3(want);
+        cfg.blockDim = dim3(kTailThreads);
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = want;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) == cudaSuccess && clusters > 0) break;
+        (void)cudaGetLastError();
+    }
+    return want;
+}
+
+// Chooses the cluster size of the fused coarse cycle for one precision;
+// called before any stream capture.
+template <class T, class M>
+void prepare_tail(Core& c, SolverAnalysis& an)
+{
+    if (an.tail_first < 0) return;
+    int& cl = an.tail_cluster[pc_mode<T, M>()];
+    const int bs = an.levels[an.tail_first].bs;
+    if (!cl) WITH_BS(bs, WITH_KMAX(an.tail_kmax, cl = tail_cluster_size<BS, KK, T, M>(c)));
+}
+
+// z = V-cycle(r) from level tail_first down, as one mg_tail_kernel launch.
+template <class T, class M>
+void launch_tail(Core& c, const SolverAnalysis& an, const T* r, T* z, const KScal* sc, int skip_if_s)
+{
+    TailParams<T, M> p;
+    for (size_t l = an.tail_first; l < an.levels.size(); ++l) {
+        const Level& L = an.levels[l];
+        TailLevel<T, M>& t = p.lv[p.nlev++];
+        t.nb = L.nb;
+        t.n = L.n;
+        t.coarsest = L.coarsest ? 1 : 0;
+        t.m = L.view();
+        t.a = level_a<M>(L);
+        t.stage_ptr = L.stage_dev->as<int>();
+        t.nstages = (int)L.stage_ptr.size() - 1;
+        if (L.coarsest) {
+            t.inv = level_inv<M>(L);
+        } else {
+            t.lu = level_lu<M>(L);
+            t.aggb = L.aggb->as<int>();
+            t.mptr = L.mptr->as<int>();
+            t.midx = L.midx->as<int>();
+        }
+        t.r = level_vec<T>(L, 0);
+        t.z = level_vec<T>(L, 1);
+        t.t = level_vec<T>(L, 2);
+        t.w = level_vec<T>(L, 3);
+    }
+    const int cl = an.tail_cluster[pc_mode<T, M>()];
+    if (cl <= 0) fail(EQG_ERR_DEVICE, "fused coarse cycle launched before its cluster size was chosen");
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(cl);
+    cfg.blockDim = dim3(kTailThreads);
+    cfg.stream = c.stream;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    WITH_BS(an.levels[an.tail_first].bs, WITH_KMAX(an.tail_kmax, launch(c, "mg_tail", [&] {
+                EQG_CUDA(cudaLaunchKernelEx(&cfg, mg_tail_kernel<BS, KK, T, M>, p, r, z, sc, skip_if_s));
+            })));
+}
+
 // out = M^{-1} b for the block ILU(0) factors of one level; with zadd,
 // zadd += out as rows finish.  One kernel per stage: forward sweeps of
 // stages 1 .. S-1 (the last one finishing its rows), then backward sweeps
 // of stages S-2 .. 0.
-template <class T>
+template <class T, class M>
 void ilu_apply(Core& c, const Level& L, const T* b, T* out, T* zadd, const KScal* sc, int skip_if_s)
 {
-    const T* lu = level_lu<T>(L);
+    const M* lu = level_lu<M>(L);
     const int ns = (int)L.stage_ptr.size() - 1;
     if (ns <= 0) return;
     const int r_first = L.stage_ptr[1];
@@ -1358,37 +1626,43 @@ void ilu_apply(Core& c, const Level& L, const T* b, T* out, T* zadd, const KScal
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
         const int last = s == ns - 1;
         WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "bilu_lower", [&] {
-                    bilu_lower_kernel<BS, KK, T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
+                    bilu_lower_kernel<BS, KK, T, M><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
                         r0, r1, r_first, last, L.view(), lu, b, out, last ? zadd : nullptr, sc, skip_if_s);
                 })));
     }
     for (int s = ns >= 2 ? ns - 2 : 0; s >= 0; --s) {
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
         WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "bilu_upper", [&] {
-                    bilu_upper_kernel<BS, KK, T><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
+                    bilu_upper_kernel<BS, KK, T, M><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
                         r0, r1, s == 0, L.view(), lu, b, out, zadd, sc, skip_if_s);
                 })));
     }
 }
 
-template <class T>
-void level_residual(Core& c, const Level& L, const T* x, const T* b, T* out, const KScal* sc, int skip_if_s)
+// out = b - A x (block rows below r_zero: 0)
+template <class T, class M>
+void level_residual(Core& c, const Level& L, const T* x, const T* b, T* out, int r_zero, const KScal* sc,
+                    int skip_if_s)
 {
     WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "mg_residual", [&] {
-                mg_residual_kernel<BS, KK, T><<<blocksFor(L.nb), kThreads, 0, c.stream>>>(
-                    L.nb, L.view(), level_a<T>(L), x, b, out, sc, skip_if_s);
+                mg_residual_kernel<BS, KK, T, M><<<blocksFor(L.nb), kThreads, 0, c.stream>>>(
+                    L.nb, r_zero, L.view(), level_a<M>(L), x, b, out, sc, skip_if_s);
             })));
 }
 
 // z = V-cycle(r) on level l.
-template <class T>
+template <class T, class M>
 void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const KScal* sc, int skip)
 {
+    if ((int)l == an.tail_first) {
+        launch_tail<T, M>(c, an, r, z, sc, skip);
+        return;
+    }
     const Level& L = an.levels[l];
-    const int n = L.n;
     if (L.coarsest) {
-        launch(c, "mg_dense_apply",
-               [&] { dense_apply_kernel<T><<<1, kThreads, 0, c.stream>>>(n, level_inv<T>(L), r, z, sc, skip); });
+        launch(c, "mg_dense_apply", [&] {
+            dense_apply_kernel<T, M><<<1, kThreads, 0, c.stream>>>(L.n, level_inv<M>(L), r, z, sc, skip);
+        });
         return;
     }
     const Level& C = an.levels[l + 1];
@@ -1396,50 +1670,45 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     T* w = level_vec<T>(L, 3);
     T* rc = level_vec<T>(C, 0);
     T* zc = level_vec<T>(C, 1);
-    ilu_apply<T>(c, L, r, z, nullptr, sc, skip);
-    level_residual<T>(c, L, z, r, t, sc, skip);
+    // pre-smoothing z = M^{-1} r.  The first stage's block rows have no
+    // lower part and were solved last, against the final z of every other
+    // stage, with their rows of A unchanged by the factorization
+    // (D_R^{-1} = A_RR^{-1}, U_RJ = A_RJ): their residual r - A z is zero.
+    ilu_apply<T, M>(c, L, r, z, nullptr, sc, skip);
+    level_residual<T, M>(c, L, z, r, t, L.stage_ptr.size() > 1 ? L.stage_ptr[1] : 0, sc, skip);
     launch(c, "mg_restrict", [&] {
         mg_restrict_kernel<T><<<blocksFor(C.n), kThreads, 0, c.stream>>>(C.n, L.mptr->as<int>(), L.midx->as<int>(), t,
                                                                           rc, sc, skip);
     });
-    vcycle<T>(c, an, l + 1, rc, zc, sc, skip);
-    launch(c, "mg_prolong", [&] {
-        mg_prolong_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(n, L.agg->as<int>(), zc, z, sc, skip);
-    });
-    level_residual<T>(c, L, z, r, t, sc, skip);
-    ilu_apply<T>(c, L, t, w, z, sc, skip);  // z += M^{-1} t
+    vcycle<T, M>(c, an, l + 1, rc, zc, sc, skip);
+    // coarse correction z += P zc, then post-smoothing z += M^{-1} (r - A z)
+    WITH_BS(L.bs, launch(c, "mg_prolong", [&] {
+                mg_prolong_kernel<BS, T><<<blocksFor(L.nb), kThreads, 0, c.stream>>>(L.nb, L.aggb->as<int>(), zc, z,
+                                                                                     sc, skip);
+            }));
+    level_residual<T, M>(c, L, z, r, t, 0, sc, skip);
+    ilu_apply<T, M>(c, L, t, w, z, sc, skip);
 }
 
-template <class T>
+template <class T, class M>
 void precondition(Core& c, const SolverAnalysis& an, const T* in, T* out, const KScal* sc, int skip_if_s)
 {
-    if (an.multigrid) vcycle<T>(c, an, 0, in, out, sc, skip_if_s);
-    else ilu_apply<T>(c, an.levels[0], in, out, nullptr, sc, skip_if_s);
+    if (an.multigrid) vcycle<T, M>(c, an, 0, in, out, sc, skip_if_s);
+    else ilu_apply<T, M>(c, an.levels[0], in, out, nullptr, sc, skip_if_s);
 }
 
-// out = M^{-1} in with the FP32 copy of the preconditioner, for FP64 vectors.
-void precondition_f32(Core& c, const SolverAnalysis& an, const double* in, double* out, const KScal* sc, int skip_if_s)
-{
-    const int n = an.n;
-    float* in32 = an.pc32->as<float>();
-    float* out32 = in32 + n;
-    launch(c, "pc_to_f32",
-           [&] { pc_to_f32_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(in, in32, n, sc, skip_if_s); });
-    precondition<float>(c, an, in32, out32, sc, skip_if_s);
-    launch(c, "pc_to_f64",
-           [&] { pc_to_f64_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(out32, out, n, sc, skip_if_s); });
-}
-
+// out = M^{-1} in; with pc32 (FP64 vectors only) from the FP32 copies of the
+// preconditioner's matrices.
 template <class T>
 void apply_pc(Core& c, const SolverAnalysis& an, const T* in, T* out, const KScal* sc, int skip_if_s, bool pc32)
 {
     if constexpr (sizeof(T) == sizeof(double)) {
         if (pc32) {
-            precondition_f32(c, an, in, out, sc, skip_if_s);
+            precondition<double, float>(c, an, in, out, sc, skip_if_s);
             return;
         }
     }
-    precondition<T>(c, an, in, out, sc, skip_if_s);
+    precondition<T, T>(c, an, in, out, sc, skip_if_s);
 }
 
 // BiCGStab on the permuted system with values a; v.b holds the right-hand
@@ -1610,10 +1879,13 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
             to_float(c, L.as64, L.as32, L.vals);
             if (L.coarsest) to_float(c, L.inv64, L.inv32, (int64_t)L.n * L.n);
             else to_float(c, L.lus64, L.lus32, L.vals);
-            if (!L.v32) L.v32 = c.allocN<float>((size_t)4 * (L.n > 0 ? L.n : 1));
+            if (refine && !L.v32) L.v32 = c.allocN<float>((size_t)4 * (L.n > 0 ? L.n : 1));
         }
         if (refine && !an.vec32) an.vec32 = c.allocN<float>((size_t)10 * n);
-        if (mixed && !an.pc32) an.pc32 = c.allocN<float>((size_t)2 * n);
+        if (refine) prepare_tail<float, float>(c, an);
+        else prepare_tail<double, float>(c, an);
+    } else {
+        prepare_tail<double, double>(c, an);
     }
     c.factor_clock.stop(c.stream);
     int fstat = 0;

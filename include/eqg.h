@@ -120,7 +120,9 @@ const char* eqg_backend_name(void);
  * BiCGStab inside FP64 refinement), linsolver_inner_tolerance (1e-4) and
  * linsolver_max_sweeps (60) for refine, linsolver_check_every (8),
  * linsolver_block (1: ncomp x ncomp block ILU(0) for 2 or 3 unknowns per
- * cell; 0: scalar ILU(0)), time_kernel
+ * cell; 0: scalar ILU(0)), linsolver_mg_fuse_rows (40000: the V-cycle
+ * levels up to this size run as one kernel; 0: none), linsolver_mg_cluster
+ * (16: thread blocks of that kernel's cluster, at most 16), time_kernel
  * (a kernel name, or "*", to time with CUDA events) and device (CUDA device
  * index; default: the calling thread's current device).  grid_filename is
  * rejected with EQG_ERR_UNSUPPORTED.
@@ -153,6 +155,9 @@ typedef struct eqg_solve_info {
     int converged;              /* residual norm <= abs_res_tol at return   */
     int64_t krylov_iterations;
     int64_t kernel_launches;    /* device kernels launched during the solve */
+    double residual_ms;         /* time in the solve's phases (as in          */
+    double factor_ms;           /* eqg_stats: device clock for the product,  */
+    double krylov_ms;           /* host clock for the oracle)                 */
 } eqg_solve_info;
 int eqg_runtime_solve_info(const eqg_runtime* rt, int64_t k, eqg_solve_info* out);
 

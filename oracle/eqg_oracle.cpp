@@ -1553,6 +1553,7 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
         eqg_runtime_mark(rt, &m0);
         rt->stats.newton_solves++;
         const int64_t krylov0 = rt->stats.krylov_iterations;
+        const double res_ms0 = rt->stats.residual_ms, fac_ms0 = rt->stats.factor_ms, kry_ms0 = rt->stats.krylov_ms;
         eqg_coll* u = nullptr;
         if (eqg_variable(rt, u0, &u) != EQG_OK) fail(EQG_ERR_ARG, g_last_error);
         auto cleanup = [&](eqg_coll* a) { eqg_coll_release(a); };
@@ -1608,6 +1609,9 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
         info.newton_iterations = iter;
         info.converged = norm(res) <= rt->abs_res_tol ? 1 : 0;
         info.krylov_iterations = rt->stats.krylov_iterations - krylov0;
+        info.residual_ms = rt->stats.residual_ms - res_ms0;
+        info.factor_ms = rt->stats.factor_ms - fac_ms0;
+        info.krylov_ms = rt->stats.krylov_ms - kry_ms0;
         *out = make_coll(adb_constant(u->a.v));
         cleanup(u);
         cleanup(res);

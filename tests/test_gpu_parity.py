@@ -166,3 +166,24 @@ def test_two_phase_block_layouts(gpu_lib, oracle_lib, block, ordering):
     oo = programs.two_phase(Runtime(oracle_lib, params), **case)
     for step, ((pg, sg), (po, so)) in enumerate(zip(og, oo)):
         assert np.max(np.abs(sg - so) / np.abs(so)) <= 1e-8, "Sw step %d" % step
+
+
+@pytest.mark.parametrize("precision", ["double", "mixed"])
+@pytest.mark.parametrize("shape", [(16, 16, 8), (64, 64, None)])
+def test_fused_coarse_cycle_identical(gpu_lib, shape, precision):
+    """The V-cycle's coarse levels fused into one cluster kernel compute every
+    element with the same operations as the launch-per-step cycle: pressure
+    and saturation are bit-identical with no levels fused, some fused, all
+    fused, and for cluster sizes 1, 8 and 16."""
+    grid, case = programs.two_phase_case(*shape, steps=2)
+    params = dict(grid, abs_res_tol=1e-10, linsolver_residual_tolerance=1e-10, linsolver_max_iterations=5000,
+                  linsolver_precision=precision)
+    runs = {}
+    for fuse, cluster in [(0, 16), (600, 16), (40000, 1), (40000, 8), (40000, 16)]:
+        eg = Runtime(gpu_lib, dict(params, linsolver_mg_fuse_rows=fuse, linsolver_mg_cluster=cluster))
+        runs[(fuse, cluster)] = (programs.two_phase(eg, **case), eg.stats())
+    base, st0 = runs[(0, 16)]
+    for key, (out, st) in runs.items():
+        assert st["krylov_iterations"] == st0["krylov_iterations"], key
+        for (pa, sa), (pb, sb) in zip(out, base):
+            assert np.array_equal(pa, pb) and np.array_equal(sa, sb), key
