@@ -139,13 +139,13 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NV], double* partials, unsi
 // Level matrices are in a block sliced ELL layout: block rows in slices of
 // 32 (one warp), each slice stored by position k in the row and padded to
 // its longest row.  Slot q = slice_ptr[R / 32] + 32 k + R % 32 holds the
-// block column col[q] of the k-th block of block row R; the B x B values of
-// that block (row-major, e = i B + j) are at
-//     (slice_ptr[R / 32] + 32 k) B^2 + 32 e + R % 32,
-// so that a warp's loads of value e at position k are one contiguous
-// segment.  Within a row, blocks are in ascending column order, so the
-// ILU(0) lower part is k < dk[R] and the upper part k > dk[R].  Vectors are
-// in block-row order: unknown c of block row R is at R B + c.
+// block column col[q] of the k-th block of block row R, and the B x B values
+// of that block (row-major, e = i B + j) are contiguous at q B^2 + e: a 2 x 2
+// block is one 128-bit load in FP32 (two in FP64), and a warp's loads at
+// position k are one contiguous segment.  Within a row, blocks are in
+// ascending column order, so the ILU(0) lower part is k < dk[R] and the
+// upper part k > dk[R].  Vectors are in block-row order: unknown c of block
+// row R is at R B + c.
 struct SellView {
     const int* __restrict__ slice_ptr;  // first slot of each slice
     const int* __restrict__ col;        // block column of each slot
@@ -181,6 +181,29 @@ __device__ __forceinline__ void store_bvec(T* __restrict__ x, int R, const doubl
     for (int c = 0; c < B; ++c) x[R * B + c] = (T)v[c];
 }
 
+// The BB values of one block (contiguous; 16-byte aligned when BB = 4).
+template <int BB, class M>
+__device__ __forceinline__ void load_block(const M* __restrict__ p, M (&v)[BB])
+{
+    if constexpr (BB == 4 && sizeof(M) == 4) {
+        const float4 t = *reinterpret_cast<const float4*>(p);
+        v[0] = t.x;
+        v[1] = t.y;
+        v[2] = t.z;
+        v[3] = t.w;
+    } else if constexpr (BB == 4 && sizeof(M) == 8) {
+        const double2 t0 = reinterpret_cast<const double2*>(p)[0];
+        const double2 t1 = reinterpret_cast<const double2*>(p)[1];
+        v[0] = t0.x;
+        v[1] = t0.y;
+        v[2] = t1.x;
+        v[3] = t1.y;
+    } else {
+#pragma unroll
+        for (int e = 0; e < BB; ++e) v[e] = p[e];
+    }
+}
+
 // acc += sum_{k0 <= k < k1} A_{R,k} x_{col(R,k)}, blocks in ascending k and
 // within a block in ascending j.  x_J is read from `x` when J < split and
 // from `x2` otherwise.  With KM > 0 (rows of at most KM blocks) the loop is
@@ -197,11 +220,12 @@ __device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int
             const int J = m.col[q + lane];
             double xv[B];
             load_bvec<B, T, CG>(J < split ? x : x2, J, xv);
-            const M* av = a + (size_t)q * BB + lane;
+            M av[BB];
+            load_block<BB, M>(a + (size_t)(q + lane) * BB, av);
 #pragma unroll
             for (int i = 0; i < B; ++i)
 #pragma unroll
-                for (int j = 0; j < B; ++j) acc[i] += (double)av[(i * B + j) << 5] * xv[j];
+                for (int j = 0; j < B; ++j) acc[i] += (double)av[i * B + j] * xv[j];
         }
     } else if constexpr (KM * BB <= 32) {
         // columns and values of the whole row first (predicated loads), then
@@ -214,7 +238,8 @@ __device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int
             const int q = sbase + (k << 5);
             ci[k] = on ? m.col[q + lane] : 0;
 #pragma unroll
-            for (int e = 0; e < BB; ++e) av[k][e] = on ? a[(size_t)q * BB + (e << 5) + lane] : (M)0;
+            for (int e = 0; e < BB; ++e) av[k][e] = (M)0;
+            if (on) load_block<BB, M>(a + (size_t)(q + lane) * BB, av[k]);
         }
 #pragma unroll
         for (int k = 0; k < KM; ++k) {
@@ -237,11 +262,12 @@ __device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int
                 const int q = sbase + (k << 5);
                 double xv[B];
                 load_bvec<B, T, CG>(ci[k] < split ? x : x2, ci[k], xv);
-                const M* av = a + (size_t)q * BB + lane;
+                M av[BB];
+                load_block<BB, M>(a + (size_t)(q + lane) * BB, av);
 #pragma unroll
                 for (int i = 0; i < B; ++i)
 #pragma unroll
-                    for (int j = 0; j < B; ++j) acc[i] += (double)av[(i * B + j) << 5] * xv[j];
+                    for (int j = 0; j < B; ++j) acc[i] += (double)av[i * B + j] * xv[j];
             }
         }
     }
@@ -252,12 +278,13 @@ __device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int
 template <int B, class M>
 __device__ __forceinline__ void bmatvec(const M* __restrict__ a, int q, int lane, const double (&x)[B], double (&y)[B])
 {
-    const M* av = a + (size_t)q * (B * B) + lane;
+    M av[B * B];
+    load_block<B * B, M>(a + (size_t)(q + lane) * (B * B), av);
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         double s = 0.0;
 #pragma unroll
-        for (int j = 0; j < B; ++j) s += (double)av[(i * B + j) << 5] * x[j];
+        for (int j = 0; j < B; ++j) s += (double)av[i * B + j] * x[j];
         y[i] = s;
     }
 }
@@ -387,7 +414,7 @@ __global__ void bilu_factor_stage_kernel(int r0, int r1, SellView m, double* lu,
         const int R = (int)rr;
         const int lane = R & 31, sb = m.slice_ptr[R >> 5], len = m.len[R], d = m.dk[R];
         auto at = [&](int sbase, int ln, int k, int e) -> double& {
-            return lu[(size_t)(sbase + (k << 5)) * BB + (e << 5) + ln];
+            return lu[(size_t)(sbase + (k << 5) + ln) * BB + e];
         };
         for (int k = 0; k < d; ++k) {
             const int K = m.col[sb + (k << 5) + lane];
@@ -890,7 +917,7 @@ __global__ void dense_inverse_kernel(int nb, SellView m, const double* __restric
             const int J = m.col[sb + (k << 5) + lane];
             for (int i = 0; i < B; ++i)
                 for (int j = 0; j < B; ++j)
-                    work[(R * B + i) * w2 + J * B + j] = a[(size_t)(sb + (k << 5)) * BB + ((i * B + j) << 5) + lane];
+                    work[(R * B + i) * w2 + J * B + j] = a[(size_t)(sb + (k << 5) + lane) * BB + i * B + j];
         }
         for (int i = 0; i < B; ++i) work[(R * B + i) * w2 + n + R * B + i] = 1.0;
     }
@@ -954,7 +981,15 @@ __global__ void dense_apply_kernel(int n, const M* __restrict__ inv, const T* __
 // barrier: loop bounds are kernel parameters or device arrays that do not
 // change while it runs, and so is the early-exit flag (a converged solve).
 constexpr int kTailThreads = 512;
-constexpr int kMaxTail = 12;
+constexpr int kMaxTail = 8;
+constexpr int kMaxPrefetch = 64;
+
+// A device array the fused cycle prefetches into L2 when it starts (the
+// fine level's sweeps between two visits evict the coarse levels' data).
+struct PrefetchRegion {
+    const void* ptr;  // 16-byte aligned
+    unsigned long long bytes;
+};
 
 template <class T, class M>
 struct TailLevel {
@@ -975,7 +1010,25 @@ template <class T, class M>
 struct TailParams {
     TailLevel<T, M> lv[kMaxTail];
     int nlev = 0;
+    int nregions = 0;
+    PrefetchRegion reg[kMaxPrefetch];
 };
+
+// Thread blocks split every region into 16-byte aligned chunks and hand them
+// to the TMA unit as bulk L2 prefetches.
+__device__ __forceinline__ void prefetch_regions(const PrefetchRegion* reg, int nregions)
+{
+    if ((int)threadIdx.x >= nregions) return;
+    const PrefetchRegion& g = reg[threadIdx.x];
+    const unsigned long long chunk = ((g.bytes / gridDim.x) + 15ull) & ~15ull;
+    const unsigned long long off = chunk * blockIdx.x;
+    if (off >= g.bytes) return;
+    unsigned long long len = g.bytes - off < chunk ? g.bytes - off : chunk;
+    len &= ~15ull;
+    if (len == 0) return;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((const char*)g.ptr + off), "r"((unsigned)len)
+                 : "memory");
+}
 
 __device__ __forceinline__ void cluster_barrier()
 {
@@ -1007,6 +1060,7 @@ __global__ void __launch_bounds__(kTailThreads)
     mg_tail_kernel(const __grid_constant__ TailParams<T, M> p, const T* r_top, T* z_top, const KScal* sc, int skip_if_s)
 {
     if (mg_skip(sc, skip_if_s)) return;
+    prefetch_regions(p.reg, p.nregions);
     THREAD_RANGE;
     int l = 0;
     for (;; ++l) {
@@ -1264,7 +1318,7 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std:
             const int* hi = pcol.data() + pptr[R + 1];
             const int k = (int)(std::lower_bound(lo, hi, J) - lo);
             const int64_t slot0 = sp[R / 32] + 32 * k;
-            vpos[e] = (int)(slot0 * bb + 32 * (cu * bs + cv) + (R % 32));
+            vpos[e] = (int)((slot0 + R % 32) * bb + cu * bs + cv);
         }
     }
     L.n = n;
@@ -1570,8 +1624,23 @@ template <class T, class M>
 void launch_tail(Core& c, const SolverAnalysis& an, const T* r, T* z, const KScal* sc, int skip_if_s)
 {
     TailParams<T, M> p;
+    auto region = [&](const void* ptr, int64_t bytes) {
+        if (p.nregions < kMaxPrefetch && bytes >= 16) p.reg[p.nregions++] = PrefetchRegion{ptr, (unsigned long long)bytes};
+    };
     for (size_t l = an.tail_first; l < an.levels.size(); ++l) {
         const Level& L = an.levels[l];
+        region(L.sell_ptr->ptr, ((L.nb + 31) / 32 + 1) * 4);
+        region(L.sell_col->ptr, L.sell_size * 4);
+        region(L.sell_len->ptr, (int64_t)L.nb * 4);
+        region(L.sell_dk->ptr, (int64_t)L.nb * 4);
+        region(level_a<M>(L), L.vals * (int64_t)sizeof(M));
+        if (L.coarsest) {
+            region(level_inv<M>(L), (int64_t)L.n * L.n * (int64_t)sizeof(M));
+        } else {
+            region(level_lu<M>(L), L.vals * (int64_t)sizeof(M));
+            region(L.aggb->ptr, (int64_t)L.nb * 4);
+            region(L.midx->ptr, (int64_t)L.n * 4);
+        }
         TailLevel<T, M>& t = p.lv[p.nlev++];
         t.nb = L.nb;
         t.n = L.n;
