@@ -680,9 +680,19 @@ __global__ void bicg_p_kernel(const T* __restrict__ r, const T* __restrict__ v, 
     GRID_STRIDE(i, n) p[i] = (T)((double)r[i] + beta * ((double)p[i] - omega * (double)v[i]));
 }
 
+// The SpMV kernels are latency bound; for the FP64 layouts with blocks of
+// at most 2 x 2 and rows of at most 8 blocks their launch bounds trade the
+// reduction's registers for resident warps (8 and 6 blocks of 256 per SM,
+// without spills); the other instantiations keep the compiler's choice.
+template <int B, int KM, class T>
+constexpr int spmv_min_blocks(int hot)
+{
+    return (B <= 2 && KM == 8 && sizeof(T) == sizeof(double)) ? hot : 1;
+}
+
 // v = A ph ; alpha = rho_new / (rhat . v)
 template <int B, int KM, class T>
-__global__ void bicg_spmv_alpha_kernel(SellView m, const T* __restrict__ a, const T* __restrict__ ph,
+__global__ void __launch_bounds__(kThreads, spmv_min_blocks<B, KM, T>(8)) bicg_spmv_alpha_kernel(SellView m, const T* __restrict__ a, const T* __restrict__ ph,
                                        const T* __restrict__ rhat, T* __restrict__ v, int nb, double* partials,
                                        unsigned int* counter, KScal* sc)
 {
@@ -735,7 +745,7 @@ __global__ void bicg_s_kernel(const T* __restrict__ r, const T* __restrict__ v, 
 
 // t = A sh ; omega = (t . s) / (t . t)
 template <int B, int KM, class T>
-__global__ void bicg_spmv_omega_kernel(SellView m, const T* __restrict__ a, const T* __restrict__ sh,
+__global__ void __launch_bounds__(kThreads, spmv_min_blocks<B, KM, T>(6)) bicg_spmv_omega_kernel(SellView m, const T* __restrict__ a, const T* __restrict__ sh,
                                        const T* __restrict__ s, T* __restrict__ t, int nb, double* partials,
                                        unsigned int* counter, KScal* sc)
 {
