@@ -30,6 +30,7 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
     "-Xcompiler", "-fPIC",
+    "-Xcompiler", "-fopenmp",  # host loops of the solver analysis
     "-Xptxas", "-v" if os.environ.get("EQG_PTXAS_VERBOSE") else "-O3",
     "-I" + INCLUDE_DIR, "-I" + CSRC,
     "-ccbin", CXX,
@@ -72,7 +73,7 @@ def build_library(force=False, verbose=False):
         # C ABI (the CPU oracle) is loaded into the process.
         # cudart is linked statically: the library does not depend on which
         # libcudart.so another component of the process loaded first.
-        _run([NVCC, "-shared", "-cudart", "static", "-Xlinker", "-Bsymbolic", "-o", LIB_PATH] + objs)
+        _run([NVCC, "-shared", "-cudart", "static", "-Xlinker", "-Bsymbolic", "-o", LIB_PATH] + objs + ["-lgomp"])
     return LIB_PATH
 
 

@@ -46,6 +46,7 @@
 #include "eqg_internal.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -862,18 +863,21 @@ __global__ void sumsq_kernel(const double* __restrict__ a, int n, double* partia
 }
 
 // ---- multilevel preconditioner kernels -------------------------------------
-// Coarse-level values: each coarse value is the sum of the finer level's
-// values that aggregate onto it (Galerkin product R A R^T with a 0/1
-// aggregation R), gathered in a fixed order; an empty list gives 0.
-__global__ void galerkin_kernel(int64_t size_c, const int* __restrict__ gptr, const int* __restrict__ gidx,
-                                const double* __restrict__ fine, double* __restrict__ coarse)
+// Coarse-level values: each entry of the coarse pattern is the sum of the
+// finer level's values that aggregate onto it (Galerkin product R A R^T with
+// a 0/1 aggregation R), gathered in ascending fine-entry order, and stored
+// at its value position gpos[c] (the other positions, padding and entries a
+// block does not have, are zeroed beforehand).
+__global__ void galerkin_kernel(int64_t nnz_c, const int* __restrict__ gptr, const int* __restrict__ gidx,
+                                const int* __restrict__ gpos, const double* __restrict__ fine,
+                                double* __restrict__ coarse)
 {
-    GRID_STRIDE(c, size_c)
+    GRID_STRIDE(c, nnz_c)
     {
         double s = 0.0;
         const int k1 = gptr[c + 1];
         for (int k = gptr[c]; k < k1; ++k) s += fine[gidx[k]];
-        coarse[c] = s;
+        coarse[gpos[c]] = s;
     }
 }
 
@@ -1128,7 +1132,7 @@ struct Level {
     std::vector<int> stage_ptr;    // stages (colours or wavefronts) of block rows, permuted order
     Buf stage_dev;                 // the same on the device (fused coarse cycle)
     Buf perm;                      // permuted unknown position -> natural unknown
-    Buf gptr, gidx;                // Galerkin gather from the finer level's values (levels > 0)
+    Buf gptr, gidx, gpos;          // Galerkin gather from the finer level's values (levels > 0)
     Buf aggb;                      // coarse block row of each block row (next coarser level)
     Buf mptr, midx;                // aggregate members (unknown positions) of each coarse unknown
     int64_t sell_size = 0;         // slots of the block sliced ELL layout
@@ -1226,12 +1230,62 @@ Buf upload_ints(Core& c, const std::vector<int>& v)
     return b;
 }
 
-// Lays out the matrix with pattern `A` (natural unknown numbering) in blocks
-// of `bs` unknowns: block row of unknown u is u % nb and its component u / nb
-// (nb = n / bs).  Orders the block rows by stage and builds the block sliced
-// ELL pattern (each row with its diagonal block).  Returns the unknown
-// permutation (position -> natural unknown), its inverse, and for every
-// entry of `A` its position in the level's value array.
+// Sorts a short list and drops repeats; returns the new length.
+inline int sort_unique(int* v, int len)
+{
+    std::sort(v, v + len);
+    return (int)(std::unique(v, v + len) - v);
+}
+
+// Position of `key` in the sorted short list v[0..len) (len if absent).
+inline int find_small(const int* v, int len, int key)
+{
+    int k = 0;
+    while (k < len && v[k] < key) ++k;
+    return (k < len && v[k] == key) ? k : len;
+}
+
+// Builds the CSR pattern whose row r is the sorted, repeat-free union of
+// the columns that gather(r, buf) writes into buf (at most `cap` of them).
+// Two passes over the rows, each parallel over rows.
+template <class Gather>
+void build_rows(int nrows, int cap, HostCsr& out, Gather gather)
+{
+    out.n = nrows;
+    out.ptr.assign(nrows + 1, 0);
+#pragma omp parallel
+    {
+        std::vector<int> buf(cap > 0 ? cap : 1);
+#pragma omp for schedule(static)
+        for (int r = 0; r < nrows; ++r) out.ptr[r + 1] = sort_unique(buf.data(), gather(r, buf.data()));
+    }
+    for (int r = 0; r < nrows; ++r) out.ptr[r + 1] += out.ptr[r];
+    out.col.resize(out.ptr[nrows] > 0 ? out.ptr[nrows] : 1);
+#pragma omp parallel
+    {
+        std::vector<int> buf(cap > 0 ? cap : 1);
+#pragma omp for schedule(static)
+        for (int r = 0; r < nrows; ++r) {
+            const int len = sort_unique(buf.data(), gather(r, buf.data()));
+            std::copy(buf.data(), buf.data() + len, out.col.begin() + out.ptr[r]);
+        }
+    }
+}
+
+inline int max_row(const HostCsr& A)
+{
+    int m = 0;
+    for (int r = 0; r < A.n; ++r) m = std::max(m, A.ptr[r + 1] - A.ptr[r]);
+    return m;
+}
+
+// Lays out the matrix with pattern `A` (natural unknown numbering, rows with
+// ascending columns) in blocks of `bs` unknowns: block row of unknown u is
+// u % nb and its component u / nb (nb = n / bs).  Orders the block rows by
+// stage and builds the block sliced ELL pattern (each row with its diagonal
+// block).  Returns the unknown permutation (position -> natural unknown),
+// its inverse, and for every entry of `A` its position in the level's value
+// array.
 void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std::vector<int>& perm,
                  std::vector<int>& iperm, std::vector<int>& vpos, bool& ok)
 {
@@ -1241,28 +1295,25 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std:
     const int64_t nnz = A.ptr[n];
     // block graph (natural block numbering), sorted, with the diagonal
     HostCsr G;
-    G.n = nb;
-    G.ptr.assign(nb + 1, 0);
-    {
-        std::vector<std::vector<int>> rows(nb);
-        for (int u = 0; u < n; ++u)
-            for (int e = A.ptr[u]; e < A.ptr[u + 1]; ++e) rows[u % nb].push_back(A.col[e] % nb);
-        for (int R = 0; R < nb; ++R) {
-            auto& r = rows[R];
-            r.push_back(R);
-            std::sort(r.begin(), r.end());
-            r.erase(std::unique(r.begin(), r.end()), r.end());
-            G.ptr[R + 1] = G.ptr[R] + (int)r.size();
+    build_rows(nb, bs * max_row(A) + 1, G, [&](int R, int* buf) {
+        int len = 0;
+        for (int cc = 0; cc < bs; ++cc) {
+            const int u = cc * nb + R;
+            for (int e = A.ptr[u]; e < A.ptr[u + 1]; ++e) buf[len++] = A.col[e] % nb;
         }
-        G.col.resize(G.ptr[nb] > 0 ? G.ptr[nb] : 1);
-        for (int R = 0; R < nb; ++R) std::copy(rows[R].begin(), rows[R].end(), G.col.begin() + G.ptr[R]);
-    }
-    if (bs == 1)
+        buf[len++] = R;
+        return len;
+    });
+    if (bs == 1) {
+        bool all = true;
+#pragma omp parallel for reduction(&& : all) schedule(static)
         for (int u = 0; u < n; ++u) {
             bool has = false;
             for (int e = A.ptr[u]; e < A.ptr[u + 1]; ++e) has = has || A.col[e] == u;
-            if (!has) ok = false;
+            all = all && has;
         }
+        if (!all) ok = false;
+    }
     const std::vector<int> key = stage_keys(G, natural);
     const int nst = nb > 0 ? *std::max_element(key.begin(), key.end()) + 1 : 0;
     L.stage_ptr.assign(nst + 1, 0);
@@ -1276,6 +1327,7 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std:
     for (int R = 0; R < nb; ++R) ipb[pb[R]] = R;
     perm.assign(n, 0);
     iperm.assign(n, 0);
+#pragma omp parallel for schedule(static)
     for (int R = 0; R < nb; ++R)
         for (int cc = 0; cc < bs; ++cc) {
             perm[R * bs + cc] = cc * nb + pb[R];
@@ -1283,9 +1335,10 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std:
         }
     // permuted block rows: sorted permuted columns
     std::vector<int> pptr(nb + 1, 0), pcol(G.ptr[nb] > 0 ? G.ptr[nb] : 1);
+    for (int R = 0; R < nb; ++R) pptr[R + 1] = pptr[R] + (G.ptr[pb[R] + 1] - G.ptr[pb[R]]);
+#pragma omp parallel for schedule(static)
     for (int R = 0; R < nb; ++R) {
         const int o = pb[R];
-        pptr[R + 1] = pptr[R] + (G.ptr[o + 1] - G.ptr[o]);
         int w = pptr[R];
         for (int e = G.ptr[o]; e < G.ptr[o + 1]; ++e) pcol[w++] = ipb[G.col[e]];
         std::sort(pcol.begin() + pptr[R], pcol.begin() + pptr[R + 1]);
@@ -1301,11 +1354,12 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std:
     const int64_t size = sp[nsl];
     if (size * bb >= (int64_t)INT_MAX) fail(EQG_ERR_UNSUPPORTED, "linear system too large for 32-bit value offsets");
     std::vector<int> scol(size > 0 ? size : 1, 0);
-    L.kmax = 0;
+    int kmax = 0;
+#pragma omp parallel for reduction(max : kmax) schedule(static)
     for (int R = 0; R < nb; ++R) {
         const int base = sp[R / 32] + (R % 32);
         len[R] = pptr[R + 1] - pptr[R];
-        L.kmax = std::max(L.kmax, len[R]);
+        kmax = std::max(kmax, len[R]);
         const int w = (sp[R / 32 + 1] - sp[R / 32]) / 32;
         dk[R] = -1;
         for (int k = 0; k < w; ++k) {
@@ -1317,18 +1371,22 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std:
             }
         }
     }
-    // value position of every scalar entry of A
+    L.kmax = kmax;
+    // value position of every scalar entry of A, block row by block row
     vpos.assign(nnz > 0 ? nnz : 1, -1);
-    for (int u = 0; u < n; ++u) {
-        const int R = ipb[u % nb], cu = u / nb;
-        for (int e = A.ptr[u]; e < A.ptr[u + 1]; ++e) {
-            const int v = A.col[e];
-            const int J = ipb[v % nb], cv = v / nb;
-            const int* lo = pcol.data() + pptr[R];
-            const int* hi = pcol.data() + pptr[R + 1];
-            const int k = (int)(std::lower_bound(lo, hi, J) - lo);
-            const int64_t slot0 = sp[R / 32] + 32 * k;
-            vpos[e] = (int)((slot0 + R % 32) * bb + cu * bs + cv);
+#pragma omp parallel for schedule(static)
+    for (int Rn = 0; Rn < nb; ++Rn) {
+        const int R = ipb[Rn];
+        const int* row = pcol.data() + pptr[R];
+        const int rl = pptr[R + 1] - pptr[R];
+        for (int cu = 0; cu < bs; ++cu) {
+            const int u = cu * nb + Rn;
+            for (int e = A.ptr[u]; e < A.ptr[u + 1]; ++e) {
+                const int v = A.col[e];
+                const int k = find_small(row, rl, ipb[v % nb]);
+                const int64_t slot0 = sp[R / 32] + 32 * k;
+                vpos[e] = (int)((slot0 + R % 32) * bb + cu * bs + v / nb);
+            }
         }
     }
     L.n = n;
@@ -1352,6 +1410,10 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std:
 
 std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
 {
+    const auto t_start = std::chrono::steady_clock::now();
+    auto since = [&] {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    };
     auto an = std::make_shared<SolverAnalysis>();
     const int n = p.rows;
     an->n = n;
@@ -1382,9 +1444,12 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
 
     std::vector<int> perm, iperm, vpos;
     an->levels.emplace_back();
+    const double t_copy = since();
     order_level(c, A, natural, bs, an->levels[0], perm, iperm, vpos, an->ok);
+    const double t_level0 = since();
     {
         std::vector<int> vmap(an->levels[0].vals > 0 ? an->levels[0].vals : 1, -1);
+#pragma omp parallel for schedule(static)
         for (int64_t e = 0; e < p.nnz; ++e) vmap[vpos[e]] = (int)e;
         an->vmap = upload_ints(c, vmap);
     }
@@ -1393,10 +1458,17 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     an->levels[0].cy = c.ny;
     an->levels[0].cz = c.nz;
     if (an->multigrid) {
-        // the finer level in its natural ordering, with its permutation and value positions
-        HostCsr fine = A;
-        std::vector<int> fperm = perm, fvpos = vpos;
+        // the finer level in its natural ordering, with its permutation and
+        // value positions (level 0: the Jacobian pattern itself)
+        const HostCsr* finep = &A;
+        const std::vector<int>* fpermp = &perm;
+        const std::vector<int>* fvposp = &vpos;
+        HostCsr owned;
+        std::vector<int> owned_perm, owned_vpos;
         for (;;) {
+            const HostCsr& fine = *finep;
+            const std::vector<int>& fperm = *fpermp;
+            const std::vector<int>& fvpos = *fvposp;
             Level& F = an->levels.back();
             const int fcx = F.cx, fcy = F.cy, fcz = F.cz;
             const int fcells = fcx * fcy * fcz;
@@ -1405,35 +1477,32 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             const int nc_unk = ncomp * ccells;
             // aggregate of every fine unknown (natural indices)
             std::vector<int> agg_nat(fine.n);
+#pragma omp parallel for schedule(static)
             for (int u = 0; u < fine.n; ++u) {
                 const int comp = u / fcells, cell = u - comp * fcells;
                 const int i = cell % fcx, j = (cell / fcx) % fcy, k = cell / (fcx * fcy);
                 agg_nat[u] = comp * ccells + (i / 2) + ccx * ((j / 2) + ccy * (fcz > 1 ? k / 2 : 0));
             }
+            // members of every coarse unknown (natural indices, ascending)
+            std::vector<int> nmptr(nc_unk + 1, 0), nmidx(fine.n);
+            for (int u = 0; u < fine.n; ++u) nmptr[agg_nat[u] + 1]++;
+            for (int U = 0; U < nc_unk; ++U) nmptr[U + 1] += nmptr[U];
+            {
+                std::vector<int> pos(nmptr.begin(), nmptr.end() - 1);
+                for (int u = 0; u < fine.n; ++u) nmidx[pos[agg_nat[u]]++] = u;
+            }
+            int max_members = 0;
+            for (int U = 0; U < nc_unk; ++U) max_members = std::max(max_members, nmptr[U + 1] - nmptr[U]);
             // coarse pattern (natural ordering, sorted rows)
             HostCsr C;
-            C.n = nc_unk;
-            {
-                std::vector<std::vector<int>> rows(nc_unk);
-                std::vector<int> mark(nc_unk, -1);
-                std::vector<std::vector<int>> members(nc_unk);
-                for (int u = 0; u < fine.n; ++u) members[agg_nat[u]].push_back(u);
-                C.ptr.assign(nc_unk + 1, 0);
-                for (int U = 0; U < nc_unk; ++U) {
-                    for (int u : members[U])
-                        for (int e = fine.ptr[u]; e < fine.ptr[u + 1]; ++e) {
-                            const int V = agg_nat[fine.col[e]];
-                            if (mark[V] != U) {
-                                mark[V] = U;
-                                rows[U].push_back(V);
-                            }
-                        }
-                    std::sort(rows[U].begin(), rows[U].end());
-                    C.ptr[U + 1] = C.ptr[U] + (int)rows[U].size();
+            build_rows(nc_unk, max_members * max_row(fine) + 1, C, [&](int U, int* buf) {
+                int len = 0;
+                for (int m = nmptr[U]; m < nmptr[U + 1]; ++m) {
+                    const int u = nmidx[m];
+                    for (int e = fine.ptr[u]; e < fine.ptr[u + 1]; ++e) buf[len++] = agg_nat[fine.col[e]];
                 }
-                C.col.resize(C.ptr[nc_unk] > 0 ? C.ptr[nc_unk] : 1);
-                for (int U = 0; U < nc_unk; ++U) std::copy(rows[U].begin(), rows[U].end(), C.col.begin() + C.ptr[U]);
-            }
+                return len;
+            });
             an->levels.emplace_back();
             Level& Lc = an->levels.back();
             Level& Lf = an->levels[an->levels.size() - 2];
@@ -1466,29 +1535,43 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             }
             Lf.mptr = upload_ints(c, mptr);
             Lf.midx = upload_ints(c, midx);
-            // Galerkin gather: coarse value <- fine values, in ascending fine entry order
+            // Galerkin gather: for every coarse entry, the value positions of
+            // the fine entries that aggregate onto it, in ascending fine-entry
+            // order.  A coarse row's entries come only from its members' rows,
+            // so both passes run per coarse row.
             const int64_t fnnz = fine.ptr[fine.n];
-            const int64_t cvals = Lc.vals;
-            std::vector<int> target(fnnz > 0 ? fnnz : 1);
-            for (int u = 0; u < fine.n; ++u) {
-                const int U = agg_nat[u];
-                for (int e = fine.ptr[u]; e < fine.ptr[u + 1]; ++e) {
-                    const int V = agg_nat[fine.col[e]];
-                    const int* lo = C.col.data() + C.ptr[U];
-                    const int* hi = C.col.data() + C.ptr[U + 1];
-                    const int* q = std::lower_bound(lo, hi, V);
-                    target[e] = cvpos[q - C.col.data()];
+            const int cnnz = C.ptr[nc_unk];
+            std::vector<int> gptr(cnnz + 1, 0), gidx(fnnz > 0 ? fnnz : 1);
+#pragma omp parallel for schedule(static)
+            for (int U = 0; U < nc_unk; ++U) {
+                const int* row = C.col.data() + C.ptr[U];
+                const int rl = C.ptr[U + 1] - C.ptr[U];
+                for (int m = nmptr[U]; m < nmptr[U + 1]; ++m) {
+                    const int u = nmidx[m];
+                    for (int e = fine.ptr[u]; e < fine.ptr[u + 1]; ++e)
+                        gptr[C.ptr[U] + find_small(row, rl, agg_nat[fine.col[e]]) + 1]++;
                 }
             }
-            std::vector<int> gptr(cvals + 1, 0), gidx(fnnz > 0 ? fnnz : 1);
-            for (int64_t e = 0; e < fnnz; ++e) gptr[target[e] + 1]++;
-            for (int64_t k = 0; k < cvals; ++k) gptr[k + 1] += gptr[k];
+            for (int k = 0; k < cnnz; ++k) gptr[k + 1] += gptr[k];
+#pragma omp parallel
             {
-                std::vector<int> pos(gptr.begin(), gptr.end() - 1);
-                for (int64_t e = 0; e < fnnz; ++e) gidx[pos[target[e]]++] = fvpos[e];
+                std::vector<int> pos;
+#pragma omp for schedule(static)
+                for (int U = 0; U < nc_unk; ++U) {
+                    const int* row = C.col.data() + C.ptr[U];
+                    const int rl = C.ptr[U + 1] - C.ptr[U];
+                    pos.assign(gptr.begin() + C.ptr[U], gptr.begin() + C.ptr[U + 1]);
+                    for (int m = nmptr[U]; m < nmptr[U + 1]; ++m) {
+                        const int u = nmidx[m];
+                        for (int e = fine.ptr[u]; e < fine.ptr[u + 1]; ++e)
+                            gidx[pos[find_small(row, rl, agg_nat[fine.col[e]])]++] = fvpos[e];
+                    }
+                }
             }
             Lc.gptr = upload_ints(c, gptr);
             Lc.gidx = upload_ints(c, gidx);
+            Lc.gpos = upload_ints(c, cvpos);
+            Lc.nnz = cnnz;
             if (nc_unk <= kCoarsest || (ccx == 1 && ccy == 1 && ccz == 1)) {
                 if (nc_unk > kCoarsest) {
                     an->multigrid = false;  // cannot coarsen further and too large to invert
@@ -1500,9 +1583,12 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
                 Lc.inv64 = c.allocN<double>((size_t)nc_unk * nc_unk);
                 break;
             }
-            fine = std::move(C);
-            fperm = std::move(cperm);
-            fvpos = std::move(cvpos);
+            owned = std::move(C);
+            owned_perm = std::move(cperm);
+            owned_vpos = std::move(cvpos);
+            finep = &owned;
+            fpermp = &owned_perm;
+            fvposp = &owned_vpos;
         }
     }
     if (an->multigrid) {
@@ -1526,6 +1612,8 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     EQG_CUDA(cudaMemsetAsync(an->counter->ptr, 0, sizeof(unsigned int), c.stream));
     c.sync();
     if (c.verbose > 2) {
+        std::printf("        linear solver analysis: %.1f ms (pattern copy %.1f, level 0 %.1f, coarse levels %.1f)\n",
+                    since(), t_copy, t_level0 - t_copy, since() - t_level0);
         std::printf("        linear solver: %dx%d blocks%s, levels:", bs, bs, an->multigrid ? ", multigrid" : "");
         for (auto& L : an->levels) std::printf(" %d(%zu stages)", L.n, L.stage_ptr.size() - 1);
         std::printf("\n");
@@ -1932,9 +2020,11 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     for (size_t l = 1; l < an.levels.size(); ++l) {
         const Level& F = an.levels[l - 1];
         const Level& C = an.levels[l];
+        EQG_CUDA(cudaMemsetAsync(C.as64->ptr, 0, (size_t)C.vals * sizeof(double), c.stream));
         launch(c, "mg_galerkin", [&] {
-            galerkin_kernel<<<blocksFor(C.vals), kThreads, 0, c.stream>>>(C.vals, C.gptr->as<int>(), C.gidx->as<int>(),
-                                                                          F.as64->as<double>(), C.as64->as<double>());
+            galerkin_kernel<<<blocksFor(C.nnz), kThreads, 0, c.stream>>>(C.nnz, C.gptr->as<int>(), C.gidx->as<int>(),
+                                                                         C.gpos->as<int>(), F.as64->as<double>(),
+                                                                         C.as64->as<double>());
         });
     }
     EQG_CUDA(cudaMemsetAsync(an.factor_status->ptr, 0, sizeof(int), c.stream));

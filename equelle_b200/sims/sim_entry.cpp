@@ -11,6 +11,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <chrono>
 #include <cstring>
 
 void equelleGeneratedCode(equelle::EquelleRuntimeCPU& er);
@@ -32,8 +33,12 @@ int eqg_sim_main(int argc, char** argv, eqg_sim_report* report)
 {
     std::memset(report, 0, sizeof(*report));
     const bool trace = std::getenv("EQG_SIM_TRACE") != nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
     auto note = [&](const char* what) {
-        if (trace) std::fprintf(stderr, "eqg_sim_main: %s\n", what), std::fflush(stderr);
+        if (!trace) return;
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        std::fprintf(stderr, "eqg_sim_main: %9.1f ms  %s\n", ms, what);
+        std::fflush(stderr);
     };
     try {
         note("parameters");
