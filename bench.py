@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["double", "mixed", "refine"], default="double")
     ap.add_argument("--ordering", choices=["multicolor", "natural"], default="multicolor")
-    ap.add_argument("--workload", choices=["twophase3d", "twophase2d", "heat"], default="twophase3d")
+    ap.add_argument("--workload", choices=["twophase3d", "twophase2d", "heat", "swe"], default="twophase3d")
     ap.add_argument("--nx", type=int)
     ap.add_argument("--ny", type=int)
     ap.add_argument("--nz", type=int)
@@ -83,6 +83,15 @@ def workload(a):
         def write(d, steps):
             return cases.two_phase(d, nx, ny, None, steps=steps, corr_len=4.0)
         tol = ["abs_res_tol=1e-8", "linsolver_residual_tolerance=1e-8", "linsolver_max_iterations=5000"]
+    elif a.workload == "swe":
+        nx, ny = a.nx or 4096, a.ny or 4096
+        name, key = "swe", "swe_%dx%d" % (nx, ny)
+        desc = "explicit shallow water %dx%d, first-order Rusanov flux, Heun steps, CFL 0.45" % (nx, ny)
+        cells = nx * ny
+
+        def write(d, steps):
+            return cases.swe(d, nx, ny, steps=steps)
+        tol = []
     else:
         nx, ny = a.nx or 64, a.ny or 64
         name, key = "heateq", "heat_%dx%d" % (nx, ny)
@@ -211,6 +220,8 @@ def main():
 
     name, key, desc, cells, write, tol = workload(a)
     W, K = a.warmup, a.steps
+    if name == "swe":
+        return main_explicit(a, rank, local_rank, world, dist, name, key, desc, cells, write)
     metric = "Newton-steps/s"
     unit = "steps/s"
 
@@ -352,6 +363,124 @@ def config(a, desc, cells):
     return {"workload": desc, "cells": cells, "precision": a.precision, "ordering": a.ordering,
             "dt": "1 day" if a.workload != "heat" else "0.5", "solver": "Newton + BiCGStab, V-cycle with block ILU(0) smoothers",
             "l2": "working set larger than L2 (126 MB), no flush", "parallelism": "replicas"}
+
+
+# Bytes one time step of the shallow-water case must move at least (two
+# stages, each reading the state (24 B) and the bottom (8 B) and writing the
+# state (24 B) per cell, the CFL maximum fused in): the fused-stencil
+# roofline the step time is compared with.
+SWE_BYTES_PER_CELL = 112
+
+
+def main_explicit(a, rank, local_rank, world, dist, name, key, desc, cells, write):
+    """The explicit shallow-water workload: steps are the intervals between
+    the program's outputs (device clock marks); the metric is cell updates
+    per second."""
+    from equelle_b200 import simrun
+    W, K = a.warmup, a.steps
+    metric = unit = "cell-updates/s"
+    oracle = os.path.join(ROOT, "oracle", "_build", "libsim_%s_oracle.so" % name)
+
+    # CPU sample: one step of the same case on at most 1024 x 1024 cells (the
+    # oracle's cost per cell is nearly independent of the grid size; a full
+    # 4096 x 4096 step takes it minutes)
+    from equelle_b200 import cases
+    sx, sy = min(a.nx or 4096, 1024), min(a.ny or 4096, 1024)
+    scells = sx * sy
+
+    def cpu_step():
+        d = input_dir("swe_%dx%d" % (sx, sy), 1, rank)
+        t0 = time.perf_counter()
+        r = simrun.run(name, cases.swe(d, sx, sy, steps=1) + ["output_values=off"], path=oracle)
+        wall = time.perf_counter() - t0
+        ms = r.solve_ms[0]
+        return scells / (ms / 1000.0), ms, wall
+
+    sample = ("oracle (serial C++ restatement of the reference backend), 1 thread: one time step of the same "
+              "case on %dx%d cells, host clock between the program's outputs" % (sx, sy))
+    if a.impl == "reference":
+        if rank != 0:
+            if dist:
+                dist.destroy_process_group()
+            return
+        times = [cpu_step()[1] for _ in range(W + K)]
+        ms_step = sum(times[W:]) / K
+        val = cells / (ms_step / 1000.0)
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": val, "unit": unit, "n_gpus": a.gpus, "steps": K,
+            "warmup": W, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": {"workload": desc, "cells": cells},
+            "cpu_baseline": {"value": val, "unit": unit, "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import equelle_b200
+    equelle_b200.load_library()
+    d = input_dir(key, W + K, rank)
+    args = write(d, W + K) + ["output_values=off", "device=%d" % local_rank] + a.extra
+    if a.kernel_profile:
+        args.append("time_kernel=*")
+    if dist:
+        dist.barrier()
+    with ClockSampler(local_rank) as clk:
+        rep = simrun.run(name, args)
+    if rep.solves < W + K:
+        raise SystemExit("simulator ran %d steps, expected %d" % (rep.solves, W + K))
+    ms = timed_window(rep, W, K)
+    if dist:
+        import torch
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * K * cells / (ms / 1000.0)
+    peak, peak_kind = peaks()
+    step_s = ms / K / 1000.0
+    achieved = SWE_BYTES_PER_CELL * cells / step_s / 1e9
+    st = rep.stats
+    line = {
+        "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded Gaussian bumps, sinusoidal bottom)",
+        "config": {"workload": desc, "cells": cells, "l2": "working set larger than L2 (126 MB), no flush",
+                   "parallelism": "replicas", "execution": "one kernel per runtime operation"},
+        "gpu_launches": int(st.kernel_launches * K / max(rep.solves, 1)),
+        "roofline": {"kernel": "one time step (all its kernels)", "bound": "hbm", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": None, "algorithmic_bytes_per_step": SWE_BYTES_PER_CELL * cells,
+                     "note": "algorithmic bytes of a fused stencil step (112 B per cell); the program runs one "
+                             "kernel per operation and moves more"},
+        "clocks": clk.summary(),
+    }
+    if not a.no_e2e:
+        d2 = input_dir(key, K, rank)
+        args2 = write(d2, K) + ["output_values=none", "device=%d" % local_rank]
+        t0 = time.perf_counter()
+        rep2 = simrun.run(name, args2)
+        wall = time.perf_counter() - t0
+        if dist:
+            import torch
+            t = torch.tensor([wall], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        inbytes = sum(os.path.getsize(os.path.join(d2, f)) for f in os.listdir(d2) if f.endswith(".f64"))
+        line["e2e"] = {"value": world * K * cells / wall, "unit": unit, "h2d_bytes_per_step": inbytes / K,
+                       "d2h_bytes_per_step": 3 * 8 * cells * (K + 1) / K,
+                       "what": "whole program run (grid build, input files, %d steps, output copies of the three "
+                               "fields every step) on the host clock" % K, "steps": rep2.solves}
+    if rank == 0 and world == 1 and not a.no_cpu:
+        val, ms_cpu, wall = cpu_step()
+        line["cpu_baseline"] = {"value": val, "unit": unit, "cores": 1, "kind": "port",
+                                "sample": sample + " (%.1f s step, %.1f s with set-up)" % (ms_cpu / 1000.0, wall)}
+    if a.kernel_profile:
+        prof = json.loads(rep.profile.decode() or "{}")
+        total = sum(v[1] for v in prof.values()) or 1.0
+        line["kernel_profile"] = {k: {"launches": v[0], "ms": round(v[1], 3), "share": round(v[1] / total, 4)}
+                                  for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])[:20]}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def window_counts(rep, w, k):

@@ -50,3 +50,24 @@ def two_phase(dirpath, nx=128, ny=128, nz=64, steps=30, dt=86400.0, seed=0, corr
         "timesteps_filename=" + _write(os.path.join(dirpath, "timesteps.txt"), c["timesteps"], "%.17g"),
     ]
     return args
+
+
+def swe(dirpath, nx=4096, ny=4096, steps=200, seed=0, sigma=40.0, binary=None):
+    """Explicit shallow water, 2D (the 4096x4096 configuration by default).
+    Large grids are written as raw FP64 files (".f64"), which the input
+    functions read without parsing text; u and v start at zero and are
+    given as constants."""
+    os.makedirs(dirpath, exist_ok=True)
+    grid, c = programs.swe_case(nx, ny, steps=steps, seed=seed, sigma=sigma)
+    if binary is None:
+        binary = nx * ny > 1 << 20
+    args = ["%s=%s" % kv for kv in grid.items()]
+    for name in ("h_init", "b_north", "b_south", "b_east", "b_west"):
+        if binary:
+            path = os.path.join(dirpath, name + ".f64")
+            np.asarray(c[name], dtype="<f8").tofile(path)
+        else:
+            path = _write(os.path.join(dirpath, name + ".txt"), c[name], "%.17g")
+        args += [name + "_from_file=true", name + "_filename=" + path]
+    args += ["u_init=0", "v_init=0", "cfl=%r" % c["cfl"], "num_steps=%d" % steps]
+    return args

@@ -206,3 +206,144 @@ def two_phase_case(nx, ny, nz=None, steps=2, dt=86400.0, seed=0, corr_len=8.0, c
                 sw_initial=np.full(n, 0.2), timesteps=[dt] * steps, corey=corey,
                 anchor_cells=np.array([prod[0]], dtype=np.int32))
     return grid, case
+
+
+def swe(er, h_init, u_init, v_init, b_north, b_south, b_east, b_west, dx, dy, cfl, num_steps, on_step=None):
+    """Explicit shallow-water equations (equelle_b200/sims/swe.cpp, op for
+    op): Rusanov fluxes, wall fluxes, bathymetry source, Heun steps with the
+    CFL time step.  Returns [(w, hu, hv)] after each step (host arrays)."""
+    col = er.collection
+    b_north, b_south, b_east, b_west = col(b_north), col(b_south), col(b_east), col(b_west)
+    h_init, u_init, v_init = col(h_init), col(u_init), col(v_init)
+    b_mid = (((b_north + b_south) + b_east) + b_west) / 4.0
+    gravity, dry, dummy = 9.81, 0.05, 1000.0
+    int_faces = er.interiorFaces()
+    bound = er.boundaryFaces()
+    cells = er.allCells()
+    vol = er.norm(cells)
+    area = er.norm(er.allFaces())
+    int_orientation = er.normal(int_faces)
+    nx, ny = int_orientation.col(0), int_orientation.col(1)
+    first = er.firstCell(int_faces)
+    second = er.secondCell(int_faces)
+    bFirst = er.operatorOn(b_mid, cells, first)
+    bSecond = er.operatorOn(b_mid, cells, second)
+    bound_orientation = er.normal(bound)
+    bound_cells = er.trinaryIf(er.isEmpty(er.firstCell(bound)), er.secondCell(bound), er.firstCell(bound))
+    bound_b = er.operatorOn(b_mid, cells, bound_cells)
+    bound_signX = er.trinaryIf(bound_orientation.col(0) > 0.0, er.operatorExtend(1.0, bound), er.operatorExtend(-1.0, bound))
+    bound_signY = er.trinaryIf(bound_orientation.col(1) > 0.0, er.operatorExtend(1.0, bound), er.operatorExtend(-1.0, bound))
+    bx = (b_east - b_west) / dx
+    by = (b_north - b_south) / dy
+
+    def sideFlux(w, hu, hv, b):
+        rawHeight = w - b
+        wet = rawHeight > dry
+        height = er.trinaryIf(wet, rawHeight, er.operatorExtend(dummy, int_faces))
+        qn = (hu * nx) + (hv * ny)
+        un = qn / height
+        pressure = (0.5 * gravity) * (height * height)
+        zero = er.operatorExtend(0.0, int_faces)
+        f0 = er.trinaryIf(wet, qn, zero)
+        f1 = er.trinaryIf(wet, (hu * un) + (pressure * nx), zero)
+        f2 = er.trinaryIf(wet, (hv * un) + (pressure * ny), zero)
+        speed = er.trinaryIf(wet, er.sqrt(un * un) + er.sqrt(gravity * height), zero)
+        return f0, f1, f2, speed
+
+    def getFlux(w, hu, hv):
+        wL = er.operatorOn(w, cells, first)
+        huL = er.operatorOn(hu, cells, first)
+        hvL = er.operatorOn(hv, cells, first)
+        wR = er.operatorOn(w, cells, second)
+        huR = er.operatorOn(hu, cells, second)
+        hvR = er.operatorOn(hv, cells, second)
+        fL = sideFlux(wL, huL, hvL, bFirst)
+        fR = sideFlux(wR, huR, hvR, bSecond)
+        a = er.trinaryIf(fL[3] > fR[3], fL[3], fR[3])
+        intFlux0 = (0.5 * (fL[0] + fR[0])) - ((0.5 * a) * (wR - wL))
+        intFlux1 = (0.5 * (fL[1] + fR[1])) - ((0.5 * a) * (huR - huL))
+        intFlux2 = (0.5 * (fL[2] + fR[2])) - ((0.5 * a) * (hvR - hvL))
+        bound_height = er.operatorOn(w, cells, bound_cells) - bound_b
+        b_flux = er.trinaryIf(bound_height > dry, (0.5 * gravity) * (bound_height * bound_height),
+                              er.operatorExtend(0.0, bound))
+        boundFlux1 = (er.sqrt(bound_orientation.col(0) * bound_orientation.col(0)) * b_flux) * bound_signX
+        boundFlux2 = (er.sqrt(bound_orientation.col(1) * bound_orientation.col(1)) * b_flux) * bound_signY
+        all_faces = er.allFaces()
+        all0 = er.operatorExtend(intFlux0, int_faces, all_faces) * area
+        all1 = (er.operatorExtend(intFlux1, int_faces, all_faces) + er.operatorExtend(boundFlux1, bound, all_faces)) * area
+        all2 = (er.operatorExtend(intFlux2, int_faces, all_faces) + er.operatorExtend(boundFlux2, bound, all_faces)) * area
+        return all0, all1, all2
+
+    def sourceTerm(w):
+        secondTerm_x = ((w - b_east) + (w - b_west)) / 2.0
+        secondTerm_y = ((w - b_north) + (w - b_south)) / 2.0
+        dryTerm = er.trinaryIf((w - b_mid) > dry, er.operatorExtend(1.0, cells), er.operatorExtend(0.0, cells))
+        return (((-gravity) * bx) * secondTerm_x) * dryTerm, (((-gravity) * by) * secondTerm_y) * dryTerm
+
+    def eulerStage(w, hu, hv, dt):
+        flux = getFlux(w, hu, hv)
+        source = sourceTerm(w)
+        w1 = w + ((dt / vol) * (-er.divergence(flux[0])))
+        hu1 = hu + ((dt / vol) * ((-er.divergence(flux[1])) + (vol * source[0])))
+        hv1 = hv + ((dt / vol) * ((-er.divergence(flux[2])) + (vol * source[1])))
+        return w1, hu1, hv1
+
+    def maxSpeed(w, hu, hv):
+        rawHeight = w - b_mid
+        wet = rawHeight > dry
+        height = er.trinaryIf(wet, rawHeight, er.operatorExtend(dummy, cells))
+        u = hu / height
+        v = hv / height
+        speed = er.trinaryIf(wet, er.sqrt((u * u) + (v * v)) + er.sqrt(gravity * height), er.operatorExtend(0.0, cells))
+        return er.maxReduce(speed)
+
+    w0 = h_init + b_mid
+    hu0 = h_init * u_init
+    hv0 = h_init * v_init
+    h_min = dx if dx < dy else dy
+    out = []
+    for _ in range(int(num_steps)):
+        dt = (cfl * h_min) / maxSpeed(w0, hu0, hv0)
+        qs = eulerStage(w0, hu0, hv0, dt)
+        qss = eulerStage(qs[0], qs[1], qs[2], dt)
+        w0 = (0.5 * w0) + (0.5 * qss[0])
+        hu0 = (0.5 * hu0) + (0.5 * qss[1])
+        hv0 = (0.5 * hv0) + (0.5 * qss[2])
+        out.append((w0.value(), hu0.value(), hv0.value()))
+        if on_step:
+            on_step(w0, hu0, hv0)
+    return out
+
+
+def swe_case(nx, ny, steps=200, seed=0, bumps=8, amplitude=0.1, sigma=40.0, bottom=0.05, dx=1.0, dy=1.0):
+    """Dam-break-like shallow-water case: depth 1 plus `bumps` Gaussian
+    bumps (amplitude, sigma in cells, centres uniform over the domain), zero
+    momentum, bottom b = bottom * sin(2 pi kx x / Lx + px) sin(2 pi ky y / Ly
+    + py) with kx, ky in {1..4} and phases from the seed, evaluated at the
+    cell faces' midpoints.  Returns (grid parameters, swe() keyword
+    arguments)."""
+    rng = np.random.default_rng(seed)
+    xc = (np.arange(nx) + 0.5) * dx
+    yc = (np.arange(ny) + 0.5) * dy
+    X, Y = np.meshgrid(xc, yc)  # [j, i]: cell i + nx j
+    h = np.ones((ny, nx))
+    cx = rng.uniform(0.0, nx * dx, bumps)
+    cy = rng.uniform(0.0, ny * dy, bumps)
+    for k in range(bumps):
+        r2 = (X - cx[k]) ** 2 + (Y - cy[k]) ** 2
+        h += amplitude * np.exp(-r2 / (2.0 * (sigma * dx) ** 2))
+    kx, ky = rng.integers(1, 5, 2)
+    px, py = rng.uniform(0.0, 2.0 * np.pi, 2)
+    Lx, Ly = nx * dx, ny * dy
+
+    def b(x, y):
+        return bottom * np.sin(2.0 * np.pi * kx * x / Lx + px) * np.sin(2.0 * np.pi * ky * y / Ly + py)
+
+    n = nx * ny
+    flat = lambda a: np.ascontiguousarray(a.reshape(n))
+    grid = dict(grid_dim=2, nx=nx, ny=ny, dx=dx, dy=dy)
+    case = dict(h_init=flat(h), u_init=np.zeros(n), v_init=np.zeros(n),
+                b_north=flat(b(X, Y + 0.5 * dy)), b_south=flat(b(X, Y - 0.5 * dy)),
+                b_east=flat(b(X + 0.5 * dx, Y)), b_west=flat(b(X - 0.5 * dx, Y)),
+                dx=dx, dy=dy, cfl=0.45, num_steps=steps)
+    return grid, case

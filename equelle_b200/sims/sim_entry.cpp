@@ -77,6 +77,26 @@ int eqg_sim_main(int argc, char** argv, eqg_sim_report* report)
         }
         report->solves = k;
         if (first_start >= 0) equelle::detail::check(eqg_runtime_elapsed_ms(rt, first_start, last_end, &report->total_ms));
+        if (k == 0 && !er.outputTags().empty()) {
+            // an explicit program: its time steps are the intervals between
+            // the outputs of its first output tag (the end of output s to the
+            // start of output s + 1)
+            const auto& marks = er.outputMarks(er.outputTags().front());
+            int64_t steps = 0;
+            for (size_t s = 0; s + 1 < marks.size() && s < 4096; ++s, ++steps) {
+                double ms = 0.0;
+                equelle::detail::check(eqg_runtime_elapsed_ms(rt, marks[s].second, marks[s + 1].first, &ms));
+                report->solve_ms[s] = ms;
+                if (s + 2 < marks.size()) {
+                    equelle::detail::check(eqg_runtime_elapsed_ms(rt, marks[s].second, marks[s + 1].second, &ms));
+                    report->gap_ms[s] = ms;
+                }
+            }
+            report->solves = steps;
+            if (steps > 0)
+                equelle::detail::check(
+                    eqg_runtime_elapsed_ms(rt, marks.front().second, marks[steps].first, &report->total_ms));
+        }
         equelle::detail::check(eqg_runtime_stats(rt, &report->stats));
         int64_t need = 0;
         equelle::detail::check(eqg_runtime_kernel_profile(rt, report->profile, sizeof(report->profile), &need));

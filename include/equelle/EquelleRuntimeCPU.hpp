@@ -30,6 +30,41 @@
 
 namespace equelle {
 
+namespace detail {
+
+// The values of an input file: whitespace-separated text (the reference's
+// format), or raw little-endian FP64 when the file name ends in ".f64"
+// (large inputs, where parsing text would dominate a run).
+inline std::vector<double> read_values(const std::string& filename)
+{
+    const bool binary = filename.size() > 4 && filename.compare(filename.size() - 4, 4, ".f64") == 0;
+    if (binary) {
+        std::ifstream is(filename.c_str(), std::ios::binary | std::ios::ate);
+        if (!is) {
+            throw std::runtime_error("Could not find file " + filename);
+        }
+        const std::streamsize bytes = is.tellg();
+        if (bytes < 0 || bytes % 8 != 0) {
+            throw std::runtime_error("File " + filename + " does not hold whole doubles");
+        }
+        std::vector<double> v((size_t)(bytes / 8));
+        is.seekg(0);
+        if (!v.empty() && !is.read(reinterpret_cast<char*>(v.data()), bytes)) {
+            throw std::runtime_error("Could not read file " + filename);
+        }
+        return v;
+    }
+    std::ifstream is(filename.c_str());
+    if (!is) {
+        throw std::runtime_error("Could not find file " + filename);
+    }
+    std::istream_iterator<double> beg(is);
+    std::istream_iterator<double> end;
+    return std::vector<double>(beg, end);
+}
+
+}  // namespace detail
+
 class EquelleRuntimeCPU {
 public:
     /// Builds the grid from grid_dim, nx, ny, nz, dx, dy, dz and reads
@@ -41,6 +76,7 @@ public:
           output_dir_(param.getDefault<std::string>("output_dir", "")),
           output_values_(param.getDefault<std::string>("output_values", "all") == "all"),
           output_last_(param.getDefault<std::string>("output_values", "all") == "last"),
+          output_off_(param.getDefault<std::string>("output_values", "all") == "off"),
           verbose_(param.getDefault("verbose", 0))
     {
         const auto items = param.items();
@@ -242,9 +278,39 @@ public:
     }
     /// Extensions for timing runs: output_values=none still copies each
     /// collection to the host but neither prints nor writes it;
-    /// output_values=last keeps the last collection of each tag and writes
-    /// <output_dir><tag>-last.output (precision 17) when the runtime ends.
+    /// output_values=off does not copy it; output_values=last keeps the last
+    /// collection of each tag and writes <output_dir><tag>-last.output
+    /// (precision 17) when the runtime ends.  Every call also records two
+    /// device clock marks, before and after the copy (outputMarks): for an
+    /// explicit program, whose time steps are the intervals between its
+    /// outputs.
     void output(const String& tag, const CollOfScalar& vals)
+    {
+        int before = 0, after = 0;
+        detail::check(eqg_runtime_mark(rt_, &before));
+        if (!output_off_) {
+            writeOutput(tag, vals);
+        }
+        detail::check(eqg_runtime_mark(rt_, &after));
+        auto it = output_marks_.find(tag);
+        if (it == output_marks_.end()) {
+            output_tags_.push_back(tag);
+            it = output_marks_.emplace(tag, std::vector<std::pair<int, int>>()).first;
+        }
+        it->second.emplace_back(before, after);
+    }
+    /// Output tags in the order of their first output.
+    const std::vector<String>& outputTags() const { return output_tags_; }
+    /// (before, after) clock marks of every output of `tag`.
+    const std::vector<std::pair<int, int>>& outputMarks(const String& tag) const
+    {
+        static const std::vector<std::pair<int, int>> none;
+        auto it = output_marks_.find(tag);
+        return it == output_marks_.end() ? none : it->second;
+    }
+
+private:
+    void writeOutput(const String& tag, const CollOfScalar& vals)
     {
         std::vector<double> v = vals.value();
         if (output_last_) {
@@ -278,6 +344,8 @@ public:
             std::cout << std::endl;
         }
     }
+
+public:
     ///@}
 
     /** @name Input (EquelleRuntimeCPU.cpp:485-551, _impl.hpp:342-365) */
@@ -302,13 +370,7 @@ public:
         eqg_coll* out = nullptr;
         if (from_file) {
             const String filename = param_.get<String>(name + "_filename");
-            std::ifstream is(filename.c_str());
-            if (!is) {
-                throw std::runtime_error("Could not find file " + filename);
-            }
-            std::istream_iterator<double> beg(is);
-            std::istream_iterator<double> end;
-            std::vector<double> data(beg, end);
+            const std::vector<double> data = detail::read_values(filename);
             if (int(data.size()) != size) {
                 throw std::runtime_error("Unexpected size of input data for " + name + " in file " + filename);
             }
@@ -502,6 +564,9 @@ private:
     std::string output_dir_;
     bool output_values_;
     bool output_last_;
+    bool output_off_;
+    std::map<String, std::vector<std::pair<int, int>>> output_marks_;
+    std::vector<String> output_tags_;
     std::map<std::string, std::vector<double>> last_output_;
     int verbose_;
     eqg_runtime* rt_ = nullptr;
