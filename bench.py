@@ -47,7 +47,12 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["double", "mixed", "refine"], default="double")
     ap.add_argument("--ordering", choices=["multicolor", "natural"], default="multicolor")
-    ap.add_argument("--workload", choices=["twophase3d", "twophase2d", "heat", "swe"], default="twophase3d")
+    ap.add_argument("--workload", choices=["twophase3d", "twophase2d", "heat", "swe", "batched", "serve"],
+                    default="twophase3d")
+    ap.add_argument("--instances", type=int, default=64, help="batched: number of instances")
+    ap.add_argument("--requests", type=int, default=48, help="serve: requests per arrival rate")
+    ap.add_argument("--rates", default="50,200,1000", help="serve: Poisson arrival rates (req/s)")
+    ap.add_argument("--slots", type=int, default=32, help="batched/serve: instances on the GPU at once")
     ap.add_argument("--nx", type=int)
     ap.add_argument("--ny", type=int)
     ap.add_argument("--nz", type=int)
@@ -218,6 +223,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
 
+    if a.workload in ("batched", "serve"):
+        return main_many(a, rank, world, dist)
     name, key, desc, cells, write, tol = workload(a)
     W, K = a.warmup, a.steps
     if name == "swe":
@@ -363,6 +370,85 @@ def config(a, desc, cells):
     return {"workload": desc, "cells": cells, "precision": a.precision, "ordering": a.ordering,
             "dt": "1 day" if a.workload != "heat" else "0.5", "solver": "Newton + BiCGStab, V-cycle with block ILU(0) smoothers",
             "l2": "working set larger than L2 (126 MB), no flush", "parallelism": "replicas"}
+
+
+def main_many(a, rank, world, dist):
+    """Many independent instances on the GPU (equelle_b200/serve.py):
+    `batched` runs a seeded set of 2D two-phase instances all at once;
+    `serve` feeds requests (heat or 2D two-phase) at Poisson arrival rates.
+    Both compare against the same requests run one at a time in plain FP64.
+    Times are host wall clock around runs that end with their results on
+    the host."""
+    from equelle_b200 import serve
+    import equelle_b200
+    equelle_b200.load_library()
+    root = os.path.join(tempfile.gettempdir(), "eqg_bench", "%s_r%d" % (a.workload, rank))
+    if a.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or serving mode; "
+                              "its arm for these workloads is the one-at-a-time FP64 line of our bench"}))
+        if dist:
+            dist.destroy_process_group()
+        return
+    if dist:
+        dist.barrier()
+
+    def prepared(reqs, precision):
+        for r in reqs:
+            serve.prepare(r, os.path.join(root, "%s_%d_%d_%d" % (r.program, r.nx, r.steps, r.seed)),
+                          ["linsolver_precision=" + precision, "device=%d" % int(os.environ.get("LOCAL_RANK", "0"))])
+        return reqs
+
+    def summary(recs, wall):
+        steps = sum(r.steps for r in recs)
+        lat = [r.latency for r in recs]
+        return {"requests": len(recs), "instance_steps": steps, "wall_s": wall,
+                "instance_steps_per_s": steps / wall, "requests_per_s": len(recs) / wall,
+                "latency_p50_s": serve.percentile(lat, 50), "latency_p99_s": serve.percentile(lat, 99),
+                "errors": sum(1 for r in recs if r.error)}
+
+    if a.workload == "batched":
+        reqs = serve.make_requests(a.instances, seed=1, programs=("twophase",), side=(32, 512), steps=(a.steps, a.steps))
+        seq = summary(*serve.Server(slots=1).run(prepared(reqs, "double"), realtime=False))
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+            bat = summary(*serve.Server(slots=a.slots).run(prepared(reqs, "mixed"), realtime=False))
+        value = world * bat["instance_steps_per_s"]
+        line = {"metric": "instance-steps/s", "value": value, "unit": "instance-steps/s", "n_gpus": world,
+                "steps": a.steps, "warmup": 0, "ms_per_step": 1000.0 * bat["wall_s"] / bat["instance_steps"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+                "data": "synthetic (seeded log-permeability per instance, corner wells)",
+                "config": {"workload": "%d 2D two-phase instances, sides log-uniform in [32, 512], %d steps each, "
+                                       "%d on the GPU at once (own runtime, stream and host thread each)"
+                                       % (a.instances, a.steps, a.slots), "precision": "mixed (batched), "
+                                       "double (sequential)", "parallelism": "replicas"},
+                "batched": bat, "sequential_fp64": seq,
+                "speedup_vs_sequential": bat["instance_steps_per_s"] / seq["instance_steps_per_s"],
+                "clocks": clk.summary()}
+    else:
+        rates = [float(x) for x in a.rates.split(",")]
+        per_rate = {}
+        base = serve.make_requests(a.requests, seed=2, side=(64, 512), steps=(10, 30))
+        seq = summary(*serve.Server(slots=1).run(prepared(base, "double"), realtime=False))
+        for lam in rates:
+            reqs = serve.make_requests(a.requests, seed=2, rate=lam, side=(64, 512), steps=(10, 30))
+            recs, wall = serve.Server(slots=a.slots).run(prepared(reqs, "mixed"), realtime=True)
+            per_rate["%g" % lam] = summary(recs, wall)
+        top = per_rate["%g" % rates[-1]]
+        line = {"metric": "requests/s", "value": world * top["requests_per_s"], "unit": "requests/s",
+                "n_gpus": world, "steps": a.requests, "warmup": 0, "ms_per_step": 1000.0 / top["requests_per_s"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+                "data": "synthetic (seeded requests: heat or 2D two-phase, sides log-uniform in [64, 512], "
+                        "10-30 steps)",
+                "config": {"workload": "serving loop, Poisson arrivals at %s req/s, %d requests per rate, up to %d on "
+                                       "the GPU at once, admission under 150 GB" % (a.rates, a.requests, a.slots),
+                           "parallelism": "replicas"},
+                "per_rate": per_rate, "one_at_a_time_fp64": seq,
+                "throughput_vs_one_at_a_time": top["requests_per_s"] / seq["requests_per_s"]}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 # Bytes one time step of the shallow-water case must move at least (two

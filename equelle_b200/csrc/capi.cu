@@ -7,6 +7,8 @@
 // residual evaluation costs only numeric kernels from its second call on.
 #include "eqg_internal.cuh"
 
+#include <mutex>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -56,6 +58,7 @@ struct HostProfile {
     }
 };
 HostProfile g_host_profile;
+std::mutex g_host_profile_mutex;  // runtimes may be driven from several threads
 
 template <class F>
 int guarded(const char* name, F&& f)
@@ -72,6 +75,7 @@ int guarded(const char* name, F&& f)
         ~Timer()
         {
             if (!g_host_profile.on) return;
+            std::lock_guard<std::mutex> lock(g_host_profile_mutex);
             auto& e = g_host_profile.calls[name];
             const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
             e.calls++;

@@ -52,6 +52,8 @@
 #include <cstring>
 #include <numeric>
 
+#include <omp.h>
+
 namespace eqg {
 
 namespace {
@@ -1414,6 +1416,10 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     auto since = [&] {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
     };
+    // host threads of the analysis (host_threads=k; default: OpenMP's), for
+    // processes that drive several runtimes at once
+    const int host_threads = c.param_i("host_threads", 0);
+    if (host_threads > 0) omp_set_num_threads(host_threads);
     auto an = std::make_shared<SolverAnalysis>();
     const int n = p.rows;
     an->n = n;

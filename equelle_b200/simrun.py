@@ -2,6 +2,7 @@
 library's `eqg_sim_main` (equelle_b200/sims/sim_entry.cpp)."""
 import ctypes as C
 import os
+import threading
 
 from . import LIB_DIR, capi
 
@@ -22,12 +23,18 @@ class SimReport(C.Structure):
 
 
 _loaded = {}
+_load_lock = threading.Lock()
 
 
 def sim_library(name, path=None):
     """The device build (equelle_b200/lib/libsim_<name>.so) unless `path`
     names another build of the same simulator source."""
     path = path or os.path.join(LIB_DIR, "libsim_%s.so" % name)
+    with _load_lock:
+        return _load(path)
+
+
+def _load(path):
     if path not in _loaded:
         if not os.path.exists(path):
             raise RuntimeError("simulator library %s is not built" % path)
