@@ -396,7 +396,8 @@ def main_many(a, rank, world, dist):
     def prepared(reqs, precision):
         for r in reqs:
             serve.prepare(r, os.path.join(root, "%s_%d_%d_%d" % (r.program, r.nx, r.steps, r.seed)),
-                          ["linsolver_precision=" + precision, "device=%d" % int(os.environ.get("LOCAL_RANK", "0"))])
+                          ["linsolver_precision=" + precision, "device=%d" % int(os.environ.get("LOCAL_RANK", "0"))]
+                          + a.extra)
         return reqs
 
     def summary(recs, wall):

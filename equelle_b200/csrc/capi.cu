@@ -252,7 +252,7 @@ eqg_coll* apply_operator(const CoreP& cp, const OpMatrix& m, const eqg_coll* x)
     Core& c = *cp;
     if (x->n != m.n_src) fail(EQG_ERR_ARG, "operator applied to a collection of the wrong size");
     Buf val = c.allocN<double>(m.n_out > 0 ? m.n_out : 1);
-    opmat_apply_values(c, m, x->val->as<double>(), val->as<double>());
+    opmat_apply_values(c, m, coll_values(c, x), val->as<double>());
     if (!x->pat) return new_coll(cp, m.n_out, val);
     PatternP p = pattern_spgemm(c, m, x->pat);
     Buf jv = c.allocN<double>(p->nnz > 0 ? p->nnz : 1);
@@ -353,6 +353,7 @@ int eqg_runtime_create(int nparams, const char* const* keys, const char* const* 
         c.dy = c.param_d("dy", 1.0);
         c.dz = c.param_d("dz", 1.0);
         c.verbose = c.param_i("verbose", 0);
+        c.lazy = c.param_i("lazy", 0) != 0;
         c.max_iter = c.param_i("max_iter", 10);
         c.abs_res_tol = c.param_d("abs_res_tol", 1e-6);
         c.timed_kernel = c.param_s("time_kernel", "");
@@ -686,7 +687,7 @@ int eqg_set_select(eqg_runtime* rt, const eqg_mask* pred, const eqg_set* a, cons
         if (a->n != pred->n || b->n != pred->n) fail(EQG_ERR_ARG, "trinaryIf: size mismatch");
         if (a->entity != b->entity) fail(EQG_ERR_ARG, "trinaryIf: entity kinds differ");
         Buf o = c.allocN<int32_t>(pred->n > 0 ? pred->n : 1);
-        k_set_select(c, pred->v->as<uint8_t>(), a->idx->as<int32_t>(), b->idx->as<int32_t>(), o->as<int32_t>(),
+        k_set_select(c, mask_values(c, pred), a->idx->as<int32_t>(), b->idx->as<int32_t>(), o->as<int32_t>(),
                      pred->n);
         *out = new_set(rt->core, a->entity, pred->n, o);
     });
@@ -734,6 +735,7 @@ int eqg_mask_to_host(const eqg_mask* m, uint8_t* out)
 {
     return guarded(__func__, [&] {
         need(m, "mask");
+        mask_values(*m->core, m);
         download(*m->core, out, m->v->ptr, (size_t)m->n);
     });
 }
@@ -745,7 +747,10 @@ void eqg_mask_retain(eqg_mask* m)
 
 void eqg_mask_release(eqg_mask* m)
 {
-    if (m && --m->refs == 0) delete m;
+    if (m && --m->refs == 0) {
+        lazy_forget(m);
+        delete m;
+    }
 }
 
 int eqg_mask_logic(eqg_runtime* rt, int op, const eqg_mask* a, const eqg_mask* b, eqg_mask** out)
@@ -760,7 +765,12 @@ int eqg_mask_logic(eqg_runtime* rt, int op, const eqg_mask* a, const eqg_mask* b
         if (op < EQG_AND || op > EQG_NOT) fail(EQG_ERR_ARG, "unknown mask operator");
         Core& c = *rt->core;
         Buf o = c.allocN<uint8_t>(a->n > 0 ? a->n : 1);
-        k_mask_logic(c, op, a->v->as<uint8_t>(), op == EQG_NOT ? a->v->as<uint8_t>() : b->v->as<uint8_t>(),
+        if (c.lazy) {
+            *out = lazy_mask(rt->core, a->n,
+                             lazy_make(LZ_LOGIC, op, a->n, true, lazy_node(a), op == EQG_NOT ? nullptr : lazy_node(b)));
+            return;
+        }
+        k_mask_logic(c, op, mask_values(c, a), op == EQG_NOT ? mask_values(c, a) : mask_values(c, b),
                      o->as<uint8_t>(), a->n);
         *out = new_mask(rt->core, a->n, o);
     });
@@ -782,6 +792,10 @@ int eqg_coll_constant(eqg_runtime* rt, double v, int64_t n, eqg_coll** out)
         need(rt, "runtime");
         if (n < 0) fail(EQG_ERR_ARG, "negative size");
         Core& c = *rt->core;
+        if (c.lazy) {
+            *out = lazy_coll(rt->core, n, lazy_make(LZ_CONST, 0, n, false, nullptr, nullptr, nullptr, v));
+            return;
+        }
         Buf b = c.allocN<double>(n > 0 ? n : 1);
         k_fill(c, b->as<double>(), v, n);
         *out = new_coll(rt->core, n, b);
@@ -800,6 +814,7 @@ int eqg_coll_to_host(const eqg_coll* c, double* out)
 {
     return guarded(__func__, [&] {
         need(c, "collection");
+        coll_values(*c->core, c);
         download(*c->core, out, c->val->ptr, (size_t)c->n * 8);
     });
 }
@@ -844,7 +859,10 @@ void eqg_coll_retain(eqg_coll* c)
 
 void eqg_coll_release(eqg_coll* c)
 {
-    if (c && --c->refs == 0) delete c;
+    if (c && --c->refs == 0) {
+        lazy_forget(c);
+        delete c;
+    }
 }
 
 int eqg_variable(eqg_runtime* rt, const eqg_coll* init, eqg_coll** out)
@@ -854,6 +872,7 @@ int eqg_variable(eqg_runtime* rt, const eqg_coll* init, eqg_coll** out)
         need(init, "collection");
         Core& c = *rt->core;
         if (init->n > INT32_MAX) fail(EQG_ERR_UNSUPPORTED, "collection too large");
+        settle(c, init);
         *out = new_coll(rt->core, init->n, init->val, pattern_identity(c, (int)init->n), ones(c, init->n));
     });
 }
@@ -863,6 +882,7 @@ int eqg_value_of(eqg_runtime* rt, const eqg_coll* x, eqg_coll** out)
     return guarded(__func__, [&] {
         need(rt, "runtime");
         need(x, "collection");
+        settle(*rt->core, x);
         *out = new_coll(rt->core, x->n, x->val);
     });
 }
@@ -877,8 +897,12 @@ int eqg_binary(eqg_runtime* rt, int op, const eqg_coll* a, const eqg_coll* b, eq
         if (a->n != b->n)
             fail(EQG_ERR_ARG, "size mismatch in binary operator: " + std::to_string(a->n) + " vs " + std::to_string(b->n));
         if (op < EQG_ADD || op > EQG_DIV) fail(EQG_ERR_ARG, "unknown binary operator");
+        if (lazy_ok(c, a) && lazy_ok(c, b)) {
+            *out = lazy_coll(rt->core, a->n, lazy_make(LZ_BIN, op, a->n, false, lazy_node(a), lazy_node(b)));
+            return;
+        }
         Buf val = c.allocN<double>(a->n > 0 ? a->n : 1);
-        k_binary(c, op, a->val->as<double>(), b->val->as<double>(), val->as<double>(), a->n);
+        k_binary(c, op, coll_values(c, a), coll_values(c, b), val->as<double>(), a->n);
         // A sum with one Jacobian shares that Jacobian unchanged (Zero + J).
         if (op == EQG_ADD && (!a->pat || !b->pat)) {
             const eqg_coll* j = a->pat ? a : b;
@@ -904,8 +928,13 @@ int eqg_binary_scalar(eqg_runtime* rt, int op, const eqg_coll* a, double s, int 
         need(a, "collection");
         Core& c = *rt->core;
         if (op < EQG_ADD || op > EQG_DIV) fail(EQG_ERR_ARG, "unknown binary operator");
+        if (lazy_ok(c, a)) {
+            *out = lazy_coll(rt->core, a->n,
+                             lazy_make(LZ_BINS, op, a->n, false, lazy_node(a), nullptr, nullptr, s, scalar_left));
+            return;
+        }
         Buf val = c.allocN<double>(a->n > 0 ? a->n : 1);
-        k_binary_scalar(c, op, a->val->as<double>(), s, scalar_left, val->as<double>(), a->n);
+        k_binary_scalar(c, op, coll_values(c, a), s, scalar_left, val->as<double>(), a->n);
         if (!a->pat) {
             *out = new_coll(rt->core, a->n, val);
             return;
@@ -955,8 +984,12 @@ int eqg_unary(eqg_runtime* rt, int op, const eqg_coll* a, eqg_coll** out)
         need(a, "collection");
         Core& c = *rt->core;
         if (op < EQG_NEG || op > EQG_ABS) fail(EQG_ERR_ARG, "unknown unary operator");
+        if (lazy_ok(c, a)) {
+            *out = lazy_coll(rt->core, a->n, lazy_make(LZ_UNARY, op, a->n, false, lazy_node(a)));
+            return;
+        }
         Buf val = c.allocN<double>(a->n > 0 ? a->n : 1);
-        k_unary_value(c, op, a->val->as<double>(), val->as<double>(), a->n);
+        k_unary_value(c, op, coll_values(c, a), val->as<double>(), a->n);
         JacArgs ja;
         ja.rule = op == EQG_NEG ? JR_NEG : op == EQG_SQRT ? JR_SQRT : JR_SIGN;
         ja.va = a->val->as<double>();
@@ -974,8 +1007,12 @@ int eqg_compare(eqg_runtime* rt, int op, const eqg_coll* a, const eqg_coll* b, e
         if (a->n != b->n) fail(EQG_ERR_ARG, "comparison size mismatch");
         if (op < EQG_LT || op > EQG_NE) fail(EQG_ERR_ARG, "unknown comparison");
         Core& c = *rt->core;
+        if (c.lazy) {
+            *out = lazy_mask(rt->core, a->n, lazy_make(LZ_CMP, op, a->n, true, lazy_node(a), lazy_node(b)));
+            return;
+        }
         Buf m = c.allocN<uint8_t>(a->n > 0 ? a->n : 1);
-        k_compare(c, op, a->val->as<double>(), b->val->as<double>(), m->as<uint8_t>(), a->n);
+        k_compare(c, op, coll_values(c, a), coll_values(c, b), m->as<uint8_t>(), a->n);
         *out = new_mask(rt->core, a->n, m);
     });
 }
@@ -987,8 +1024,13 @@ int eqg_compare_scalar(eqg_runtime* rt, int op, const eqg_coll* a, double s, int
         need(a, "collection");
         if (op < EQG_LT || op > EQG_NE) fail(EQG_ERR_ARG, "unknown comparison");
         Core& c = *rt->core;
+        if (c.lazy) {
+            *out = lazy_mask(rt->core, a->n,
+                             lazy_make(LZ_CMPS, op, a->n, true, lazy_node(a), nullptr, nullptr, s, scalar_left));
+            return;
+        }
         Buf m = c.allocN<uint8_t>(a->n > 0 ? a->n : 1);
-        k_compare_scalar(c, op, a->val->as<double>(), s, scalar_left, m->as<uint8_t>(), a->n);
+        k_compare_scalar(c, op, coll_values(c, a), s, scalar_left, m->as<uint8_t>(), a->n);
         *out = new_mask(rt->core, a->n, m);
     });
 }
@@ -1075,12 +1117,17 @@ int eqg_select(eqg_runtime* rt, const eqg_mask* pred, const eqg_coll* a, const e
         need(b, "iffalse");
         if (a->n != pred->n || b->n != pred->n) fail(EQG_ERR_ARG, "trinaryIf: size mismatch");
         Core& c = *rt->core;
+        if (lazy_ok(c, a) && lazy_ok(c, b)) {
+            *out = lazy_coll(rt->core, pred->n,
+                             lazy_make(LZ_SEL, 0, pred->n, false, lazy_node(pred), lazy_node(a), lazy_node(b)));
+            return;
+        }
         Buf val = c.allocN<double>(pred->n > 0 ? pred->n : 1);
-        k_select_value(c, pred->v->as<uint8_t>(), a->val->as<double>(), b->val->as<double>(), val->as<double>(),
-                       pred->n);
+        const uint8_t* mv = mask_values(c, pred);
+        k_select_value(c, mv, coll_values(c, a), coll_values(c, b), val->as<double>(), pred->n);
         JacArgs ja;
         ja.rule = JR_SELECT;
-        ja.mask = pred->v->as<uint8_t>();
+        ja.mask = mv;
         *out = jac_rule(rt->core, pred->n, val, ja, a, b);
     });
 }
@@ -1114,7 +1161,7 @@ int eqg_reduce(eqg_runtime* rt, int op, const eqg_coll* a, double* out)
         need(a, "collection");
         if (op < EQG_MIN || op > EQG_PROD) fail(EQG_ERR_ARG, "unknown reduction");
         if (a->n == 0 && (op == EQG_MIN || op == EQG_MAX)) fail(EQG_ERR_ARG, "min/maxReduce of an empty collection");
-        *out = k_reduce(*rt->core, op, a->val->as<double>(), a->n);
+        *out = k_reduce(*rt->core, op, coll_values(*rt->core, a), a->n);
     });
 }
 
@@ -1123,7 +1170,7 @@ int eqg_two_norm(eqg_runtime* rt, const eqg_coll* a, double* out)
     return guarded(__func__, [&] {
         need(rt, "runtime");
         need(a, "collection");
-        *out = k_two_norm(*rt->core, a->val->as<double>(), a->n);
+        *out = k_two_norm(*rt->core, coll_values(*rt->core, a), a->n);
     });
 }
 
@@ -1184,7 +1231,7 @@ int eqg_solve_for_update(eqg_runtime* rt, const eqg_coll* residual, eqg_coll** d
         if (!residual->pat) fail(EQG_ERR_ARG, "solveForUpdate: residual has no Jacobian");
         if (residual->pat->rows != residual->pat->cols) fail(EQG_ERR_ARG, "solveForUpdate: Jacobian is not square");
         Buf x = c.allocN<double>(residual->n > 0 ? residual->n : 1);
-        SolveResult r = linear_solve(c, residual->pat, residual->jval->as<double>(), residual->val->as<double>(),
+        SolveResult r = linear_solve(c, residual->pat, residual->jval->as<double>(), coll_values(c, residual),
                                      x->as<double>());
         c.solver.linear_solves++;
         c.solver.krylov_iterations += r.iterations;
@@ -1237,7 +1284,7 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
         if (evaluate(u.p, &tmp) != 0 || !tmp) fail(EQG_ERR_CALLBACK, "residual callback failed");
         res.reset(tmp);
         if (res.p->n != u.p->n) fail(EQG_ERR_ARG, "newtonSolve: residual and unknown differ in size");
-        double norm = k_two_norm(c, res.p->val->as<double>(), res.p->n);
+        double norm = k_two_norm(c, coll_values(c, res.p), res.p->n);
         int iter = 0;
         if (c.verbose > 1)
             std::printf("    newtonSolve: iter = %d (max = %d), norm(residual) = %g (tol = %g)\n", iter, c.max_iter,
@@ -1255,7 +1302,7 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
             tmp = nullptr;
             if (evaluate(u.p, &tmp) != 0 || !tmp) fail(EQG_ERR_CALLBACK, "residual callback failed");
             res.reset(tmp);
-            norm = k_two_norm(c, res.p->val->as<double>(), res.p->n);
+            norm = k_two_norm(c, coll_values(c, res.p), res.p->n);
             ++iter;
             c.newton_iterations++;
             if (c.verbose > 1)
@@ -1266,6 +1313,7 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
             if (norm > c.abs_res_tol) std::printf("Newton solver failed to converge in %d iterations\n", c.max_iter);
             else std::printf("Newton solver converged in %d iterations\n", iter);
         }
+        settle(c, u.p);
         *out = new_coll(rt->core, u.p->n, u.p->val);
         eqg_solve_info info{};
         info.start_mark = m0;

@@ -24,7 +24,11 @@
 #include <string>
 #include <tuple>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
+
+struct eqg_coll;
+struct eqg_mask;
 
 namespace eqg {
 
@@ -187,6 +191,12 @@ struct Core {
     };
     std::vector<TimedLaunch> timer_pairs;
     PhaseClock residual_clock, factor_clock, krylov_clock;
+    // deferred elementwise expressions: mode, handles with pending values,
+    // evaluation passes run
+    bool lazy = true;
+    std::unordered_set<eqg_coll*> lazy_colls;
+    std::unordered_set<eqg_mask*> lazy_masks;
+    int64_t lazy_passes = 0;
 
     Core();
     ~Core();
@@ -211,6 +221,49 @@ struct Core {
 };
 
 using CoreP = std::shared_ptr<Core>;
+
+// ---- deferred elementwise expressions (lazy.cu) -------------------------
+// Value-only elementwise operations (arithmetic, with a scalar, unary,
+// comparisons, trinaryIf, mask logic) and constant collections are recorded
+// as nodes of a DAG over materialized arrays instead of being launched.  The
+// first operation that needs values (any other operation, a reduction, a
+// host copy) evaluates every pending node of that length in one kernel pass
+// (one thread per element, shared subexpressions computed once), with the
+// same floating-point operations, in the same order, as the
+// one-kernel-per-operation path.  Runtime parameter lazy=1 turns it on (off
+// by default: with its intermediates in shared memory an evaluation pass
+// costs about as much as the launches it replaces).
+enum LazyOp { LZ_LEAF, LZ_CONST, LZ_BIN, LZ_BINS, LZ_UNARY, LZ_CMP, LZ_CMPS, LZ_SEL, LZ_LOGIC };
+
+struct LazyNode {
+    int op = LZ_LEAF;
+    int sub = 0;           // the operator of LZ_BIN/BINS/UNARY/CMP/CMPS/LOGIC
+    double s = 0.0;        // scalar operand (LZ_BINS, LZ_CMPS) or value (LZ_CONST)
+    int scalar_left = 0;
+    bool mask = false;     // a mask (uint8) rather than doubles
+    int64_t n = 0;
+    int cost = 1;          // nodes below (an upper bound; shared nodes counted twice)
+    std::shared_ptr<LazyNode> a, b, c;
+    Buf leaf;              // LZ_LEAF: the values
+};
+using LazyP = std::shared_ptr<LazyNode>;
+
+// Values of a collection or mask, evaluating its pending expression first.
+const double* coll_values(Core& c, const eqg_coll* x);
+const uint8_t* mask_values(Core& c, const eqg_mask* m);
+void settle(Core& c, const eqg_coll* x);
+void settle(Core& c, const eqg_mask* m);
+// True when `x` may be an operand of a deferred operation (lazy mode, no
+// Jacobian).
+bool lazy_ok(const Core& c, const eqg_coll* x);
+LazyP lazy_node(const eqg_coll* x);
+LazyP lazy_node(const eqg_mask* m);
+LazyP lazy_make(int op, int sub, int64_t n, bool mask, LazyP a, LazyP b = nullptr, LazyP c = nullptr,
+                double s = 0.0, int scalar_left = 0);
+eqg_coll* lazy_coll(const CoreP& core, int64_t n, LazyP node);
+eqg_mask* lazy_mask(const CoreP& core, int64_t n, LazyP node);
+void lazy_forget(eqg_coll* x);
+void lazy_forget(eqg_mask* m);
 
 // Launches a kernel through `f`, checks the launch, and brackets it with
 // CUDA events on the runtime stream when `name` is the timed kernel.
@@ -339,16 +392,18 @@ struct eqg_mask {
     std::atomic<int> refs{1};
     eqg::CoreP core;
     int64_t n = 0;
-    eqg::Buf v;  // uint8[n]
+    eqg::Buf v;  // uint8[n]; null while `lazy` is pending
+    eqg::LazyP lazy;
 };
 
 struct eqg_coll {
     std::atomic<int> refs{1};
     eqg::CoreP core;
     int64_t n = 0;
-    eqg::Buf val;           // double[n]
+    eqg::Buf val;           // double[n]; null while `lazy` is pending
     eqg::PatternP pat;      // null: no Jacobian
     eqg::Buf jval;          // double[nnz]
+    eqg::LazyP lazy;        // deferred value-only expression
 };
 
 struct eqg_runtime {
