@@ -108,6 +108,9 @@ SIGNATURES = {
     "eqg_coll_constant": (C.c_int, [vp, C.c_double, C.c_int64, vpp]),
     "eqg_coll_size": (C.c_int, [vp, c_i64_p]),
     "eqg_coll_to_host": (C.c_int, [vp, c_dbl_p]),
+    "eqg_output_begin": (C.c_int, [vp, vp, c_i64_p]),
+    "eqg_output_wait": (C.c_int, [vp, C.c_int64, C.POINTER(c_dbl_p), c_i64_p]),
+    "eqg_output_release": (C.c_int, [vp, C.c_int64]),
     "eqg_coll_jacobian_info": (C.c_int, [vp, c_i64_p, c_i64_p, c_i64_p]),
     "eqg_coll_jacobian_to_host": (C.c_int, [vp, c_i64_p, c_i32_p, c_dbl_p]),
     "eqg_coll_retain": (None, [vp]),

@@ -810,6 +810,83 @@ int eqg_coll_size(const eqg_coll* c, int64_t* n)
     });
 }
 
+int eqg_output_begin(eqg_runtime* rt, const eqg_coll* x, int64_t* ticket)
+{
+    return guarded(__func__, [&] {
+        need(rt, "runtime");
+        need(x, "collection");
+        need(ticket, "ticket");
+        Core& c = *rt->core;
+        c.reap_outputs();
+        const double* v = coll_values(c, x);
+        Core::OutputCopy oc;
+        oc.values = x->val;
+        oc.n = x->n;
+        oc.bytes = (size_t)(x->n > 0 ? x->n : 1) * sizeof(double);
+        {
+            std::lock_guard<std::mutex> lock(c.output_mutex);
+            auto it = c.pinned_pool.lower_bound(oc.bytes);
+            if (it != c.pinned_pool.end() && it->first <= 2 * oc.bytes) {
+                oc.host = it->second;
+                oc.bytes = it->first;
+                c.pinned_pool.erase(it);
+            }
+        }
+        if (!oc.host) EQG_CUDA(cudaMallocHost(&oc.host, oc.bytes));
+        cudaEvent_t ready = nullptr;
+        EQG_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        EQG_CUDA(cudaEventRecord(ready, c.stream));
+        EQG_CUDA(cudaStreamWaitEvent(c.copy_stream, ready, 0));
+        cudaEventDestroy(ready);
+        if (x->n > 0)
+            EQG_CUDA(cudaMemcpyAsync(oc.host, v, (size_t)x->n * sizeof(double), cudaMemcpyDeviceToHost,
+                                     c.copy_stream));
+        EQG_CUDA(cudaEventCreateWithFlags(&oc.done, cudaEventDisableTiming));
+        EQG_CUDA(cudaEventRecord(oc.done, c.copy_stream));
+        std::lock_guard<std::mutex> lock(c.output_mutex);
+        *ticket = c.next_ticket++;
+        c.output_copies.emplace(*ticket, std::move(oc));
+    });
+}
+
+int eqg_output_wait(eqg_runtime* rt, int64_t ticket, const double** values, int64_t* n)
+{
+    return guarded(__func__, [&] {
+        need(rt, "runtime");
+        Core& c = *rt->core;
+        double* host = nullptr;
+        cudaEvent_t done = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(c.output_mutex);
+            auto it = c.output_copies.find(ticket);
+            if (it == c.output_copies.end()) fail(EQG_ERR_ARG, "unknown output ticket");
+            host = it->second.host;
+            done = it->second.done;
+            *n = it->second.n;
+        }
+        EQG_CUDA(cudaEventSynchronize(done));
+        *values = host;
+    });
+}
+
+int eqg_output_release(eqg_runtime* rt, int64_t ticket)
+{
+    return guarded(__func__, [&] {
+        need(rt, "runtime");
+        Core& c = *rt->core;
+        std::lock_guard<std::mutex> lock(c.output_mutex);
+        auto it = c.output_copies.find(ticket);
+        if (it == c.output_copies.end()) fail(EQG_ERR_ARG, "unknown output ticket");
+        Core::OutputCopy oc = std::move(it->second);
+        c.output_copies.erase(it);
+        cudaEventSynchronize(oc.done);
+        cudaEventDestroy(oc.done);
+        c.pinned_pool.emplace(oc.bytes, oc.host);
+        oc.host = nullptr;
+        c.output_released.push_back(std::move(oc));  // device buffer dropped by the runtime's thread
+    });
+}
+
 int eqg_coll_to_host(const eqg_coll* c, double* out)
 {
     return guarded(__func__, [&] {

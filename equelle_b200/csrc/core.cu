@@ -33,10 +33,38 @@ Core::Core()
     uint64_t threshold = UINT64_MAX;  // keep freed blocks cached in the pool
     EQG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
     EQG_CUDA(cudaMallocHost(&pinned, 64 * sizeof(double)));
+    EQG_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+}
+
+// Drops the device buffers of output copies that were released (possibly
+// by another thread); runs on the runtime's thread, the only one that may
+// touch the allocator.
+void Core::reap_outputs()
+{
+    std::vector<OutputCopy> done;
+    {
+        std::lock_guard<std::mutex> lock(output_mutex);
+        done.swap(output_released);
+    }
+    done.clear();
 }
 
 Core::~Core()
 {
+    // Finish and drop outstanding output copies, then the pinned pool.
+    {
+        std::lock_guard<std::mutex> lock(output_mutex);
+        for (auto& kv : output_copies) {
+            cudaEventSynchronize(kv.second.done);
+            cudaEventDestroy(kv.second.done);
+            cudaFreeHost(kv.second.host);
+        }
+        output_copies.clear();
+        for (auto& kv : pinned_pool) cudaFreeHost(kv.second);
+        pinned_pool.clear();
+    }
+    reap_outputs();
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     // Release cached device objects before the stream goes away.
     for (auto& kv : derived_sets) eqg_set_release(kv.second);
     derived_sets.clear();

@@ -197,6 +197,24 @@ struct Core {
     std::unordered_set<eqg_coll*> lazy_colls;
     std::unordered_set<eqg_mask*> lazy_masks;
     int64_t lazy_passes = 0;
+    // asynchronous output copies (eqg_output_*): device -> pinned host on
+    // their own stream.  The ticket table and the pinned pool are shared with
+    // the thread that waits for copies (mutex); device buffers of finished
+    // copies are dropped on the runtime's own thread (reap_outputs).
+    struct OutputCopy {
+        Buf values;              // kept alive until the copy has finished
+        double* host = nullptr;  // pinned
+        size_t bytes = 0;
+        int64_t n = 0;
+        cudaEvent_t done = nullptr;
+    };
+    cudaStream_t copy_stream = nullptr;
+    std::mutex output_mutex;
+    std::map<int64_t, OutputCopy> output_copies;
+    std::vector<OutputCopy> output_released;
+    std::multimap<size_t, double*> pinned_pool;
+    int64_t next_ticket = 1;
+    void reap_outputs();
 
     Core();
     ~Core();

@@ -210,6 +210,15 @@ int eqg_coll_from_host(eqg_runtime* rt, const double* v, int64_t n, eqg_coll** o
 int eqg_coll_constant(eqg_runtime* rt, double v, int64_t n, eqg_coll** out);
 int eqg_coll_size(const eqg_coll* c, int64_t* n);
 int eqg_coll_to_host(const eqg_coll* c, double* out);
+/* Asynchronous output (the copies behind EquelleRuntimeCPU::output,
+ * EquelleRuntimeCPU_impl.hpp:342-365): eqg_output_begin starts copying the
+ * values to library-owned host memory after the work already enqueued and
+ * returns at once with a ticket; eqg_output_wait blocks until that copy is
+ * done and gives its values, valid until eqg_output_release.  Wait and
+ * release may be called from another thread than the runtime's. */
+int eqg_output_begin(eqg_runtime* rt, const eqg_coll* c, int64_t* ticket);
+int eqg_output_wait(eqg_runtime* rt, int64_t ticket, const double** values, int64_t* n);
+int eqg_output_release(eqg_runtime* rt, int64_t ticket);
 /* nnz = -1 when the collection carries no Jacobian (an ADB constant). */
 int eqg_coll_jacobian_info(const eqg_coll* c, int64_t* rows, int64_t* cols, int64_t* nnz);
 /* CSR with ascending column indices; explicit zeros of the symbolic

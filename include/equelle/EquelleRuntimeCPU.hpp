@@ -16,14 +16,18 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
 #include <exception>
 #include <fstream>
 #include <iomanip>
 #include <iostream>
 #include <iterator>
 #include <map>
+#include <mutex>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <utility>
 #include <vector>
@@ -92,6 +96,10 @@ public:
     EquelleRuntimeCPU& operator=(const EquelleRuntimeCPU&) = delete;
     ~EquelleRuntimeCPU()
     {
+        drainOutputs();
+        if (!out_error_.empty()) {
+            std::cerr << out_error_ << std::endl;
+        }
         writeLastOutputs();
         eqg_runtime_destroy(rt_);
     }
@@ -276,20 +284,31 @@ public:
             std::cout << tag << " = " << val << std::endl;
         }
     }
+    /// The copy to the host runs on the device while the program goes on:
+    /// a writer thread waits for it and writes the file, in call order (at
+    /// most kPendingOutputs copies in flight); printed output waits for its
+    /// copy, to keep its place among the program's other prints.
     /// Extensions for timing runs: output_values=none still copies each
     /// collection to the host but neither prints nor writes it;
     /// output_values=off does not copy it; output_values=last keeps the last
     /// collection of each tag and writes <output_dir><tag>-last.output
     /// (precision 17) when the runtime ends.  Every call also records two
-    /// device clock marks, before and after the copy (outputMarks): for an
-    /// explicit program, whose time steps are the intervals between its
-    /// outputs.
+    /// device clock marks, before and after starting the copy
+    /// (outputMarks): for an explicit program, whose time steps are the
+    /// intervals between its outputs.
     void output(const String& tag, const CollOfScalar& vals)
     {
+        rethrowOutputError();
         int before = 0, after = 0;
         detail::check(eqg_runtime_mark(rt_, &before));
         if (!output_off_) {
-            writeOutput(tag, vals);
+            int64_t ticket = 0;
+            detail::check(eqg_output_begin(rt_, vals.handle(), &ticket));
+            if (output_values_ && !output_to_file_) {
+                writeTicket(tag, ticket);
+            } else {
+                enqueueOutput(tag, ticket);
+            }
         }
         detail::check(eqg_runtime_mark(rt_, &after));
         auto it = output_marks_.find(tag);
@@ -310,11 +329,81 @@ public:
     }
 
 private:
-    void writeOutput(const String& tag, const CollOfScalar& vals)
+    static constexpr size_t kPendingOutputs = 8;
+
+    void enqueueOutput(const String& tag, int64_t ticket)
     {
-        std::vector<double> v = vals.value();
+        std::unique_lock<std::mutex> lock(out_mutex_);
+        if (!writer_.joinable()) {
+            writer_ = std::thread([this] { writerLoop(); });
+        }
+        out_cv_.wait(lock, [this] { return out_queue_.size() < kPendingOutputs; });
+        out_queue_.emplace_back(tag, ticket);
+        out_cv_.notify_all();
+    }
+    void writerLoop()
+    {
+        for (;;) {
+            std::pair<String, int64_t> item;
+            {
+                std::unique_lock<std::mutex> lock(out_mutex_);
+                out_cv_.wait(lock, [this] { return !out_queue_.empty() || out_stop_; });
+                if (out_queue_.empty()) {
+                    return;
+                }
+                item = out_queue_.front();
+            }
+            try {
+                writeTicket(item.first, item.second);
+            } catch (const std::exception& e) {
+                std::lock_guard<std::mutex> lock(out_mutex_);
+                if (out_error_.empty()) {
+                    out_error_ = e.what();
+                }
+            }
+            {
+                std::lock_guard<std::mutex> lock(out_mutex_);
+                out_queue_.pop_front();
+            }
+            out_cv_.notify_all();
+        }
+    }
+    void drainOutputs()
+    {
+        {
+            std::lock_guard<std::mutex> lock(out_mutex_);
+            out_stop_ = true;
+        }
+        out_cv_.notify_all();
+        if (writer_.joinable()) {
+            writer_.join();
+        }
+    }
+    void rethrowOutputError()
+    {
+        std::lock_guard<std::mutex> lock(out_mutex_);
+        if (!out_error_.empty()) {
+            const std::string e = out_error_;
+            out_error_.clear();
+            throw std::runtime_error(e);
+        }
+    }
+    void writeTicket(const String& tag, int64_t ticket)
+    {
+        struct Release {
+            eqg_runtime* rt;
+            int64_t ticket;
+            ~Release() { eqg_output_release(rt, ticket); }
+        } release{rt_, ticket};
+        const double* v = nullptr;
+        int64_t n = 0;
+        detail::check(eqg_output_wait(rt_, ticket, &v, &n));
+        writeValues(tag, v, v + n);
+    }
+    void writeValues(const String& tag, const double* first, const double* last)
+    {
         if (output_last_) {
-            last_output_[tag] = std::move(v);
+            last_output_[tag].assign(first, last);
             return;
         }
         if (!output_values_) {
@@ -335,11 +424,11 @@ private:
                 throw std::runtime_error("Failed to open " + fname.str());
             }
             file.precision(16);
-            std::copy(v.begin(), v.end(), std::ostream_iterator<double>(file, "\n"));
+            std::copy(first, last, std::ostream_iterator<double>(file, "\n"));
         } else {
             std::cout << tag << " =\n";
-            for (size_t i = 0; i < v.size(); ++i) {
-                std::cout << std::setw(15) << std::left << v[i] << " ";
+            for (const double* p = first; p != last; ++p) {
+                std::cout << std::setw(15) << std::left << *p << " ";
             }
             std::cout << std::endl;
         }
@@ -572,6 +661,13 @@ private:
     eqg_runtime* rt_ = nullptr;
     eqg_grid_info info_{};
     std::map<std::string, int> outputcount_;
+    // asynchronous outputs: queue of (tag, copy ticket) and its writer
+    std::mutex out_mutex_;
+    std::condition_variable out_cv_;
+    std::deque<std::pair<std::string, int64_t>> out_queue_;
+    std::thread writer_;
+    bool out_stop_ = false;
+    std::string out_error_;
 };
 
 }  // namespace equelle

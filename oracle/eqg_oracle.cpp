@@ -46,6 +46,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -675,6 +676,10 @@ struct eqg_runtime {
     std::vector<std::chrono::steady_clock::time_point> marks;
     std::vector<eqg_solve_info> solves;
     eqg_stats stats{};
+    // output copies (eqg_output_*), made at once; shared with a waiting thread
+    std::mutex output_mutex;
+    std::map<int64_t, std::vector<double>> outputs;
+    int64_t next_ticket = 1;
 };
 
 struct eqg_set {
@@ -1130,6 +1135,38 @@ int eqg_coll_to_host(const eqg_coll* c, double* out)
     return guarded([&] {
         need(c, "collection");
         std::copy(c->a.v.begin(), c->a.v.end(), out);
+    });
+}
+
+int eqg_output_begin(eqg_runtime* rt, const eqg_coll* c, int64_t* ticket)
+{
+    return guarded([&] {
+        need(rt, "runtime");
+        need(c, "collection");
+        std::lock_guard<std::mutex> lock(rt->output_mutex);
+        *ticket = rt->next_ticket++;
+        rt->outputs[*ticket] = c->a.v;
+    });
+}
+
+int eqg_output_wait(eqg_runtime* rt, int64_t ticket, const double** values, int64_t* n)
+{
+    return guarded([&] {
+        need(rt, "runtime");
+        std::lock_guard<std::mutex> lock(rt->output_mutex);
+        auto it = rt->outputs.find(ticket);
+        if (it == rt->outputs.end()) fail(EQG_ERR_ARG, "unknown output ticket");
+        *values = it->second.data();
+        *n = (int64_t)it->second.size();
+    });
+}
+
+int eqg_output_release(eqg_runtime* rt, int64_t ticket)
+{
+    return guarded([&] {
+        need(rt, "runtime");
+        std::lock_guard<std::mutex> lock(rt->output_mutex);
+        if (!rt->outputs.erase(ticket)) fail(EQG_ERR_ARG, "unknown output ticket");
     });
 }
 
