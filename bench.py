@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--ny", type=int)
     ap.add_argument("--nz", type=int)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="two-phase: skip the mixed and refine runs that the line compares with FP64")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--extra", action="append", default=[],
                     help="extra key=value runtime parameter (repeatable)")
@@ -328,6 +330,30 @@ def main():
         "roofline": roofline,
         "clocks": clk.summary(),
     }
+
+    # the reduced-precision forms of the same workload against this FP64 run:
+    # throughput, and the saturation field after the last step relative to
+    # the FP64 run's (both written with precision 17)
+    if name == "twophase" and a.precision == "double" and not a.no_forms:
+        def last_sw(rdir, precision):
+            args4 = write(d, W + K) + tol + ["output_values=last", "output_dir=%s/" % rdir, "device=%d" % local_rank,
+                                             "linsolver_precision=" + precision, "linsolver_ordering=" + a.ordering]
+            os.makedirs(rdir, exist_ok=True)
+            r = simrun.run(name, args4 + a.extra)
+            import numpy as np
+            return r, np.loadtxt(os.path.join(rdir, "saturation-last.output"))
+
+        base_dir = os.path.join(tempfile.gettempdir(), "eqg_bench", "forms_r%d" % rank)
+        _, sw64 = last_sw(os.path.join(base_dir, "double"), "double")
+        forms = {}
+        for form in ("mixed", "refine"):
+            r, sw = last_sw(os.path.join(base_dir, form), form)
+            ms_f = timed_window(r, W, K)
+            forms[form] = {"value": world * K / (ms_f / 1000.0), "ms_per_step": ms_f / K,
+                           "speedup_vs_fp64": ms / ms_f,
+                           "krylov_iterations_per_step": window_counts(r, W, K)["krylov"] / K,
+                           "sw_max_rel_err_vs_fp64": float(abs(sw - sw64).max() / abs(sw64).max())}
+        line["precision_forms"] = forms
 
     # end to end through the public entry point: host input files in, host
     # outputs out every step, host wall clock
