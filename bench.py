@@ -215,29 +215,22 @@ def cpu_sample(name, args, sample_krylov, per_step):
 # ---------------------------------------------------------------------------
 def main():
     a = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    dist = None
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    from equelle_b200.replicas import Replicas
+    # the reference arm runs on rank 0's host cores alone: no group
+    rp = Replicas("nccl", group=a.impl != "reference")
+    rank, local_rank, world = rp.rank, rp.local_rank, rp.world
 
     if a.workload in ("batched", "serve"):
-        return main_many(a, rank, world, dist)
+        return main_many(a, rp)
     name, key, desc, cells, write, tol = workload(a)
     W, K = a.warmup, a.steps
     if name == "swe":
-        return main_explicit(a, rank, local_rank, world, dist, name, key, desc, cells, write)
+        return main_explicit(a, rp, name, key, desc, cells, write)
     metric = "Newton-steps/s"
     unit = "steps/s"
 
     if a.impl == "reference":
         if rank != 0:
-            if dist:
-                dist.destroy_process_group()
             return
         d = input_dir(key, 1, rank)
         args = write(d, 1) + tol + ["output_values=none"]
@@ -270,20 +263,14 @@ def main():
     args += a.extra
     if a.kernel_profile:
         args.append("time_kernel=*")
-    if dist:
-        dist.barrier()
+    rp.barrier()
     with ClockSampler(local_rank) as clk:
         rep = simrun.run(name, args)
     if rep.solves < W + K:
         raise SystemExit("simulator ran %d solves, expected %d" % (rep.solves, W + K))
-    ms = timed_window(rep, W, K)
+    ms = rp.max(timed_window(rep, W, K))
     infos = window_counts(rep, W, K)
-    if dist:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * K / (ms / 1000.0)
+    value = rp.throughput(K, ms)
     st = rep.stats
     n_rows, nnz = st.last_matrix_rows, st.last_matrix_nnz
     bsz, nblk = max(st.last_block_size, 1), st.last_matrix_blocks or st.last_matrix_nnz
@@ -348,7 +335,7 @@ def main():
         forms = {}
         for form in ("mixed", "refine"):
             r, sw = last_sw(os.path.join(base_dir, form), form)
-            ms_f = timed_window(r, W, K)
+            ms_f = rp.max(timed_window(r, W, K))
             forms[form] = {"value": world * K / (ms_f / 1000.0), "ms_per_step": ms_f / K,
                            "speedup_vs_fp64": ms / ms_f,
                            "krylov_iterations_per_step": window_counts(r, W, K)["krylov"] / K,
@@ -361,14 +348,10 @@ def main():
         d2 = input_dir(key, K, rank)
         args2 = write(d2, K) + tol + ["output_values=none", "device=%d" % local_rank,
                                       "linsolver_precision=" + a.precision, "linsolver_ordering=" + a.ordering]
+        rp.barrier()
         t0 = time.perf_counter()
         rep2 = simrun.run(name, args2)
-        wall = time.perf_counter() - t0
-        if dist:
-            import torch
-            t = torch.tensor([wall], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
+        wall = rp.max(time.perf_counter() - t0)
         nfields = 2 if name == "twophase" else 1
         line["e2e"] = {"value": world * K / wall, "unit": unit,
                        "h2d_bytes_per_step": dir_bytes(d2) / K,
@@ -387,9 +370,7 @@ def main():
                                   for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
     if rank == 0:
         print(json.dumps(line))
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    rp.close()
 
 
 def config(a, desc, cells):
@@ -398,7 +379,7 @@ def config(a, desc, cells):
             "l2": "working set larger than L2 (126 MB), no flush", "parallelism": "replicas"}
 
 
-def main_many(a, rank, world, dist):
+def main_many(a, rp):
     """Many independent instances on the GPU (equelle_b200/serve.py):
     `batched` runs a seeded set of 2D two-phase instances all at once;
     `serve` feeds requests (heat or 2D two-phase) at Poisson arrival rates.
@@ -408,21 +389,19 @@ def main_many(a, rank, world, dist):
     from equelle_b200 import serve
     import equelle_b200
     equelle_b200.load_library()
+    rank, world = rp.rank, rp.world
     root = os.path.join(tempfile.gettempdir(), "eqg_bench", "%s_r%d" % (a.workload, rank))
     if a.impl == "reference":
         if rank == 0:
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or serving mode; "
                               "its arm for these workloads is the one-at-a-time FP64 line of our bench"}))
-        if dist:
-            dist.destroy_process_group()
         return
-    if dist:
-        dist.barrier()
+    rp.barrier()
 
     def prepared(reqs, precision):
         for r in reqs:
             serve.prepare(r, os.path.join(root, "%s_%d_%d_%d" % (r.program, r.nx, r.steps, r.seed)),
-                          ["linsolver_precision=" + precision, "device=%d" % int(os.environ.get("LOCAL_RANK", "0"))]
+                          ["linsolver_precision=" + precision, "device=%d" % rp.local_rank]
                           + a.extra)
         return reqs
 
@@ -437,9 +416,9 @@ def main_many(a, rank, world, dist):
     if a.workload == "batched":
         reqs = serve.make_requests(a.instances, seed=1, programs=("twophase",), side=(32, 512), steps=(a.steps, a.steps))
         seq = summary(*serve.Server(slots=1).run(prepared(reqs, "double"), realtime=False))
-        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        with ClockSampler(rp.local_rank) as clk:
             bat = summary(*serve.Server(slots=a.slots).run(prepared(reqs, "mixed"), realtime=False))
-        value = world * bat["instance_steps_per_s"]
+        value = rp.throughput(bat["instance_steps"], 1000.0 * rp.max(bat["wall_s"]))
         line = {"metric": "instance-steps/s", "value": value, "unit": "instance-steps/s", "n_gpus": world,
                 "steps": a.steps, "warmup": 0, "ms_per_step": 1000.0 * bat["wall_s"] / bat["instance_steps"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
@@ -461,7 +440,8 @@ def main_many(a, rank, world, dist):
             recs, wall = serve.Server(slots=a.slots).run(prepared(reqs, "mixed"), realtime=True)
             per_rate["%g" % lam] = summary(recs, wall)
         top = per_rate["%g" % rates[-1]]
-        line = {"metric": "requests/s", "value": world * top["requests_per_s"], "unit": "requests/s",
+        line = {"metric": "requests/s", "value": rp.throughput(top["requests"], 1000.0 * rp.max(top["wall_s"])),
+                "unit": "requests/s",
                 "n_gpus": world, "steps": a.requests, "warmup": 0, "ms_per_step": 1000.0 / top["requests_per_s"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
                 "data": "synthetic (seeded requests: heat or 2D two-phase, sides log-uniform in [64, 512], "
@@ -473,9 +453,7 @@ def main_many(a, rank, world, dist):
                 "throughput_vs_one_at_a_time": top["requests_per_s"] / seq["requests_per_s"]}
     if rank == 0:
         print(json.dumps(line))
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    rp.close()
 
 
 # Bytes one time step of the shallow-water case must move at least (two
@@ -485,11 +463,12 @@ def main_many(a, rank, world, dist):
 SWE_BYTES_PER_CELL = 112
 
 
-def main_explicit(a, rank, local_rank, world, dist, name, key, desc, cells, write):
+def main_explicit(a, rp, name, key, desc, cells, write):
     """The explicit shallow-water workload: steps are the intervals between
     the program's outputs (device clock marks); the metric is cell updates
     per second."""
     from equelle_b200 import simrun
+    rank, local_rank, world = rp.rank, rp.local_rank, rp.world
     W, K = a.warmup, a.steps
     metric = unit = "cell-updates/s"
     oracle = os.path.join(ROOT, "oracle", "_build", "libsim_%s_oracle.so" % name)
@@ -513,8 +492,6 @@ def main_explicit(a, rank, local_rank, world, dist, name, key, desc, cells, writ
               "case on %dx%d cells, host clock between the program's outputs" % (sx, sy))
     if a.impl == "reference":
         if rank != 0:
-            if dist:
-                dist.destroy_process_group()
             return
         times = [cpu_step()[1] for _ in range(W + K)]
         ms_step = sum(times[W:]) / K
@@ -533,19 +510,13 @@ def main_explicit(a, rank, local_rank, world, dist, name, key, desc, cells, writ
     args = write(d, W + K) + ["output_values=off", "device=%d" % local_rank] + a.extra
     if a.kernel_profile:
         args.append("time_kernel=*")
-    if dist:
-        dist.barrier()
+    rp.barrier()
     with ClockSampler(local_rank) as clk:
         rep = simrun.run(name, args)
     if rep.solves < W + K:
         raise SystemExit("simulator ran %d steps, expected %d" % (rep.solves, W + K))
-    ms = timed_window(rep, W, K)
-    if dist:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * K * cells / (ms / 1000.0)
+    ms = rp.max(timed_window(rep, W, K))
+    value = rp.throughput(K * cells, ms)
     peak, peak_kind = peaks()
     step_s = ms / K / 1000.0
     achieved = SWE_BYTES_PER_CELL * cells / step_s / 1e9
@@ -567,14 +538,10 @@ def main_explicit(a, rank, local_rank, world, dist, name, key, desc, cells, writ
     if not a.no_e2e:
         d2 = input_dir(key, K, rank)
         args2 = write(d2, K) + ["output_values=none", "device=%d" % local_rank]
+        rp.barrier()
         t0 = time.perf_counter()
         rep2 = simrun.run(name, args2)
-        wall = time.perf_counter() - t0
-        if dist:
-            import torch
-            t = torch.tensor([wall], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
+        wall = rp.max(time.perf_counter() - t0)
         inbytes = sum(os.path.getsize(os.path.join(d2, f)) for f in os.listdir(d2) if f.endswith(".f64"))
         line["e2e"] = {"value": world * K * cells / wall, "unit": unit, "h2d_bytes_per_step": inbytes / K,
                        "d2h_bytes_per_step": 3 * 8 * cells * (K + 1) / K,
@@ -591,9 +558,7 @@ def main_explicit(a, rank, local_rank, world, dist, name, key, desc, cells, writ
                                   for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])[:20]}
     if rank == 0:
         print(json.dumps(line))
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    rp.close()
 
 
 def window_counts(rep, w, k):
