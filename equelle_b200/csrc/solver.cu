@@ -148,13 +148,27 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NV], double* partials, unsi
 // position k are one contiguous segment.  Within a row, blocks are in
 // ascending column order, so the ILU(0) lower part is k < dk[R] and the
 // upper part k > dk[R].  Vectors are in block-row order: unknown c of block
-// row R is at R B + c.
+// row R is at R B + c.  A level whose slices all have the same width (the
+// small levels of the fused coarse cycle) also records that width: there the
+// slot of (R, k) is known without a load, and the kernels read a row's
+// columns and values in the same round trip as its length and diagonal
+// position.  Padding slots hold a valid column (the row itself) and zero
+// values.
 struct SellView {
     const int* __restrict__ slice_ptr;  // first slot of each slice
     const int* __restrict__ col;        // block column of each slot
     const int* __restrict__ len;        // blocks of each block row
     const int* __restrict__ dk;         // position of the diagonal block in each row
+    int width;                          // slots per row of every slice (0: slices differ)
 };
+
+// First slot of the slice of block row R; with U the level's slices all have
+// m.width slots per row.
+template <bool U>
+__device__ __forceinline__ int slice_base(const SellView& m, int R)
+{
+    return U ? (R >> 5) * (m.width << 5) : m.slice_ptr[R >> 5];
+}
 
 // Block J of a vector.  With CG the loads bypass L1 (ld.global.cg): for
 // vectors that other thread blocks of the same kernel wrote.
@@ -212,7 +226,11 @@ __device__ __forceinline__ void load_block(const M* __restrict__ p, M (&v)[BB])
 // from `x2` otherwise.  With KM > 0 (rows of at most KM blocks) the loop is
 // unrolled so that a thread issues its column loads before the dependent
 // gathers of x: the kernels using it are bound by the latency of that chain.
-template <int B, int KM, class T, class M, bool CG = false>
+//
+// With U (slices of uniform width) the column and value loads cover every
+// slot k < m.width, so they do not wait for k0 and k1 (the row's diagonal
+// position or length); only the sums skip the slots outside [k0, k1).
+template <int B, int KM, class T, class M, bool CG = false, bool U = false>
 __device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int k0, int k1, const M* __restrict__ a,
                                      const T* __restrict__ x, const T* __restrict__ x2, int split, double (&acc)[B])
 {
@@ -237,12 +255,12 @@ __device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int
         M av[KM][BB];
 #pragma unroll
         for (int k = 0; k < KM; ++k) {
-            const bool on = k >= k0 && k < k1;
+            const bool ld = U ? k < m.width : (k >= k0 && k < k1);
             const int q = sbase + (k << 5);
-            ci[k] = on ? m.col[q + lane] : 0;
+            ci[k] = ld ? m.col[q + lane] : 0;
 #pragma unroll
             for (int e = 0; e < BB; ++e) av[k][e] = (M)0;
-            if (on) load_block<BB, M>(a + (size_t)(q + lane) * BB, av[k]);
+            if (ld) load_block<BB, M>(a + (size_t)(q + lane) * BB, av[k]);
         }
 #pragma unroll
         for (int k = 0; k < KM; ++k) {
@@ -258,7 +276,8 @@ __device__ __forceinline__ void bdot(const SellView& m, int sbase, int lane, int
     } else {
         int ci[KM];
 #pragma unroll
-        for (int k = 0; k < KM; ++k) ci[k] = (k >= k0 && k < k1) ? m.col[sbase + (k << 5) + lane] : 0;
+        for (int k = 0; k < KM; ++k)
+            ci[k] = (U ? k < m.width : (k >= k0 && k < k1)) ? m.col[sbase + (k << 5) + lane] : 0;
 #pragma unroll
         for (int k = 0; k < KM; ++k) {
             if (k >= k0 && k < k1) {
@@ -486,17 +505,17 @@ __device__ __forceinline__ void update_z(T* __restrict__ zadd, int R, const doub
 // with y_K = b_K for rows of the first stage (K < r_first) and out_K
 // otherwise.  The last stage has no upper part: there the row is finished,
 // out_R = D_R^{-1} y_R (and zadd_R += out_R when zadd is given).
-template <int B, int KM, class T, class M, bool CG>
+template <int B, int KM, class T, class M, bool CG, bool U = false>
 __device__ __forceinline__ void lower_rows(int r0, int r1, int r_first, int last, const SellView& m,
                                            const M* __restrict__ lu, const T* __restrict__ b, T* __restrict__ out,
                                            T* __restrict__ zadd, int tid, int nth)
 {
     for (int R = r0 + tid; R < r1; R += nth) {
-        const int lane = R & 31, sb = m.slice_ptr[R >> 5], d = m.dk[R];
+        const int lane = R & 31, sb = slice_base<U>(m, R), d = m.dk[R];
         double acc[B];
 #pragma unroll
         for (int c = 0; c < B; ++c) acc[c] = 0.0;
-        bdot<B, KM, T, M, CG>(m, sb, lane, 0, d, lu, b, out, r_first, acc);
+        bdot<B, KM, T, M, CG, U>(m, sb, lane, 0, d, lu, b, out, r_first, acc);
         double y[B];
         load_bvec<B, T, CG>(b, R, y);
 #pragma unroll
@@ -518,17 +537,17 @@ __device__ __forceinline__ void lower_rows(int r0, int r1, int r_first, int last
 //   out_R = D_R^{-1} (y_R - sum_{k > dk} U_Rk out_K),
 // with y_R = b_R in the first stage and the forward-sweep value out_R
 // otherwise; zadd_R += out_R when zadd is given.
-template <int B, int KM, class T, class M, bool CG>
+template <int B, int KM, class T, class M, bool CG, bool U = false>
 __device__ __forceinline__ void upper_rows(int r0, int r1, int first, const SellView& m, const M* __restrict__ lu,
                                            const T* __restrict__ b, T* __restrict__ out, T* __restrict__ zadd,
                                            int tid, int nth)
 {
     for (int R = r0 + tid; R < r1; R += nth) {
-        const int lane = R & 31, sb = m.slice_ptr[R >> 5], d = m.dk[R];
+        const int lane = R & 31, sb = slice_base<U>(m, R), d = m.dk[R];
         double acc[B];
 #pragma unroll
         for (int c = 0; c < B; ++c) acc[c] = 0.0;
-        bdot<B, KM, T, M, CG>(m, sb, lane, d + 1, m.len[R], lu, out, out, INT_MAX, acc);
+        bdot<B, KM, T, M, CG, U>(m, sb, lane, d + 1, m.len[R], lu, out, out, INT_MAX, acc);
         double y[B];
         load_bvec<B, T, CG>(first ? b : out, R, y);
 #pragma unroll
@@ -544,7 +563,7 @@ __device__ __forceinline__ void upper_rows(int r0, int r1, int first, const Sell
 
 // out = b - A x.  Block rows below r_zero get 0 without being computed:
 // after a full ILU(0) sweep their residual is zero (see vcycle).
-template <int B, int KM, class T, class M, bool CG>
+template <int B, int KM, class T, class M, bool CG, bool U = false>
 __device__ __forceinline__ void residual_rows(int nb, int r_zero, const SellView& m, const M* __restrict__ a,
                                               const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ out,
                                               int tid, int nth)
@@ -558,7 +577,7 @@ __device__ __forceinline__ void residual_rows(int nb, int r_zero, const SellView
         double acc[B];
 #pragma unroll
         for (int c = 0; c < B; ++c) acc[c] = 0.0;
-        bdot<B, KM, T, M, CG>(m, m.slice_ptr[R >> 5], R & 31, 0, m.len[R], a, x, x, INT_MAX, acc);
+        bdot<B, KM, T, M, CG, U>(m, slice_base<U>(m, R), R & 31, 0, m.len[R], a, x, x, INT_MAX, acc);
         double y[B];
         load_bvec<B, T, CG>(b, R, y);
 #pragma unroll
@@ -567,15 +586,54 @@ __device__ __forceinline__ void residual_rows(int nb, int r_zero, const SellView
     }
 }
 
-// rc[P] = sum of t over the members of aggregate P
+// rc[P] = sum of t over the members of aggregate P, in member order.  An
+// aggregate of at most kMembers members (2 x 2 x 2 cells) issues all its
+// index loads, then all its gathers, before the sum: the step is bound by the
+// latency of that chain, not by its bytes.
+constexpr int kMembers = 8;
+
 template <class T, bool CG>
 __device__ __forceinline__ void restrict_rows(int nc, const int* __restrict__ mptr, const int* __restrict__ midx,
                                               const T* __restrict__ t, T* __restrict__ rc, int tid, int nth)
 {
     for (int P = tid; P < nc; P += nth) {
         double s = 0.0;
-        const int k1 = mptr[P + 1];
-        for (int k = mptr[P]; k < k1; ++k) s += (double)(CG ? __ldcg(t + midx[k]) : t[midx[k]]);
+        const int k0 = mptr[P], k1 = mptr[P + 1];
+        if (k1 - k0 <= kMembers) {
+            int mi[kMembers];
+#pragma unroll
+            for (int j = 0; j < kMembers; ++j) mi[j] = k0 + j < k1 ? midx[k0 + j] : 0;
+            double tv[kMembers];
+#pragma unroll
+            for (int j = 0; j < kMembers; ++j)
+                tv[j] = k0 + j < k1 ? (double)(CG ? __ldcg(t + mi[j]) : t[mi[j]]) : 0.0;
+#pragma unroll
+            for (int j = 0; j < kMembers; ++j)
+                if (k0 + j < k1) s += tv[j];
+        } else {
+            for (int k = k0; k < k1; ++k) s += (double)(CG ? __ldcg(t + midx[k]) : t[midx[k]]);
+        }
+        rc[P] = (T)s;
+    }
+}
+
+// restrict_rows with the members of each aggregate at P kMembers + j
+// (-1 past the last): the member loads need no offsets first.  Same sums.
+template <class T, bool CG>
+__device__ __forceinline__ void restrict_padded_rows(int nc, const int* __restrict__ mpad, const T* __restrict__ t,
+                                                     T* __restrict__ rc, int tid, int nth)
+{
+    for (int P = tid; P < nc; P += nth) {
+        int mi[kMembers];
+#pragma unroll
+        for (int j = 0; j < kMembers; ++j) mi[j] = mpad[P * kMembers + j];
+        double tv[kMembers];
+#pragma unroll
+        for (int j = 0; j < kMembers; ++j) tv[j] = mi[j] >= 0 ? (double)(CG ? __ldcg(t + mi[j]) : t[mi[j]]) : 0.0;
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < kMembers; ++j)
+            if (mi[j] >= 0) s += tv[j];
         rc[P] = (T)s;
     }
 }
@@ -592,15 +650,21 @@ __device__ __forceinline__ void prolong_rows(int nb, const int* __restrict__ agg
     }
 }
 
-// z = inv r with the dense inverse of the coarsest level
+// z = inv r with the dense inverse of the coarsest level: one warp per row,
+// lane l summing columns l, l + 32, ... in order, then a butterfly over the
+// warp (every lane ends with the same sum).  tid and nth are multiples of 32
+// apart from the lane, so every lane of a warp takes the same rows.
 template <class T, class M, bool CG>
 __device__ __forceinline__ void dense_rows(int n, const M* __restrict__ inv, const T* __restrict__ r,
                                            T* __restrict__ z, int tid, int nth)
 {
-    for (int i = tid; i < n; i += nth) {
+    const int lane = tid & 31;
+    for (int i = tid >> 5; i < n; i += nth >> 5) {
         double s = 0.0;
-        for (int j = 0; j < n; ++j) s += (double)inv[i * n + j] * (double)(CG ? __ldcg(r + j) : r[j]);
-        z[i] = (T)s;
+        for (int j = lane; j < n; j += 32) s += (double)inv[i * n + j] * (double)(CG ? __ldcg(r + j) : r[j]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) z[i] = (T)s;
     }
 }
 
@@ -1007,18 +1071,39 @@ struct PrefetchRegion {
     unsigned long long bytes;
 };
 
+// Stages of a level the fused cycle takes (their bounds are kernel
+// parameters).
+constexpr int kTailStages = 8;
+
+// Offsets (bytes) of a level's arrays in the shared memory of block 0, for
+// the levels at the coarse end that the fused cycle keeps there.
+struct TailLocal {
+    int a, lu, inv, col, len, dk, aggb, mpad, r, z, t, w;
+};
+
+// One device array copied into block 0's shared memory when the kernel starts.
+struct TailCopy {
+    const void* src;  // 16-byte aligned
+    int dst;          // shared memory offset, 16-byte aligned
+    int bytes;        // a multiple of 4
+};
+constexpr int kMaxCopies = 32;
+// Shared memory of the levels kept there (block 0; every block of the
+// cluster is launched with the same size).
+constexpr int kTailSmem = 200 * 1024;
+
 template <class T, class M>
 struct TailLevel {
     int nb = 0, n = 0, coarsest = 0;
-    SellView m{};
+    TailLocal so{};              // shared memory layout (levels >= local_first)
+    SellView m{};                // slices of uniform width m.width
     const M* a = nullptr;
     const M* lu = nullptr;
     const M* inv = nullptr;      // coarsest level
-    const int* stage_ptr = nullptr;
     int nstages = 0;
+    int sp[kTailStages + 1] = {};  // stage bounds
     const int* aggb = nullptr;   // to the next coarser level
-    const int* mptr = nullptr;
-    const int* midx = nullptr;
+    const int* mpad = nullptr;   // aggregate members, kMembers per coarse unknown
     T *r = nullptr, *z = nullptr, *t = nullptr, *w = nullptr;
 };
 
@@ -1026,8 +1111,12 @@ template <class T, class M>
 struct TailParams {
     TailLevel<T, M> lv[kMaxTail];
     int nlev = 0;
+    int local_first = kMaxTail;  // first level kept in block 0's shared memory (>= 1; nlev: none)
     int nregions = 0;
+    int ncopies = 0;
     PrefetchRegion reg[kMaxPrefetch];
+    TailCopy copies[kMaxCopies];
+    long long* trace = nullptr;  // SM clock after each step (linsolver_tail_trace)
 };
 
 // Thread blocks split every region into 16-byte aligned chunks and hand them
@@ -1051,23 +1140,147 @@ __device__ __forceinline__ void cluster_barrier()
     asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
 }
 
+// Entries of the step trace: the start, then one per step.
+constexpr int kTraceMax = 128;
+
+// Ends one step of the fused cycle: a cluster barrier, after which thread 0
+// of block 0 records the SM clock when a trace buffer is given.
+__device__ __forceinline__ void tail_step(long long* trace, int& k)
+{
+    cluster_barrier();
+    if (trace != nullptr && blockIdx.x == 0 && threadIdx.x == 0 && k < kTraceMax) trace[k] = clock64();
+    ++k;
+}
+
 // out = M^{-1} b on one level (zadd += out when given), stage by stage.
 template <int B, int KM, class T, class M>
-__device__ __forceinline__ void tail_ilu(const TailLevel<T, M>& L, const T* b, T* out, T* zadd, int tid, int nth)
+__device__ __forceinline__ void tail_ilu(const TailLevel<T, M>& L, const T* b, T* out, T* zadd, int tid, int nth,
+                                         long long* trace, int& tk)
 {
+    constexpr bool U = KM > 0;
     const int ns = L.nstages;
     if (ns <= 0) return;
-    const int r_first = L.stage_ptr[1];
+    const int r_first = L.sp[1];
     for (int s = 1; s < ns; ++s) {
         const int last = s == ns - 1;
-        lower_rows<B, KM, T, M, true>(L.stage_ptr[s], L.stage_ptr[s + 1], r_first, last, L.m, L.lu, b, out,
-                                   last ? zadd : nullptr, tid, nth);
-        cluster_barrier();
+        lower_rows<B, KM, T, M, true, U>(L.sp[s], L.sp[s + 1], r_first, last, L.m, L.lu, b, out,
+                                         last ? zadd : nullptr, tid, nth);
+        tail_step(trace, tk);
     }
     for (int s = ns >= 2 ? ns - 2 : 0; s >= 0; --s) {
-        upper_rows<B, KM, T, M, true>(L.stage_ptr[s], L.stage_ptr[s + 1], s == 0, L.m, L.lu, b, out, zadd, tid, nth);
-        cluster_barrier();
+        upper_rows<B, KM, T, M, true, U>(L.sp[s], L.sp[s + 1], s == 0, L.m, L.lu, b, out, zadd, tid, nth);
+        tail_step(trace, tk);
     }
+}
+
+static_assert(sizeof(TailParams<double, double>) <= 4096, "fused cycle parameters exceed 4 KB");
+
+// Block 0 starts the copies of the shared-memory levels' arrays (cp.async:
+// global to shared without registers; waited for with cp.async.wait_all,
+// which ends when this thread's copies have landed).
+__device__ __forceinline__ void start_local_copies(const TailCopy* cp, int ncopies, unsigned char* sm)
+{
+    for (int i = 0; i < ncopies; ++i) {
+        const char* src = (const char*)cp[i].src;
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(sm + cp[i].dst);
+        const int n16 = cp[i].bytes >> 4;
+        for (int j = threadIdx.x; j < n16; j += blockDim.x)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16 * j), "l"(src + 16 * j) : "memory");
+        for (int j = (n16 << 2) + threadIdx.x; j < (cp[i].bytes >> 2); j += blockDim.x)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst + 4 * j), "l"(src + 4 * j) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// A level's arrays in block 0's shared memory.
+template <class T, class M>
+struct LocalView {
+    SellView m;
+    const M *a, *lu, *inv;
+    const int *aggb, *mpad;
+    T *r, *z, *t, *w;
+};
+
+template <class T, class M>
+__device__ __forceinline__ LocalView<T, M> local_view(const TailLevel<T, M>& G, unsigned char* sm)
+{
+    const TailLocal& o = G.so;
+    LocalView<T, M> v;
+    v.m = SellView{nullptr, (const int*)(sm + o.col), (const int*)(sm + o.len), (const int*)(sm + o.dk), G.m.width};
+    v.a = (const M*)(sm + o.a);
+    v.lu = (const M*)(sm + o.lu);
+    v.inv = (const M*)(sm + o.inv);
+    v.aggb = (const int*)(sm + o.aggb);
+    v.mpad = (const int*)(sm + o.mpad);
+    v.r = (T*)(sm + o.r);
+    v.z = (T*)(sm + o.z);
+    v.t = (T*)(sm + o.t);
+    v.w = (T*)(sm + o.w);
+    return v;
+}
+
+// out = M^{-1} b on a shared-memory level, stage by stage (block barriers).
+template <int B, int KM, class T, class M>
+__device__ __forceinline__ void local_ilu(const TailLevel<T, M>& G, const LocalView<T, M>& V, const T* b, T* out,
+                                          T* zadd)
+{
+    const int tid = (int)threadIdx.x, nth = (int)blockDim.x;
+    const int ns = G.nstages;
+    if (ns <= 0) return;
+    for (int s = 1; s < ns; ++s) {
+        const int last = s == ns - 1;
+        lower_rows<B, KM, T, M, false, true>(G.sp[s], G.sp[s + 1], G.sp[1], last, V.m, V.lu, b, out,
+                                             last ? zadd : nullptr, tid, nth);
+        __syncthreads();
+    }
+    for (int s = ns >= 2 ? ns - 2 : 0; s >= 0; --s) {
+        upper_rows<B, KM, T, M, false, true>(G.sp[s], G.sp[s + 1], s == 0, V.m, V.lu, b, out, zadd, tid, nth);
+        __syncthreads();
+    }
+}
+
+// The coarse end of the cycle on block 0 alone, from level lf (whose right
+// side is restricted from the residual t of level lf - 1 in global memory)
+// down to the dense solve and back; the correction of level lf is written to
+// its global z.  Same steps and operations as the cluster-wide ones.
+template <int B, int KM, class T, class M>
+__device__ void local_cycle(const TailParams<T, M>& p, int lf, unsigned char* sm)
+{
+    const int tid = (int)threadIdx.x, nth = (int)blockDim.x;
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    {
+        const TailLevel<T, M>& F = p.lv[lf - 1];
+        restrict_padded_rows<T, true>(p.lv[lf].n, F.mpad, F.t, local_view(p.lv[lf], sm).r, tid, nth);
+        __syncthreads();
+    }
+    int l = lf;
+    for (;; ++l) {
+        const TailLevel<T, M>& G = p.lv[l];
+        const LocalView<T, M> V = local_view(G, sm);
+        if (G.coarsest || l == p.nlev - 1) {
+            dense_rows<T, M, false>(G.n, V.inv, V.r, V.z, tid, nth);
+            __syncthreads();
+            break;
+        }
+        local_ilu<B, KM, T, M>(G, V, V.r, V.z, nullptr);
+        residual_rows<B, KM, T, M, false, true>(G.nb, G.nstages >= 1 ? G.sp[1] : 0, V.m, V.a, V.z, V.r, V.t, tid,
+                                                nth);
+        __syncthreads();
+        restrict_padded_rows<T, false>(p.lv[l + 1].n, V.mpad, V.t, local_view(p.lv[l + 1], sm).r, tid, nth);
+        __syncthreads();
+    }
+    for (--l; l >= lf; --l) {
+        const TailLevel<T, M>& G = p.lv[l];
+        const LocalView<T, M> V = local_view(G, sm);
+        prolong_rows<B, T, false>(G.nb, V.aggb, local_view(p.lv[l + 1], sm).z, V.z, tid, nth);
+        __syncthreads();
+        residual_rows<B, KM, T, M, false, true>(G.nb, 0, V.m, V.a, V.z, V.r, V.t, tid, nth);
+        __syncthreads();
+        local_ilu<B, KM, T, M>(G, V, V.t, V.w, V.z);
+    }
+    const T* zs = local_view(p.lv[lf], sm).z;
+    for (int i = tid; i < p.lv[lf].n; i += nth) p.lv[lf].z[i] = zs[i];
 }
 
 // z = V-cycle(r) from level lv[0] down; r and z of lv[0] are r_top, z_top.
@@ -1075,34 +1288,56 @@ template <int B, int KM, class T, class M>
 __global__ void __launch_bounds__(kTailThreads)
     mg_tail_kernel(const __grid_constant__ TailParams<T, M> p, const T* r_top, T* z_top, const KScal* sc, int skip_if_s)
 {
+    constexpr bool U = KM > 0;  // slices of uniform width (unrolled rows only)
+    extern __shared__ __align__(16) unsigned char tail_smem[];
     if (mg_skip(sc, skip_if_s)) return;
+    long long* const trace = p.trace;
+    int tk = 0;
+    if (trace != nullptr && blockIdx.x == 0 && threadIdx.x == 0) trace[tk] = clock64();
+    ++tk;
+    const int lf = p.local_first < p.nlev ? p.local_first : p.nlev;
+    if (lf < p.nlev && blockIdx.x == 0) start_local_copies(p.copies, p.ncopies, tail_smem);
     prefetch_regions(p.reg, p.nregions);
-    THREAD_RANGE;
+    // rows go to threads a warp (one slice of 32 rows) at a time, round robin
+    // over the cluster's blocks, so that a step of a few slices still spreads
+    // over every SM of the cluster
+    const int tid = (((int)(threadIdx.x >> 5) * (int)gridDim.x + (int)blockIdx.x) << 5) | (int)(threadIdx.x & 31);
+    const int nth = (int)(gridDim.x * blockDim.x);
     int l = 0;
-    for (;; ++l) {
+    for (; l < lf; ++l) {
         const TailLevel<T, M>& L = p.lv[l];
         const T* r = l == 0 ? r_top : L.r;
         T* z = l == 0 ? z_top : L.z;
         if (L.coarsest || l == p.nlev - 1) {
             dense_rows<T, M, true>(L.n, L.inv, r, z, tid, nth);
-            cluster_barrier();
+            tail_step(trace, tk);
             break;
         }
-        tail_ilu<B, KM, T, M>(L, r, z, nullptr, tid, nth);
-        residual_rows<B, KM, T, M, true>(L.nb, L.nstages >= 1 ? L.stage_ptr[1] : 0, L.m, L.a, z, r, L.t, tid, nth);
-        cluster_barrier();
-        restrict_rows<T, true>(p.lv[l + 1].n, L.mptr, L.midx, L.t, p.lv[l + 1].r, tid, nth);
-        cluster_barrier();
+        tail_ilu<B, KM, T, M>(L, r, z, nullptr, tid, nth, trace, tk);
+        residual_rows<B, KM, T, M, true, U>(L.nb, L.nstages >= 1 ? L.sp[1] : 0, L.m, L.a, z, r, L.t, tid, nth);
+        tail_step(trace, tk);
+        if (l + 1 < lf) {
+            restrict_padded_rows<T, true>(p.lv[l + 1].n, L.mpad, L.t, p.lv[l + 1].r, tid, nth);
+            tail_step(trace, tk);
+        }
+    }
+    if (l == lf) {
+        // the levels kept in shared memory: block 0 alone, the other blocks
+        // wait at the next cluster barrier
+        if constexpr (U) {
+            if (blockIdx.x == 0) local_cycle<B, KM, T, M>(p, lf, tail_smem);
+        }
+        tail_step(trace, tk);
     }
     for (--l; l >= 0; --l) {
         const TailLevel<T, M>& L = p.lv[l];
         const T* r = l == 0 ? r_top : L.r;
         T* z = l == 0 ? z_top : L.z;
         prolong_rows<B, T, true>(L.nb, L.aggb, p.lv[l + 1].z, z, tid, nth);
-        cluster_barrier();
-        residual_rows<B, KM, T, M, true>(L.nb, 0, L.m, L.a, z, r, L.t, tid, nth);
-        cluster_barrier();
-        tail_ilu<B, KM, T, M>(L, L.t, L.w, z, tid, nth);
+        tail_step(trace, tk);
+        residual_rows<B, KM, T, M, true, U>(L.nb, 0, L.m, L.a, z, r, L.t, tid, nth);
+        tail_step(trace, tk);
+        tail_ilu<B, KM, T, M>(L, L.t, L.w, z, tid, nth, trace, tk);
     }
 }
 
@@ -1132,21 +1367,22 @@ struct Level {
     int cx = 1, cy = 1, cz = 1;    // cells of this level's grid
     bool coarsest = false;
     std::vector<int> stage_ptr;    // stages (colours or wavefronts) of block rows, permuted order
-    Buf stage_dev;                 // the same on the device (fused coarse cycle)
     Buf perm;                      // permuted unknown position -> natural unknown
     Buf gptr, gidx, gpos;          // Galerkin gather from the finer level's values (levels > 0)
     Buf aggb;                      // coarse block row of each block row (next coarser level)
     Buf mptr, midx;                // aggregate members (unknown positions) of each coarse unknown
+    Buf mpad;                      // the same, kMembers per coarse unknown, -1 past the last (or none)
     int64_t sell_size = 0;         // slots of the block sliced ELL layout
     int64_t vals = 0;              // sell_size * bs^2
     int64_t blocks = 0;            // block entries of the pattern (without padding)
     int kmax = 0;                  // longest block row
+    int width = 0;                 // slots per row of every slice when uniform (else 0)
     Buf sell_ptr, sell_col, sell_len, sell_dk;
     Buf as64, lus64, as32, lus32;  // matrix, block ILU(0) factors (inverted diagonal blocks)
     Buf v64, v32;                  // 4 work vectors: r, z, t, w
     SellView view() const
     {
-        return SellView{sell_ptr->as<int>(), sell_col->as<int>(), sell_len->as<int>(), sell_dk->as<int>()};
+        return SellView{sell_ptr->as<int>(), sell_col->as<int>(), sell_len->as<int>(), sell_dk->as<int>(), width};
     }
     Buf work64, inv64, inv32;      // coarsest level
 };
@@ -1165,6 +1401,12 @@ struct SolverAnalysis {
     int tail_first = -1;
     int tail_kmax = 0;
     int tail_cluster[3] = {0, 0, 0};
+    // per precision: first fused level kept in block 0's shared memory
+    // (index into the fused levels; their count: none) and its bytes
+    int tail_local[3] = {0, 0, 0};
+    int tail_smem[3] = {0, 0, 0};
+    int last_mode = 0;  // precision of the last solve (pc_mode)
+    Buf tail_trace;  // SM clock after each step of the last fused cycle
     // CUDA graphs of `chunk` BiCGStab iterations: [0] FP64, [1] FP32, [2] FP64
     // with an FP32 preconditioner
     struct IterGraph {
@@ -1287,8 +1529,8 @@ inline int max_row(const HostCsr& A)
 // stage and builds the block sliced ELL pattern (each row with its diagonal
 // block).  Returns the unknown permutation (position -> natural unknown),
 // its inverse, and for every entry of `A` its position in the level's value
-// array.
-void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std::vector<int>& perm,
+// array.  With `uniform`, every slice is as wide as the longest row.
+void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, Level& L, std::vector<int>& perm,
                  std::vector<int>& iperm, std::vector<int>& vpos, bool& ok)
 {
     const int n = A.n;
@@ -1348,11 +1590,14 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std:
     // block sliced ELL, 32 block rows per slice
     const int nsl = (nb + 31) / 32;
     std::vector<int> sp(nsl + 1, 0), len(nb > 0 ? nb : 1), dk(nb > 0 ? nb : 1);
+    int wmax = 0;
+    for (int R = 0; R < nb; ++R) wmax = std::max(wmax, pptr[R + 1] - pptr[R]);
     for (int sl = 0; sl < nsl; ++sl) {
         int w = 0;
         for (int R = sl * 32; R < std::min(nb, sl * 32 + 32); ++R) w = std::max(w, pptr[R + 1] - pptr[R]);
-        sp[sl + 1] = sp[sl] + 32 * w;
+        sp[sl + 1] = sp[sl] + 32 * (uniform ? wmax : w);
     }
+    L.width = uniform ? wmax : 0;
     const int64_t size = sp[nsl];
     if (size * bb >= (int64_t)INT_MAX) fail(EQG_ERR_UNSUPPORTED, "linear system too large for 32-bit value offsets");
     std::vector<int> scol(size > 0 ? size : 1, 0);
@@ -1398,7 +1643,6 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, Level& L, std:
     L.sell_size = size;
     L.vals = size * bb;
     L.blocks = pptr[nb];
-    L.stage_dev = upload_ints(c, L.stage_ptr);
     L.sell_ptr = upload_ints(c, sp);
     L.sell_col = upload_ints(c, scol);
     L.sell_len = upload_ints(c, len);
@@ -1451,7 +1695,9 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     std::vector<int> perm, iperm, vpos;
     an->levels.emplace_back();
     const double t_copy = since();
-    order_level(c, A, natural, bs, an->levels[0], perm, iperm, vpos, an->ok);
+    // levels small enough for the fused coarse cycle get slices of uniform width
+    const int fuse_rows = c.param_i("linsolver_mg_fuse_rows", 40000);
+    order_level(c, A, natural, bs, n <= fuse_rows, an->levels[0], perm, iperm, vpos, an->ok);
     const double t_level0 = since();
     {
         std::vector<int> vmap(an->levels[0].vals > 0 ? an->levels[0].vals : 1, -1);
@@ -1517,7 +1763,7 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             Lc.cz = ccz;
             std::vector<int> cperm, ciperm, cvpos;
             bool cok = true;
-            order_level(c, C, natural, bs, Lc, cperm, ciperm, cvpos, cok);
+            order_level(c, C, natural, bs, nc_unk <= fuse_rows, Lc, cperm, ciperm, cvpos, cok);
             if (!cok) fail(EQG_ERR_DEVICE, "coarse level without a diagonal entry");
             // aggregation in permuted positions, and aggregate members
             std::vector<int> aggp(fine.n);
@@ -1541,6 +1787,12 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             }
             Lf.mptr = upload_ints(c, mptr);
             Lf.midx = upload_ints(c, midx);
+            if (max_members <= kMembers) {
+                std::vector<int> mpad((size_t)nc_unk * kMembers, -1);
+                for (int P = 0; P < nc_unk; ++P)
+                    for (int k = mptr[P]; k < mptr[P + 1]; ++k) mpad[(size_t)P * kMembers + (k - mptr[P])] = midx[k];
+                Lf.mpad = upload_ints(c, mpad);
+            }
             // Galerkin gather: for every coarse entry, the value positions of
             // the fine entries that aggregate onto it, in ascending fine-entry
             // order.  A coarse row's entries come only from its members' rows,
@@ -1598,14 +1850,17 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
         }
     }
     if (an->multigrid) {
-        // fuse the levels of at most linsolver_mg_fuse_rows unknowns (0: none)
-        const int fuse_rows = c.param_i("linsolver_mg_fuse_rows", 40000);
+        // fuse the levels of at most linsolver_mg_fuse_rows unknowns (0: none):
+        // from the first level from which on every level is that small, has
+        // slices of uniform width, at most kTailStages stages and aggregates
+        // of at most kMembers members (the coarsest needs none of these)
         const int nl = (int)an->levels.size();
-        for (int l = 0; l < nl; ++l)
-            if (an->levels[l].n <= fuse_rows && nl - l <= kMaxTail) {
-                an->tail_first = l;
-                break;
-            }
+        auto fusable = [&](const Level& L) {
+            return L.coarsest || (L.n <= fuse_rows && L.width > 0 && (int)L.stage_ptr.size() - 1 <= kTailStages &&
+                                  L.mpad);
+        };
+        for (int l = nl - 1; l >= 0 && nl - l <= kMaxTail && fusable(an->levels[l]); --l)
+            if (!an->levels[l].coarsest) an->tail_first = l;
         if (an->tail_first >= 0)
             for (int l = an->tail_first; l < nl; ++l)
                 if (!an->levels[l].coarsest) an->tail_kmax = std::max(an->tail_kmax, an->levels[l].kmax);
@@ -1694,11 +1949,13 @@ int tail_cluster_size(Core& c)
     int want = std::min(16, std::max(1, c.param_i("linsolver_mg_cluster", 16)));
     auto kern = mg_tail_kernel<B, KM, T, M>;
     if (want > 8) EQG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    EQG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kTailSmem));
     for (; want > 1; want /= 2) {
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute attr[1];
         cfg.gridDim = dim3(want);
         cfg.blockDim = dim3(kTailThreads);
+        cfg.dynamicSmemBytes = kTailSmem;
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = want;
         attr[0].val.clusterDim.y = 1;
@@ -1712,15 +1969,103 @@ int tail_cluster_size(Core& c)
     return want;
 }
 
+// The fused levels kept in block 0's shared memory: from the coarsest level
+// upward while their arrays fit in kTailSmem bytes (the first fused level
+// stays cluster-wide).  Only for slices of uniform width (rows of at most 16
+// blocks) and with linsolver_mg_local=1 (the default).  Returns the first
+// such level as an index into the fused levels (their count: none); fills
+// `bytes` and, when `p` is given, the layout and the copies.
+template <class T, class M>
+int plan_local(Core& c, const SolverAnalysis& an, int& bytes, TailParams<T, M>* p)
+{
+    const int nlev = (int)an.levels.size() - an.tail_first;
+    bytes = 0;
+    if (an.tail_first < 0 || an.tail_kmax > 16 || !c.param_i("linsolver_mg_local", 1)) return nlev;
+    auto al = [](int64_t b) { return (b + 15) & ~(int64_t)15; };
+    int lf = nlev;
+    int64_t total = 0;
+    int copies = 0;
+    for (int i = nlev - 1; i >= 1; --i) {
+        const Level& L = an.levels[an.tail_first + i];
+        int64_t b = 2 * al((int64_t)L.n * sizeof(T));
+        int nc = 0;
+        if (L.coarsest) {
+            b += al((int64_t)L.n * L.n * sizeof(M));
+            nc = 1;
+        } else {
+            const Level& C = an.levels[an.tail_first + i + 1];
+            b += 2 * al(L.vals * (int64_t)sizeof(M)) + al(L.sell_size * 4) + 3 * al((int64_t)L.nb * 4) +
+                 al((int64_t)C.n * kMembers * 4) + 2 * al((int64_t)L.n * sizeof(T));
+            nc = 7;
+        }
+        if (total + b > kTailSmem || copies + nc > kMaxCopies) break;
+        total += b;
+        copies += nc;
+        lf = i;
+    }
+    if (lf == nlev) return nlev;
+    bytes = (int)total;
+    if (p) {
+        int off = 0;
+        auto place = [&](int64_t b) {
+            const int o = off;
+            off += (int)al(b);
+            return o;
+        };
+        auto copy = [&](const void* src, int dst, int64_t b) {
+            p->copies[p->ncopies++] = TailCopy{src, dst, (int)b};
+        };
+        for (int i = lf; i < nlev; ++i) {
+            const Level& L = an.levels[an.tail_first + i];
+            TailLocal& o = p->lv[i].so;
+            o = TailLocal{};
+            o.r = place((int64_t)L.n * sizeof(T));
+            o.z = place((int64_t)L.n * sizeof(T));
+            if (L.coarsest) {
+                o.inv = place((int64_t)L.n * L.n * sizeof(M));
+                copy(level_inv<M>(L), o.inv, (int64_t)L.n * L.n * sizeof(M));
+                continue;
+            }
+            const Level& C = an.levels[an.tail_first + i + 1];
+            o.t = place((int64_t)L.n * sizeof(T));
+            o.w = place((int64_t)L.n * sizeof(T));
+            o.a = place(L.vals * (int64_t)sizeof(M));
+            o.lu = place(L.vals * (int64_t)sizeof(M));
+            o.col = place(L.sell_size * 4);
+            o.len = place((int64_t)L.nb * 4);
+            o.dk = place((int64_t)L.nb * 4);
+            o.aggb = place((int64_t)L.nb * 4);
+            o.mpad = place((int64_t)C.n * kMembers * 4);
+            copy(level_a<M>(L), o.a, L.vals * (int64_t)sizeof(M));
+            copy(level_lu<M>(L), o.lu, L.vals * (int64_t)sizeof(M));
+            copy(L.sell_col->ptr, o.col, L.sell_size * 4);
+            copy(L.sell_len->ptr, o.len, (int64_t)L.nb * 4);
+            copy(L.sell_dk->ptr, o.dk, (int64_t)L.nb * 4);
+            copy(L.aggb->ptr, o.aggb, (int64_t)L.nb * 4);
+            copy(L.mpad->ptr, o.mpad, (int64_t)C.n * kMembers * 4);
+        }
+        if (off != bytes) fail(EQG_ERR_DEVICE, "fused coarse cycle: shared memory layout mismatch");
+        p->local_first = lf;
+    }
+    return lf;
+}
+
 // Chooses the cluster size of the fused coarse cycle for one precision;
 // called before any stream capture.
 template <class T, class M>
 void prepare_tail(Core& c, SolverAnalysis& an)
 {
     if (an.tail_first < 0) return;
-    int& cl = an.tail_cluster[pc_mode<T, M>()];
+    if (c.param_i("linsolver_tail_trace", 0) && !an.tail_trace) {
+        an.tail_trace = c.allocN<long long>(kTraceMax);
+        EQG_CUDA(cudaMemsetAsync(an.tail_trace->ptr, 0, kTraceMax * sizeof(long long), c.stream));
+    }
+    const int mode = pc_mode<T, M>();
+    int& cl = an.tail_cluster[mode];
     const int bs = an.levels[an.tail_first].bs;
     if (!cl) WITH_BS(bs, WITH_KMAX(an.tail_kmax, cl = tail_cluster_size<BS, KK, T, M>(c)));
+    an.tail_local[mode] = plan_local<T, M>(c, an, an.tail_smem[mode], nullptr);
+    an.last_mode = mode;
 }
 
 // z = V-cycle(r) from level tail_first down, as one mg_tail_kernel launch.
@@ -1743,7 +2088,7 @@ void launch_tail(Core& c, const SolverAnalysis& an, const T* r, T* z, const KSca
         } else {
             region(level_lu<M>(L), L.vals * (int64_t)sizeof(M));
             region(L.aggb->ptr, (int64_t)L.nb * 4);
-            region(L.midx->ptr, (int64_t)L.n * 4);
+            region(L.mpad->ptr, (int64_t)an.levels[l + 1].n * kMembers * 4);
         }
         TailLevel<T, M>& t = p.lv[p.nlev++];
         t.nb = L.nb;
@@ -1751,27 +2096,31 @@ void launch_tail(Core& c, const SolverAnalysis& an, const T* r, T* z, const KSca
         t.coarsest = L.coarsest ? 1 : 0;
         t.m = L.view();
         t.a = level_a<M>(L);
-        t.stage_ptr = L.stage_dev->as<int>();
         t.nstages = (int)L.stage_ptr.size() - 1;
+        for (int s = 0; s <= t.nstages && s <= kTailStages; ++s) t.sp[s] = L.stage_ptr[s];
         if (L.coarsest) {
             t.inv = level_inv<M>(L);
         } else {
             t.lu = level_lu<M>(L);
             t.aggb = L.aggb->as<int>();
-            t.mptr = L.mptr->as<int>();
-            t.midx = L.midx->as<int>();
+            t.mpad = L.mpad->as<int>();
         }
         t.r = level_vec<T>(L, 0);
         t.z = level_vec<T>(L, 1);
         t.t = level_vec<T>(L, 2);
         t.w = level_vec<T>(L, 3);
     }
+    if (an.tail_trace) p.trace = an.tail_trace->as<long long>();
+    p.local_first = p.nlev;
+    int smem = 0;
+    if (an.tail_local[pc_mode<T, M>()] < p.nlev) plan_local<T, M>(c, an, smem, &p);
     const int cl = an.tail_cluster[pc_mode<T, M>()];
     if (cl <= 0) fail(EQG_ERR_DEVICE, "fused coarse cycle launched before its cluster size was chosen");
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     cfg.gridDim = dim3(cl);
     cfg.blockDim = dim3(kTailThreads);
+    cfg.dynamicSmemBytes = (size_t)smem;
     cfg.stream = c.stream;
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = cl;
@@ -1782,6 +2131,51 @@ void launch_tail(Core& c, const SolverAnalysis& an, const T* r, T* z, const KSca
     WITH_BS(an.levels[an.tail_first].bs, WITH_KMAX(an.tail_kmax, launch(c, "mg_tail", [&] {
                 EQG_CUDA(cudaLaunchKernelEx(&cfg, mg_tail_kernel<BS, KK, T, M>, p, r, z, sc, skip_if_s));
             })));
+}
+
+// Prints the steps of the last fused coarse cycle (linsolver_tail_trace=1):
+// SM clock cycles from the end of one step to the end of the next, named in
+// the kernel's order.
+void report_tail_trace(Core& c, const SolverAnalysis& an)
+{
+    if (!an.tail_trace || an.tail_first < 0) return;
+    std::vector<long long> t(kTraceMax);
+    c.sync();
+    EQG_CUDA(cudaMemcpy(t.data(), an.tail_trace->ptr, kTraceMax * sizeof(long long), cudaMemcpyDeviceToHost));
+    std::vector<std::string> names;
+    const int last = (int)an.levels.size() - 1;
+    auto ilu = [&](int l) {
+        const int ns = (int)an.levels[l].stage_ptr.size() - 1;
+        for (int s = 1; s < ns; ++s) names.push_back("L" + std::to_string(l) + ".lower" + std::to_string(s));
+        for (int s = ns >= 2 ? ns - 2 : 0; s >= 0 && ns > 0; --s)
+            names.push_back("L" + std::to_string(l) + ".upper" + std::to_string(s));
+    };
+    const int lf = an.tail_first + an.tail_local[an.last_mode];  // first shared-memory level (last + 1: none)
+    int l = an.tail_first;
+    for (; l < lf; ++l) {
+        if (an.levels[l].coarsest || l == last) {
+            names.push_back("L" + std::to_string(l) + ".dense");
+            break;
+        }
+        ilu(l);
+        names.push_back("L" + std::to_string(l) + ".residual");
+        if (l + 1 < lf) names.push_back("L" + std::to_string(l) + ".restrict");
+    }
+    if (l == lf && lf <= last)
+        names.push_back("L" + std::to_string(lf - 1) + ".restrict+L" + std::to_string(lf) + "-L" +
+                        std::to_string(last) + ".shared");
+    for (--l; l >= an.tail_first; --l) {
+        names.push_back("L" + std::to_string(l) + ".prolong");
+        names.push_back("L" + std::to_string(l) + ".residual");
+        ilu(l);
+    }
+    const int nsteps = std::min((int)names.size(), kTraceMax - 1);
+    int khz = 0;
+    cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, c.device);
+    std::printf("        fused coarse cycle: %lld SM cycles (%.1f us at %.0f MHz), per step:",
+                t[nsteps] - t[0], khz > 0 ? (t[nsteps] - t[0]) / (khz * 1e-3) : 0.0, khz * 1e-3);
+    for (int i = 0; i < nsteps; ++i) std::printf(" %s=%lld", names[i].c_str(), t[i + 1] - t[i]);
+    std::printf("\n");
 }
 
 // out = M^{-1} b for the block ILU(0) factors of one level; with zadd,
@@ -2120,6 +2514,7 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         res.rel_residual = bb > 0 ? std::sqrt(rr / bb) : 0.0;
     }
     c.krylov_clock.stop(c.stream);
+    report_tail_trace(c, an);
     launch(c, "unpermute",
            [&] { unpermute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, L0.perm->as<int>(), xout, n); });
     res.block_size = L0.bs;

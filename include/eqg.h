@@ -122,7 +122,11 @@ const char* eqg_backend_name(void);
  * linsolver_block (1: ncomp x ncomp block ILU(0) for 2 or 3 unknowns per
  * cell; 0: scalar ILU(0)), linsolver_mg_fuse_rows (40000: the V-cycle
  * levels up to this size run as one kernel; 0: none), linsolver_mg_cluster
- * (16: thread blocks of that kernel's cluster, at most 16), lazy (0; 1:
+ * (16: thread blocks of that kernel's cluster, at most 16),
+ * linsolver_mg_local (1: that kernel keeps its coarsest levels in one thread
+ * block's shared memory while they fit in 200 KB; 0: off),
+ * linsolver_tail_trace (0; 1: print the SM clock cycles of every step of the
+ * last fused cycle after each linear solve), lazy (0; 1:
  * defer value-only elementwise operations and evaluate them in batches),
  * host_threads (0: OpenMP's default for the solver analysis), time_kernel
  * (a kernel name, or "*", to time with CUDA events) and device (CUDA device

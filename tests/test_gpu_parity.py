@@ -174,15 +174,18 @@ def test_fused_coarse_cycle_identical(gpu_lib, shape, precision):
     """The V-cycle's coarse levels fused into one cluster kernel compute every
     element with the same operations as the launch-per-step cycle: pressure
     and saturation are bit-identical with no levels fused, some fused, all
-    fused, and for cluster sizes 1, 8 and 16."""
+    fused, for cluster sizes 1, 8 and 16, and with the coarsest fused levels
+    in block 0's shared memory or not (linsolver_mg_local)."""
     grid, case = programs.two_phase_case(*shape, steps=2)
     params = dict(grid, abs_res_tol=1e-10, linsolver_residual_tolerance=1e-10, linsolver_max_iterations=5000,
                   linsolver_precision=precision)
     runs = {}
-    for fuse, cluster in [(0, 16), (600, 16), (40000, 1), (40000, 8), (40000, 16)]:
-        eg = Runtime(gpu_lib, dict(params, linsolver_mg_fuse_rows=fuse, linsolver_mg_cluster=cluster))
-        runs[(fuse, cluster)] = (programs.two_phase(eg, **case), eg.stats())
-    base, st0 = runs[(0, 16)]
+    for fuse, cluster, local in [(0, 16, 1), (600, 16, 1), (600, 16, 0), (40000, 1, 1), (40000, 8, 1),
+                                 (40000, 16, 1), (40000, 16, 0)]:
+        eg = Runtime(gpu_lib, dict(params, linsolver_mg_fuse_rows=fuse, linsolver_mg_cluster=cluster,
+                                   linsolver_mg_local=local))
+        runs[(fuse, cluster, local)] = (programs.two_phase(eg, **case), eg.stats())
+    base, st0 = runs[(0, 16, 1)]
     for key, (out, st) in runs.items():
         assert st["krylov_iterations"] == st0["krylov_iterations"], key
         for (pa, sa), (pb, sb) in zip(out, base):
