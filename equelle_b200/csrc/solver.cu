@@ -638,14 +638,24 @@ __device__ __forceinline__ void restrict_padded_rows(int nc, const int* __restri
     }
 }
 
-// z_R += zc_{aggb[R]} (piecewise-constant prolongation, per block row)
+// z_R += alpha zc_{aggb[R]} (piecewise-constant prolongation, per block
+// row, scaled by the over-correction factor alpha).  Piecewise-constant
+// interpolation from aggregates underestimates the smooth error it
+// corrects.  Measured on the two-phase cases, BiCGStab iterations per time
+// step: 2 x 2 x 2 aggregates (128 x 128 x 64) 121 at 1.0, 97 at 1.25 to
+// 1.45, 104 at 1.6, 127 at 1.9; 2 x 2 aggregates (512 x 512) 92 at 1.0, 49
+// at 1.3, 29 at 1.6, 24 at 1.8, 22 at 2.0, 27 at 2.2.
+constexpr double kMgAlpha3d = 1.4;
+constexpr double kMgAlpha2d = 1.9;
 template <int B, class T, bool CG>
 __device__ __forceinline__ void prolong_rows(int nb, const int* __restrict__ aggb, const T* __restrict__ zc,
-                                             T* __restrict__ z, int tid, int nth)
+                                             T* __restrict__ z, double alpha, int tid, int nth)
 {
     for (int R = tid; R < nb; R += nth) {
         double e[B];
         load_bvec<B, T, CG>(zc, aggb[R], e);
+#pragma unroll
+        for (int c = 0; c < B; ++c) e[c] *= alpha;
         update_z<B, T, CG>(z, R, e);
     }
 }
@@ -967,11 +977,11 @@ __global__ void mg_restrict_kernel(int nc, const int* __restrict__ mptr, const i
 
 template <int B, class T>
 __global__ void mg_prolong_kernel(int nb, const int* __restrict__ aggb, const T* __restrict__ zc, T* __restrict__ z,
-                                  const KScal* sc, int skip_if_s)
+                                  double alpha, const KScal* sc, int skip_if_s)
 {
     if (mg_skip(sc, skip_if_s)) return;
     THREAD_RANGE;
-    prolong_rows<B, T, false>(nb, aggb, zc, z, tid, nth);
+    prolong_rows<B, T, false>(nb, aggb, zc, z, alpha, tid, nth);
 }
 
 // Inverse of the coarsest matrix (n <= kCoarsest unknowns) by Gauss-Jordan
@@ -1116,6 +1126,7 @@ struct TailParams {
     int ncopies = 0;
     PrefetchRegion reg[kMaxPrefetch];
     TailCopy copies[kMaxCopies];
+    double alpha = 1.0;          // coarse-correction factor
     long long* trace = nullptr;  // SM clock after each step (linsolver_tail_trace)
 };
 
@@ -1273,7 +1284,7 @@ __device__ void local_cycle(const TailParams<T, M>& p, int lf, unsigned char* sm
     for (--l; l >= lf; --l) {
         const TailLevel<T, M>& G = p.lv[l];
         const LocalView<T, M> V = local_view(G, sm);
-        prolong_rows<B, T, false>(G.nb, V.aggb, local_view(p.lv[l + 1], sm).z, V.z, tid, nth);
+        prolong_rows<B, T, false>(G.nb, V.aggb, local_view(p.lv[l + 1], sm).z, V.z, p.alpha, tid, nth);
         __syncthreads();
         residual_rows<B, KM, T, M, false, true>(G.nb, 0, V.m, V.a, V.z, V.r, V.t, tid, nth);
         __syncthreads();
@@ -1333,7 +1344,7 @@ __global__ void __launch_bounds__(kTailThreads)
         const TailLevel<T, M>& L = p.lv[l];
         const T* r = l == 0 ? r_top : L.r;
         T* z = l == 0 ? z_top : L.z;
-        prolong_rows<B, T, true>(L.nb, L.aggb, p.lv[l + 1].z, z, tid, nth);
+        prolong_rows<B, T, true>(L.nb, L.aggb, p.lv[l + 1].z, z, p.alpha, tid, nth);
         tail_step(trace, tk);
         residual_rows<B, KM, T, M, true, U>(L.nb, 0, L.m, L.a, z, r, L.t, tid, nth);
         tail_step(trace, tk);
@@ -1393,6 +1404,7 @@ struct SolverAnalysis {
     bool natural = false;
     bool ok = true;  // every row has a diagonal entry (1 x 1 blocks)
     bool multigrid = false;
+    double mg_alpha = 1.0;  // coarse-grid correction factor
     std::vector<Level> levels;
     Buf vmap;        // level-0 value <- Jacobian entry (-1: zero)
     Buf vec64, vec32, scal, partials, counter, factor_status;
@@ -1706,6 +1718,7 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
         an->vmap = upload_ints(c, vmap);
     }
     an->multigrid = mg_wanted && an->ok;
+    an->mg_alpha = c.param_d("linsolver_mg_alpha", c.nz > 1 ? kMgAlpha3d : kMgAlpha2d);
     an->levels[0].cx = c.nx;
     an->levels[0].cy = c.ny;
     an->levels[0].cz = c.nz;
@@ -2111,6 +2124,7 @@ void launch_tail(Core& c, const SolverAnalysis& an, const T* r, T* z, const KSca
         t.w = level_vec<T>(L, 3);
     }
     if (an.tail_trace) p.trace = an.tail_trace->as<long long>();
+    p.alpha = an.mg_alpha;
     p.local_first = p.nlev;
     int smem = 0;
     if (an.tail_local[pc_mode<T, M>()] < p.nlev) plan_local<T, M>(c, an, smem, &p);
@@ -2250,8 +2264,8 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     vcycle<T, M>(c, an, l + 1, rc, zc, sc, skip);
     // coarse correction z += P zc, then post-smoothing z += M^{-1} (r - A z)
     WITH_BS(L.bs, launch(c, "mg_prolong", [&] {
-                mg_prolong_kernel<BS, T><<<blocksFor(L.nb), kThreads, 0, c.stream>>>(L.nb, L.aggb->as<int>(), zc, z,
-                                                                                     sc, skip);
+                mg_prolong_kernel<BS, T><<<blocksFor(L.nb), kThreads, 0, c.stream>>>(
+                    L.nb, L.aggb->as<int>(), zc, z, an.mg_alpha, sc, skip);
             }));
     level_residual<T, M>(c, L, z, r, t, 0, sc, skip);
     ilu_apply<T, M>(c, L, t, w, z, sc, skip);
