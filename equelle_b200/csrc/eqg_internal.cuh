@@ -185,6 +185,7 @@ struct Core {
     std::vector<eqg_solve_info> solves;
     // device timing of one named kernel (parameter time_kernel)
     std::string timed_kernel;  // a kernel name, or "*" for all of them
+    bool pdl_launch = false;   // BiCGStab iteration kernels as programmatic dependent launches (linsolver_pdl)
     struct TimedLaunch {
         const char* name;
         cudaEvent_t a, b;

@@ -75,6 +75,13 @@ enum { ST_RUN = 0, ST_CONV = 1, ST_BREAK = 2 };
 
 __device__ __forceinline__ bool stopped(const KScal* sc) { return sc->status != ST_RUN; }
 
+// First statement of every kernel of a BiCGStab iteration: those kernels are
+// launched as programmatic dependent launches (launch_k), so their blocks may
+// be scheduled while the kernel before them on the stream still runs; this
+// waits until that kernel has completed and its writes are visible (at once
+// when the kernel was launched normally).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Block-wide sum of NV values; returns sums to thread 0.
 template <int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV])
@@ -687,6 +694,7 @@ __global__ void bilu_lower_kernel(int r0, int r1, int r_first, int last, SellVie
                                   const T* __restrict__ b, T* __restrict__ out, T* __restrict__ zadd,
                                   const KScal* sc, int skip_if_s)
 {
+    pdl_wait();
     if (mg_skip(sc, skip_if_s)) return;
     THREAD_RANGE;
     lower_rows<B, KM, T, M, false>(r0, r1, r_first, last, m, lu, b, out, zadd, tid, nth);
@@ -697,6 +705,7 @@ __global__ void bilu_upper_kernel(int r0, int r1, int first, SellView m, const M
                                   const T* __restrict__ b, T* __restrict__ out, T* __restrict__ zadd,
                                   const KScal* sc, int skip_if_s)
 {
+    pdl_wait();
     if (mg_skip(sc, skip_if_s)) return;
     THREAD_RANGE;
     upper_rows<B, KM, T, M, false>(r0, r1, first, m, lu, b, out, zadd, tid, nth);
@@ -747,14 +756,84 @@ __global__ void bicg_init_kernel(const T* __restrict__ b, T* r, T* rhat, T* p, T
     }
 }
 
+// The BiCGStab vectors in 16-byte chunks (two doubles or four floats); each
+// vector starts on a 16-byte boundary (vec_stride), the elements past the
+// last whole chunk are done one by one.
+template <class T>
+struct Chunk;
+template <>
+struct Chunk<double> {
+    using V = double2;
+    static constexpr int W = 2;
+};
+template <>
+struct Chunk<float> {
+    using V = float4;
+    static constexpr int W = 4;
+};
+
+template <class T>
+__device__ __forceinline__ void load_chunk(const T* __restrict__ p, int64_t c, double (&v)[Chunk<T>::W])
+{
+    const typename Chunk<T>::V t = reinterpret_cast<const typename Chunk<T>::V*>(p)[c];
+    if constexpr (Chunk<T>::W == 2) {
+        v[0] = t.x;
+        v[1] = t.y;
+    } else {
+        v[0] = t.x;
+        v[1] = t.y;
+        v[2] = t.z;
+        v[3] = t.w;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void store_chunk(T* __restrict__ p, int64_t c, const T (&v)[Chunk<T>::W])
+{
+    typename Chunk<T>::V t;
+    if constexpr (Chunk<T>::W == 2) {
+        t.x = v[0];
+        t.y = v[1];
+    } else {
+        t.x = v[0];
+        t.y = v[1];
+        t.z = v[2];
+        t.w = v[3];
+    }
+    reinterpret_cast<typename Chunk<T>::V*>(p)[c] = t;
+}
+
+// Elements between the starts of two BiCGStab vectors: a multiple of 4, so
+// that every vector of a buffer from allocN starts on a 16-byte boundary.
+inline size_t vec_stride(int n) { return ((size_t)(n > 0 ? n : 1) + 3) & ~(size_t)3; }
+
+// Chunks c of n elements for this thread, then the remaining elements i.
+#define CHUNK_STRIDE(c, n, W) GRID_STRIDE(c, (int64_t)(n) / (W))
+#define REST_STRIDE(i, n, W)                                                                                  \
+    for (int64_t i = (int64_t)(n) / (W) * (W) + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); \
+         i += (int64_t)gridDim.x * blockDim.x)
+
 template <class T>
 __global__ void bicg_p_kernel(const T* __restrict__ r, const T* __restrict__ v, T* __restrict__ p, int n,
                               const KScal* sc)
 {
+    pdl_wait();
     if (stopped(sc)) return;
     const double beta = (sc->rho_new / sc->rho) * (sc->alpha / sc->omega);
     const double omega = sc->omega;
-    GRID_STRIDE(i, n) p[i] = (T)((double)r[i] + beta * ((double)p[i] - omega * (double)v[i]));
+    constexpr int W = Chunk<T>::W;
+    CHUNK_STRIDE(c, n, W)
+    {
+        double rv[W], pv[W], vv[W];
+        load_chunk<T>(r, c, rv);
+        load_chunk<T>(p, c, pv);
+        load_chunk<T>(v, c, vv);
+        T o[W];
+#pragma unroll
+        for (int j = 0; j < W; ++j) o[j] = (T)(rv[j] + beta * (pv[j] - omega * vv[j]));
+        store_chunk<T>(p, c, o);
+    }
+    REST_STRIDE(i, n, W) p[i] = (T)((double)r[i] + beta * ((double)p[i] - omega * (double)v[i]));
 }
 
 // The SpMV kernels are latency bound; for the FP64 layouts with blocks of
@@ -773,6 +852,7 @@ __global__ void __launch_bounds__(kThreads, spmv_min_blocks<B, KM, T>(8)) bicg_s
                                        const T* __restrict__ rhat, T* __restrict__ v, int nb, double* partials,
                                        unsigned int* counter, KScal* sc)
 {
+    pdl_wait();
     if (stopped(sc)) return;
     double d[1] = {0.0};
     GRID_STRIDE(rr, nb)
@@ -804,10 +884,25 @@ template <class T>
 __global__ void bicg_s_kernel(const T* __restrict__ r, const T* __restrict__ v, T* __restrict__ s, int n,
                               double* partials, unsigned int* counter, KScal* sc)
 {
+    pdl_wait();
     if (stopped(sc)) return;
     const double alpha = sc->alpha;
     double d[1] = {0.0};
-    GRID_STRIDE(i, n)
+    constexpr int W = Chunk<T>::W;
+    CHUNK_STRIDE(c, n, W)
+    {
+        double rv[W], vv[W];
+        load_chunk<T>(r, c, rv);
+        load_chunk<T>(v, c, vv);
+        T o[W];
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            o[j] = (T)(rv[j] - alpha * vv[j]);
+            d[0] += (double)o[j] * (double)o[j];
+        }
+        store_chunk<T>(s, c, o);
+    }
+    REST_STRIDE(i, n, W)
     {
         const T si = (T)((double)r[i] - alpha * (double)v[i]);
         s[i] = si;
@@ -826,6 +921,7 @@ __global__ void __launch_bounds__(kThreads, spmv_min_blocks<B, KM, T>(6)) bicg_s
                                        const T* __restrict__ s, T* __restrict__ t, int nb, double* partials,
                                        unsigned int* counter, KScal* sc)
 {
+    pdl_wait();
     if (stopped(sc) || sc->s_conv) return;
     double d[2] = {0.0, 0.0};
     GRID_STRIDE(rr, nb)
@@ -860,16 +956,48 @@ __global__ void bicg_xr_kernel(const T* __restrict__ ph, const T* __restrict__ s
                                const T* __restrict__ t, const T* __restrict__ rhat, T* __restrict__ x,
                                T* __restrict__ r, int n, double* partials, unsigned int* counter, KScal* sc)
 {
+    pdl_wait();
     if (stopped(sc)) return;
     const double alpha = sc->alpha;
     const int half = sc->s_conv;
     const double omega = half ? 0.0 : sc->omega;
     double d[2] = {0.0, 0.0};
-    GRID_STRIDE(i, n)
-    {
-        if (half) {
-            x[i] = (T)((double)x[i] + alpha * (double)ph[i]);
-        } else {
+    constexpr int W = Chunk<T>::W;
+    if (half) {
+        CHUNK_STRIDE(c, n, W)
+        {
+            double xv[W], pv[W];
+            load_chunk<T>(x, c, xv);
+            load_chunk<T>(ph, c, pv);
+            T o[W];
+#pragma unroll
+            for (int j = 0; j < W; ++j) o[j] = (T)(xv[j] + alpha * pv[j]);
+            store_chunk<T>(x, c, o);
+        }
+        REST_STRIDE(i, n, W) x[i] = (T)((double)x[i] + alpha * (double)ph[i]);
+    } else {
+        CHUNK_STRIDE(c, n, W)
+        {
+            double xv[W], pv[W], shv[W], sv[W], tv[W], hv[W];
+            load_chunk<T>(x, c, xv);
+            load_chunk<T>(ph, c, pv);
+            load_chunk<T>(sh, c, shv);
+            load_chunk<T>(s, c, sv);
+            load_chunk<T>(t, c, tv);
+            load_chunk<T>(rhat, c, hv);
+            T xo[W], ro[W];
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                xo[j] = (T)(xv[j] + alpha * pv[j] + omega * shv[j]);
+                ro[j] = (T)(sv[j] - omega * tv[j]);
+                d[0] += (double)ro[j] * (double)ro[j];
+                d[1] += hv[j] * (double)ro[j];
+            }
+            store_chunk<T>(x, c, xo);
+            store_chunk<T>(r, c, ro);
+        }
+        REST_STRIDE(i, n, W)
+        {
             x[i] = (T)((double)x[i] + alpha * (double)ph[i] + omega * (double)sh[i]);
             const T ri = (T)((double)s[i] - omega * (double)t[i]);
             r[i] = ri;
@@ -961,6 +1089,7 @@ template <int B, int KM, class T, class M>
 __global__ void mg_residual_kernel(int nb, int r_zero, SellView m, const M* __restrict__ a, const T* __restrict__ x,
                                    const T* __restrict__ b, T* __restrict__ out, const KScal* sc, int skip_if_s)
 {
+    pdl_wait();
     if (mg_skip(sc, skip_if_s)) return;
     THREAD_RANGE;
     residual_rows<B, KM, T, M, false>(nb, r_zero, m, a, x, b, out, tid, nth);
@@ -970,6 +1099,7 @@ template <class T>
 __global__ void mg_restrict_kernel(int nc, const int* __restrict__ mptr, const int* __restrict__ midx,
                                    const T* __restrict__ t, T* __restrict__ rc, const KScal* sc, int skip_if_s)
 {
+    pdl_wait();
     if (mg_skip(sc, skip_if_s)) return;
     THREAD_RANGE;
     restrict_rows<T, false>(nc, mptr, midx, t, rc, tid, nth);
@@ -979,6 +1109,7 @@ template <int B, class T>
 __global__ void mg_prolong_kernel(int nb, const int* __restrict__ aggb, const T* __restrict__ zc, T* __restrict__ z,
                                   double alpha, const KScal* sc, int skip_if_s)
 {
+    pdl_wait();
     if (mg_skip(sc, skip_if_s)) return;
     THREAD_RANGE;
     prolong_rows<B, T, false>(nb, aggb, zc, z, alpha, tid, nth);
@@ -1056,6 +1187,7 @@ template <class T, class M>
 __global__ void dense_apply_kernel(int n, const M* __restrict__ inv, const T* __restrict__ r, T* __restrict__ z,
                                    const KScal* sc, int skip_if_s)
 {
+    pdl_wait();
     if (mg_skip(sc, skip_if_s)) return;
     dense_rows<T, M, false>(n, inv, r, z, (int)threadIdx.x, (int)blockDim.x);
 }
@@ -1299,6 +1431,7 @@ template <int B, int KM, class T, class M>
 __global__ void __launch_bounds__(kTailThreads)
     mg_tail_kernel(const __grid_constant__ TailParams<T, M> p, const T* r_top, T* z_top, const KScal* sc, int skip_if_s)
 {
+    pdl_wait();
     constexpr bool U = KM > 0;  // slices of uniform width (unrolled rows only)
     extern __shared__ __align__(16) unsigned char tail_smem[];
     if (mg_skip(sc, skip_if_s)) return;
@@ -1878,7 +2011,7 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             for (int l = an->tail_first; l < nl; ++l)
                 if (!an->levels[l].coarsest) an->tail_kmax = std::max(an->tail_kmax, an->levels[l].kmax);
     }
-    an->vec64 = c.allocN<double>((size_t)10 * (n > 0 ? n : 1));
+    an->vec64 = c.allocN<double>((size_t)10 * vec_stride(n));
     an->scal = c.alloc(sizeof(KScal));
     an->partials = c.allocN<double>((size_t)kRedBlocks * 2);
     an->counter = c.allocN<unsigned int>(1);
@@ -1905,7 +2038,7 @@ Vecs<T> vecs(T* base, int n)
 {
     Vecs<T> v;
     T* q[10];
-    for (int k = 0; k < 10; ++k) q[k] = base + (size_t)k * (n > 0 ? n : 1);
+    for (int k = 0; k < 10; ++k) q[k] = base + (size_t)k * vec_stride(n);
     v.x = q[0];
     v.r = q[1];
     v.rhat = q[2];
@@ -2063,6 +2196,26 @@ int plan_local(Core& c, const SolverAnalysis& an, int& bytes, TailParams<T, M>* 
     return lf;
 }
 
+// Launches kernel k on the runtime stream.  With c.pdl_launch it is a
+// programmatic dependent launch: its blocks may be scheduled while the
+// kernel before it on the stream finishes, which hides the launch latency
+// between the dependent kernels of a BiCGStab iteration; k starts with
+// pdl_wait(), so it reads nothing before that kernel has completed.
+template <class... KArgs, class... Args>
+void launch_k(Core& c, void (*k)(KArgs...), int grid, int block, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = c.stream;
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = c.pdl_launch ? 1 : 0;
+    EQG_CUDA(cudaLaunchKernelEx(&cfg, k, args...));
+}
+
 // Chooses the cluster size of the fused coarse cycle for one precision;
 // called before any stream capture.
 template <class T, class M>
@@ -2131,7 +2284,7 @@ void launch_tail(Core& c, const SolverAnalysis& an, const T* r, T* z, const KSca
     const int cl = an.tail_cluster[pc_mode<T, M>()];
     if (cl <= 0) fail(EQG_ERR_DEVICE, "fused coarse cycle launched before its cluster size was chosen");
     cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     cfg.gridDim = dim3(cl);
     cfg.blockDim = dim3(kTailThreads);
     cfg.dynamicSmemBytes = (size_t)smem;
@@ -2140,8 +2293,10 @@ void launch_tail(Core& c, const SolverAnalysis& an, const T* r, T* z, const KSca
     attr[0].val.clusterDim.x = cl;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = c.pdl_launch ? 2 : 1;
     WITH_BS(an.levels[an.tail_first].bs, WITH_KMAX(an.tail_kmax, launch(c, "mg_tail", [&] {
                 EQG_CUDA(cudaLaunchKernelEx(&cfg, mg_tail_kernel<BS, KK, T, M>, p, r, z, sc, skip_if_s));
             })));
@@ -2207,15 +2362,15 @@ void ilu_apply(Core& c, const Level& L, const T* b, T* out, T* zadd, const KScal
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
         const int last = s == ns - 1;
         WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "bilu_lower", [&] {
-                    bilu_lower_kernel<BS, KK, T, M><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
-                        r0, r1, r_first, last, L.view(), lu, b, out, last ? zadd : nullptr, sc, skip_if_s);
+                    launch_k(c, bilu_lower_kernel<BS, KK, T, M>, blocksFor(r1 - r0), kThreads, r0, r1, r_first, last,
+                             L.view(), lu, b, out, last ? zadd : nullptr, sc, skip_if_s);
                 })));
     }
     for (int s = ns >= 2 ? ns - 2 : 0; s >= 0; --s) {
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
         WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "bilu_upper", [&] {
-                    bilu_upper_kernel<BS, KK, T, M><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
-                        r0, r1, s == 0, L.view(), lu, b, out, zadd, sc, skip_if_s);
+                    launch_k(c, bilu_upper_kernel<BS, KK, T, M>, blocksFor(r1 - r0), kThreads, r0, r1, (int)(s == 0),
+                             L.view(), lu, b, out, zadd, sc, skip_if_s);
                 })));
     }
 }
@@ -2226,8 +2381,8 @@ void level_residual(Core& c, const Level& L, const T* x, const T* b, T* out, int
                     int skip_if_s)
 {
     WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "mg_residual", [&] {
-                mg_residual_kernel<BS, KK, T, M><<<blocksFor(L.nb), kThreads, 0, c.stream>>>(
-                    L.nb, r_zero, L.view(), level_a<M>(L), x, b, out, sc, skip_if_s);
+                launch_k(c, mg_residual_kernel<BS, KK, T, M>, blocksFor(L.nb), kThreads, L.nb, r_zero, L.view(),
+                         level_a<M>(L), x, b, out, sc, skip_if_s);
             })));
 }
 
@@ -2242,7 +2397,7 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     const Level& L = an.levels[l];
     if (L.coarsest) {
         launch(c, "mg_dense_apply", [&] {
-            dense_apply_kernel<T, M><<<1, kThreads, 0, c.stream>>>(L.n, level_inv<M>(L), r, z, sc, skip);
+            launch_k(c, dense_apply_kernel<T, M>, 1, kThreads, L.n, level_inv<M>(L), r, z, sc, skip);
         });
         return;
     }
@@ -2258,14 +2413,14 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     ilu_apply<T, M>(c, L, r, z, nullptr, sc, skip);
     level_residual<T, M>(c, L, z, r, t, L.stage_ptr.size() > 1 ? L.stage_ptr[1] : 0, sc, skip);
     launch(c, "mg_restrict", [&] {
-        mg_restrict_kernel<T><<<blocksFor(C.n), kThreads, 0, c.stream>>>(C.n, L.mptr->as<int>(), L.midx->as<int>(), t,
-                                                                          rc, sc, skip);
+        launch_k(c, mg_restrict_kernel<T>, blocksFor(C.n), kThreads, C.n, (const int*)L.mptr->as<int>(),
+                 (const int*)L.midx->as<int>(), (const T*)t, rc, sc, skip);
     });
     vcycle<T, M>(c, an, l + 1, rc, zc, sc, skip);
     // coarse correction z += P zc, then post-smoothing z += M^{-1} (r - A z)
     WITH_BS(L.bs, launch(c, "mg_prolong", [&] {
-                mg_prolong_kernel<BS, T><<<blocksFor(L.nb), kThreads, 0, c.stream>>>(
-                    L.nb, L.aggb->as<int>(), zc, z, an.mg_alpha, sc, skip);
+                launch_k(c, mg_prolong_kernel<BS, T>, blocksFor(L.nb), kThreads, L.nb, (const int*)L.aggb->as<int>(),
+                         (const T*)zc, z, an.mg_alpha, sc, skip);
             }));
     level_residual<T, M>(c, L, z, r, t, 0, sc, skip);
     ilu_apply<T, M>(c, L, t, w, z, sc, skip);
@@ -2309,20 +2464,26 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double 
         bicg_init_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.b, v.r, v.rhat, v.p, v.v, v.x, n, part, cnt, sc, tol * tol);
     });
     auto iteration = [&] {
-        launch(c, "bicg_p", [&] { bicg_p_kernel<T><<<blocksFor(n), kThreads, 0, c.stream>>>(v.r, v.v, v.p, n, sc); });
+        launch(c, "bicg_p", [&] {
+            launch_k(c, bicg_p_kernel<T>, blocksFor(n), kThreads, (const T*)v.r, (const T*)v.v, v.p, n,
+                     (const KScal*)sc);
+        });
         apply_pc<T>(c, an, v.p, v.ph, sc, 0, pc32);
         WITH_BS(L0.bs, WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_alpha", [&] {
-                    bicg_spmv_alpha_kernel<BS, KK, T><<<nbr, kThreads, 0, c.stream>>>(L0.view(), a, v.ph, v.rhat, v.v,
-                                                                                       L0.nb, part, cnt, sc);
+                    launch_k(c, bicg_spmv_alpha_kernel<BS, KK, T>, nbr, kThreads, L0.view(), a, (const T*)v.ph,
+                             (const T*)v.rhat, v.v, L0.nb, part, cnt, sc);
                 })));
-        launch(c, "bicg_s", [&] { bicg_s_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.r, v.v, v.s, n, part, cnt, sc); });
+        launch(c, "bicg_s", [&] {
+            launch_k(c, bicg_s_kernel<T>, nb, kThreads, (const T*)v.r, (const T*)v.v, v.s, n, part, cnt, sc);
+        });
         apply_pc<T>(c, an, v.s, v.sh, sc, 1, pc32);
         WITH_BS(L0.bs, WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_omega", [&] {
-                    bicg_spmv_omega_kernel<BS, KK, T><<<nbr, kThreads, 0, c.stream>>>(L0.view(), a, v.sh, v.s, v.t,
-                                                                                       L0.nb, part, cnt, sc);
+                    launch_k(c, bicg_spmv_omega_kernel<BS, KK, T>, nbr, kThreads, L0.view(), a, (const T*)v.sh,
+                             (const T*)v.s, v.t, L0.nb, part, cnt, sc);
                 })));
         launch(c, "bicg_xr", [&] {
-            bicg_xr_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.ph, v.sh, v.s, v.t, v.rhat, v.x, v.r, n, part, cnt, sc);
+            launch_k(c, bicg_xr_kernel<T>, nb, kThreads, (const T*)v.ph, (const T*)v.sh, (const T*)v.s,
+                     (const T*)v.t, (const T*)v.rhat, v.x, v.r, n, part, cnt, sc);
         });
     };
     // Graph of `check_every` iterations, captured once per analysis and
@@ -2416,6 +2577,7 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     const int check_every = std::max(1, c.param_i("linsolver_check_every", 8));
 
     if (!p->analysis || p->analysis->natural != natural) p->analysis = analyse(c, *p, natural);
+    c.pdl_launch = c.param_i("linsolver_pdl", 1) != 0;
     SolverAnalysis& an = *p->analysis;
     SolveResult res;
     if (!an.ok) return res;  // structurally missing diagonal: ILU(0) cannot factor
@@ -2464,7 +2626,7 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
             else to_float(c, L.lus64, L.lus32, L.vals);
             if (refine && !L.v32) L.v32 = c.allocN<float>((size_t)4 * (L.n > 0 ? L.n : 1));
         }
-        if (refine && !an.vec32) an.vec32 = c.allocN<float>((size_t)10 * n);
+        if (refine && !an.vec32) an.vec32 = c.allocN<float>((size_t)10 * vec_stride(n));
         if (refine) prepare_tail<float, float>(c, an);
         else prepare_tail<double, float>(c, an);
     } else {
