@@ -1115,71 +1115,101 @@ __global__ void mg_prolong_kernel(int nb, const int* __restrict__ aggb, const T*
     prolong_rows<B, T, false>(nb, aggb, zc, z, alpha, tid, nth);
 }
 
-// Inverse of the coarsest matrix (n <= kCoarsest unknowns) by Gauss-Jordan
-// with partial pivoting on [A | I], one thread block; A is expanded from its
-// block sliced ELL values.
+// Inverse of the coarsest matrix (n <= kCoarsest unknowns), one thread block,
+// in place in shared memory: Gauss-Jordan elimination with partial pivoting
+// (Numerical Recipes, gaussj, row pivots only).  Per pivot k: a warp finds
+// the largest |a_rk|, r >= k (the lowest r among equals) while every thread
+// copies column k; rows k and p are swapped and row k is divided by the
+// pivot; every other row r takes a_rj - a_kj f_r with f_r its entry in
+// column k (column k itself becomes -f_r / pivot).  The row swaps show up
+// as column swaps of the result, undone in reverse order when the inverse
+// is written out.  A zero or non-finite pivot sets *status.
 constexpr int kCoarsest = 128;
 
 template <int B>
-__global__ void dense_inverse_kernel(int nb, SellView m, const double* __restrict__ a, double* __restrict__ work,
-                                     double* __restrict__ inv, int* status)
+__global__ void __launch_bounds__(1024) dense_inverse_kernel(int nb, SellView m, const double* __restrict__ a,
+                                                             double* __restrict__ inv, int* status)
 {
     constexpr int BB = B * B;
-    __shared__ double factor[kCoarsest];
-    __shared__ int piv;
-    __shared__ double pval;
+    extern __shared__ __align__(16) double dsm[];
     const int n = nb * B;
-    const int w2 = 2 * n;
-    for (int idx = threadIdx.x; idx < n * w2; idx += blockDim.x) work[idx] = 0.0;
+    double* w = dsm;                  // n x n, row-major
+    double* colk = dsm + n * n;       // column k before the row swap
+    __shared__ int piv_row;
+    __shared__ int perm[kCoarsest];   // row swapped with k at step k
+    for (int i = threadIdx.x; i < n * n; i += blockDim.x) w[i] = 0.0;
     __syncthreads();
     for (int R = threadIdx.x; R < nb; R += blockDim.x) {
         const int lane = R & 31, sb = m.slice_ptr[R >> 5];
         for (int k = 0; k < m.len[R]; ++k) {
             const int J = m.col[sb + (k << 5) + lane];
             for (int i = 0; i < B; ++i)
-                for (int j = 0; j < B; ++j)
-                    work[(R * B + i) * w2 + J * B + j] = a[(size_t)(sb + (k << 5) + lane) * BB + i * B + j];
+                for (int j = 0; j < B; ++j) w[(R * B + i) * n + J * B + j] = a[(size_t)(sb + (k << 5) + lane) * BB + i * B + j];
         }
-        for (int i = 0; i < B; ++i) work[(R * B + i) * w2 + n + R * B + i] = 1.0;
     }
     __syncthreads();
     for (int k = 0; k < n; ++k) {
-        if (threadIdx.x == 0) {
-            int best = k;
-            double bv = fabs(work[k * w2 + k]);
-            for (int r = k + 1; r < n; ++r) {
-                const double v = fabs(work[r * w2 + k]);
-                if (v > bv) {
-                    bv = v;
-                    best = r;
+        for (int r = threadIdx.x; r < n; r += blockDim.x) colk[r] = w[r * n + k];
+        if (threadIdx.x < 32) {
+            double best = -1.0;
+            int bi = n;
+            for (int r = k + (int)threadIdx.x; r < n; r += 32) {
+                const double v = fabs(w[r * n + k]);
+                if (v > best) {
+                    best = v;
+                    bi = r;
                 }
             }
-            piv = best;
-            if (bv == 0.0) *status = 1;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (threadIdx.x == 0) {
+                piv_row = bi < n ? bi : k;
+                perm[k] = piv_row;
+                if (!(best > 0.0) || !isfinite(best)) *status = 1;
+            }
         }
         __syncthreads();
-        if (piv != k)
-            for (int j = threadIdx.x; j < w2; j += blockDim.x) {
-                const double t = work[k * w2 + j];
-                work[k * w2 + j] = work[piv * w2 + j];
-                work[piv * w2 + j] = t;
-            }
+        const int p = piv_row;
+        const double pv = colk[p];
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double tk = w[k * n + j], tp = w[p * n + j];
+            w[p * n + j] = tk;
+            w[k * n + j] = (j == k ? 1.0 : tp) / pv;
+        }
         __syncthreads();
-        if (threadIdx.x == 0) pval = work[k * w2 + k];
-        __syncthreads();
-        for (int j = threadIdx.x; j < w2; j += blockDim.x) work[k * w2 + j] /= pval;
-        __syncthreads();
-        for (int r = threadIdx.x; r < n; r += blockDim.x) factor[r] = work[r * w2 + k];
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < n * w2; idx += blockDim.x) {
-            const int r = idx / w2, j = idx - r * w2;
-            if (r != k) work[idx] -= factor[r] * work[k * w2 + j];
+        for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
+            const int r = i / n, j = i - r * n;
+            if (r == k) continue;
+            const double f = r == p ? colk[k] : colk[r];
+            w[i] = (j == k ? 0.0 : w[i]) - w[k * n + j] * f;
         }
         __syncthreads();
     }
-    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-        const int r = idx / n, j = idx - r * n;
-        inv[idx] = work[r * w2 + n + j];
+    // column j of the inverse is column src[j] of w: the swaps of steps
+    // n-1 .. 0 applied to the columns in turn
+    __shared__ int src[kCoarsest];
+    if (threadIdx.x == 0) {
+        for (int j = 0; j < n; ++j) src[j] = j;
+        for (int k = n - 1; k >= 0; --k) {
+            const int p = perm[k];
+            if (p != k) {
+                const int t = src[k];
+                src[k] = src[p];
+                src[p] = t;
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
+        const int r = i / n, j = i - r * n;
+        inv[i] = w[r * n + src[j]];
     }
 }
 
@@ -1528,7 +1558,7 @@ struct Level {
     {
         return SellView{sell_ptr->as<int>(), sell_col->as<int>(), sell_len->as<int>(), sell_dk->as<int>(), width};
     }
-    Buf work64, inv64, inv32;      // coarsest level
+    Buf inv64, inv32;              // coarsest level
 };
 
 struct SolverAnalysis {
@@ -1983,7 +2013,6 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
                     break;
                 }
                 Lc.coarsest = true;
-                Lc.work64 = c.allocN<double>((size_t)2 * nc_unk * nc_unk);
                 Lc.inv64 = c.allocN<double>((size_t)nc_unk * nc_unk);
                 break;
             }
@@ -2607,11 +2636,12 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     for (auto& L : an.levels) {
         if (L.coarsest) {
             WITH_BS(L.bs, launch(c, "mg_dense_inverse", [&] {
-                        dense_inverse_kernel<BS><<<1, 1024, 0, c.stream>>>(L.nb, L.view(), L.as64->as<double>(),
-                                                                           L.work64->as<double>(),
-                                                                           L.inv64->as<double>(),
-                                                                           an.factor_status->as<int>());
-                    }));
+                const size_t smem = ((size_t)L.n * L.n + L.n) * sizeof(double);
+                EQG_CUDA(cudaFuncSetAttribute(dense_inverse_kernel<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem));
+                dense_inverse_kernel<BS><<<1, 1024, smem, c.stream>>>(L.nb, L.view(), L.as64->as<double>(),
+                                                                     L.inv64->as<double>(), an.factor_status->as<int>());
+            }));
         } else {
             factor_level(c, L, an.factor_status->as<int>());
         }
