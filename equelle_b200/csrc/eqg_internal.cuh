@@ -69,6 +69,9 @@ struct Pattern {
     Buf rowptr;                 // int32[rows+1]
     Buf colind;                 // int32[nnz]
     Buf rowidx;                 // int32[nnz], built on demand (row of each entry)
+    // for a union pattern: per pair of operand patterns (ids), the position
+    // of each entry in either operand (-1: absent), int32[2 nnz]
+    std::map<std::pair<uint64_t, uint64_t>, Buf> merge_maps;
     std::shared_ptr<SolverAnalysis> analysis;  // linear-solver analysis, built on demand
 };
 using PatternP = std::shared_ptr<Pattern>;

@@ -294,6 +294,45 @@ __global__ void ew_merge_kernel(Rule r, int rows, const int* __restrict__ aptr, 
     }
 }
 
+// Position in each operand of every entry of the union pattern (-1: absent),
+// built once per operand pattern pair.
+__global__ void merge_map_kernel(int rows, const int* __restrict__ aptr, const int* __restrict__ acol,
+                                 const int* __restrict__ bptr, const int* __restrict__ bcol,
+                                 const int* __restrict__ optr, const int* __restrict__ ocol, int* __restrict__ ia,
+                                 int* __restrict__ ib)
+{
+    GRID_STRIDE(i, rows)
+    {
+        int pa = aptr ? aptr[i] : 0, ea = aptr ? aptr[i + 1] : 0;
+        int pb = bptr ? bptr[i] : 0, eb = bptr ? bptr[i + 1] : 0;
+        const int p1 = optr[i + 1];
+        for (int p = optr[i]; p < p1; ++p) {
+            const int c = ocol[p];
+            ia[p] = (pa < ea && acol[pa] == c) ? pa++ : -1;
+            ib[p] = (pb < eb && bcol[pb] == c) ? pb++ : -1;
+        }
+    }
+}
+
+// ew_merge_kernel through the position maps: one thread per nonzero, the
+// same operations in the same order.
+__global__ void ew_mapped_kernel(Rule r, const int* __restrict__ rowidx, const int* __restrict__ ia,
+                                 const int* __restrict__ ib, const double* __restrict__ ja,
+                                 const double* __restrict__ jb, double* __restrict__ out, int64_t nnz)
+{
+    GRID_STRIDE(e, nnz)
+    {
+        const int i = rowidx[e];
+        double wa, wb, post;
+        rule_weights(r, i, wa, wb, post);
+        const int xa = ia[e], xb = ib[e];
+        double acc = 0.0;
+        if (xa >= 0) acc += wa * ja[xa];
+        if (xb >= 0) acc += wb * jb[xb];
+        out[e] = post * acc;
+    }
+}
+
 // Union pattern of two patterns with the same shape.
 template <bool FILL>
 __global__ void union_kernel(int rows, const int* aptr, const int* acol, const int* bptr, const int* bcol,
@@ -567,6 +606,26 @@ void jacobian_elementwise(Core& c, const JacArgs& a, const Pattern& out, double*
         pattern_build_rowidx(c, const_cast<Pattern&>(out));
         launch(c, "jac_flat", [&] { ew_flat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(r, out.rowidx->as<int>(), a.pa ? a.ja : nullptr,
                                                                       a.pb ? a.jb : nullptr, jout, out.nnz); });
+    } else if (out.nnz < (int64_t)INT_MAX / 2) {
+        // through position maps kept with the output pattern
+        Pattern& o = const_cast<Pattern&>(out);
+        pattern_build_rowidx(c, o);
+        const auto key = std::make_pair(a.pa ? a.pa->id : 0, a.pb ? a.pb->id : 0);
+        Buf& maps = o.merge_maps[key];
+        if (!maps) {
+            maps = c.allocN<int>((size_t)2 * out.nnz);
+            launch(c, "merge_map", [&] {
+                merge_map_kernel<<<blocksFor(out.rows), kThreads, 0, c.stream>>>(
+                    out.rows, a.pa ? a.pa->rowptr->as<int>() : nullptr, a.pa ? a.pa->colind->as<int>() : nullptr,
+                    a.pb ? a.pb->rowptr->as<int>() : nullptr, a.pb ? a.pb->colind->as<int>() : nullptr,
+                    out.rowptr->as<int>(), out.colind->as<int>(), maps->as<int>(), maps->as<int>() + out.nnz);
+            });
+        }
+        launch(c, "jac_merge", [&] {
+            ew_mapped_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(
+                r, out.rowidx->as<int>(), maps->as<int>(), maps->as<int>() + out.nnz, a.pa ? a.ja : nullptr,
+                a.pb ? a.jb : nullptr, jout, out.nnz);
+        });
     } else {
         launch(c, "jac_merge", [&] { ew_merge_kernel<<<blocksFor(out.rows), kThreads, 0, c.stream>>>(
             r, out.rows, a.pa ? a.pa->rowptr->as<int>() : nullptr, a.pa ? a.pa->colind->as<int>() : nullptr,
