@@ -75,9 +75,11 @@ enum { ST_RUN = 0, ST_CONV = 1, ST_BREAK = 2 };
 
 __device__ __forceinline__ bool stopped(const KScal* sc) { return sc->status != ST_RUN; }
 
-// First statement of every kernel of a BiCGStab iteration: those kernels are
-// launched as programmatic dependent launches (launch_k), so their blocks may
-// be scheduled while the kernel before them on the stream still runs; this
+// Every kernel of a BiCGStab iteration calls this before it reads anything
+// that an earlier kernel wrote (first thing, except for the fused coarse
+// cycle's prefetches of constant data): those kernels are launched as
+// programmatic dependent launches (launch_k), so their blocks may be
+// scheduled while the kernel before them on the stream still runs; this
 // waits until that kernel has completed and its writes are visible (at once
 // when the kernel was launched normally).
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
@@ -1461,17 +1463,23 @@ template <int B, int KM, class T, class M>
 __global__ void __launch_bounds__(kTailThreads)
     mg_tail_kernel(const __grid_constant__ TailParams<T, M> p, const T* r_top, T* z_top, const KScal* sc, int skip_if_s)
 {
-    pdl_wait();
     constexpr bool U = KM > 0;  // slices of uniform width (unrolled rows only)
     extern __shared__ __align__(16) unsigned char tail_smem[];
-    if (mg_skip(sc, skip_if_s)) return;
+    // the levels' matrices and index arrays do not change during a solve:
+    // their L2 prefetches and shared-memory copies start before the wait for
+    // the previous kernel
+    const int lf = p.local_first < p.nlev ? p.local_first : p.nlev;
+    if (lf < p.nlev && blockIdx.x == 0) start_local_copies(p.copies, p.ncopies, tail_smem);
+    prefetch_regions(p.reg, p.nregions);
+    pdl_wait();
+    if (mg_skip(sc, skip_if_s)) {
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        return;
+    }
     long long* const trace = p.trace;
     int tk = 0;
     if (trace != nullptr && blockIdx.x == 0 && threadIdx.x == 0) trace[tk] = clock64();
     ++tk;
-    const int lf = p.local_first < p.nlev ? p.local_first : p.nlev;
-    if (lf < p.nlev && blockIdx.x == 0) start_local_copies(p.copies, p.ncopies, tail_smem);
-    prefetch_regions(p.reg, p.nregions);
     // rows go to threads a warp (one slice of 32 rows) at a time, round robin
     // over the cluster's blocks, so that a step of a few slices still spreads
     // over every SM of the cluster
