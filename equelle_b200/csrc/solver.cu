@@ -1117,6 +1117,55 @@ __global__ void mg_prolong_kernel(int nb, const int* __restrict__ aggb, const T*
     prolong_rows<B, T, false>(nb, aggb, zc, z, alpha, tid, nth);
 }
 
+// The coarse correction of a level that stores A P (A times the
+// piecewise-constant prolongation; blocks of each fine block row summed per
+// coarse block column, about 4 per row against 7 in A).  With t = r - A z
+// left by the down-leg:
+//   t -= alpha (A P) zc   (= r - A (z + alpha P zc), by linearity)
+//   z += alpha P zc       (as prolong_rows)
+// one pass over A P instead of the prolongation and a pass over A.
+template <int B, int KM, class T, class M>
+__global__ void mg_correct_kernel(int nb, SellView ap, const M* __restrict__ apv, const int* __restrict__ aggb,
+                                  const T* __restrict__ zc, T* __restrict__ z, T* __restrict__ t, double alpha,
+                                  const KScal* sc, int skip_if_s)
+{
+    pdl_wait();
+    if (mg_skip(sc, skip_if_s)) return;
+    THREAD_RANGE;
+    for (int R = tid; R < nb; R += nth) {
+        double acc[B];
+#pragma unroll
+        for (int c = 0; c < B; ++c) acc[c] = 0.0;
+        bdot<B, KM, T, M>(ap, ap.slice_ptr[R >> 5], R & 31, 0, ap.len[R], apv, zc, zc, INT_MAX, acc);
+        double tv[B];
+        load_bvec<B, T>(t, R, tv);
+#pragma unroll
+        for (int c = 0; c < B; ++c) tv[c] -= alpha * acc[c];
+        store_bvec<B, T>(t, R, tv);
+        double e[B];
+        load_bvec<B, T>(zc, aggb[R], e);
+#pragma unroll
+        for (int c = 0; c < B; ++c) e[c] *= alpha;
+        update_z<B, T, false>(z, R, e);
+    }
+}
+
+// Values of A P: slot q of A P is the sum, value by value, of the A slots
+// gidx[gptr[q] .. gptr[q + 1]) (ascending); padding slots get 0.
+__global__ void ap_values_kernel(int64_t slots, int bb, const int* __restrict__ gptr, const int* __restrict__ gidx,
+                                 const double* __restrict__ a, double* __restrict__ ap)
+{
+    GRID_STRIDE(i, slots * bb)
+    {
+        const int64_t q = i / bb;
+        const int e = (int)(i - q * bb);
+        double s = 0.0;
+        const int g1 = gptr[q + 1];
+        for (int g = gptr[q]; g < g1; ++g) s += a[(int64_t)gidx[g] * bb + e];
+        ap[i] = s;
+    }
+}
+
 // Inverse of the coarsest matrix (n <= kCoarsest unknowns), one thread block,
 // in place in shared memory: Gauss-Jordan elimination with partial pivoting
 // (Numerical Recipes, gaussj, row pivots only).  Per pivot k: a warp finds
@@ -1552,6 +1601,19 @@ struct Level {
     Buf perm;                      // permuted unknown position -> natural unknown
     Buf gptr, gidx, gpos;          // Galerkin gather from the finer level's values (levels > 0)
     Buf aggb;                      // coarse block row of each block row (next coarser level)
+    // A P (see mg_correct_kernel), in the same sliced layout: slots, the
+    // longest row, slices, coarse block columns, row lengths, and the A slots
+    // summed into each slot (gptr/gidx); levels above linsolver_mg_ap_rows
+    int64_t ap_slots = 0;
+    int ap_kmax = 0;
+    Buf ap_sp, ap_col, ap_len, ap_gptr, ap_gidx, ap64, ap32;
+    SellView ap_view() const
+    {
+        return SellView{ap_sp->as<int>(), ap_col->as<int>(), ap_len->as<int>(), ap_len->as<int>(), 0};
+    }
+    // host copies of the slices, columns and row lengths while the
+    // hierarchy is built
+    std::vector<int> h_sp, h_col, h_len;
     Buf mptr, midx;                // aggregate members (unknown positions) of each coarse unknown
     Buf mpad;                      // the same, kMembers per coarse unknown, -1 past the last (or none)
     int64_t sell_size = 0;         // slots of the block sliced ELL layout
@@ -1828,6 +1890,9 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
     L.blocks = pptr[nb];
     L.sell_ptr = upload_ints(c, sp);
     L.sell_col = upload_ints(c, scol);
+    L.h_sp = sp;
+    L.h_col = scol;
+    L.h_len = len;
     L.sell_len = upload_ints(c, len);
     L.sell_dk = upload_ints(c, dk);
     const size_t nv = (size_t)(L.vals > 0 ? L.vals : 1);
@@ -1835,6 +1900,81 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
     L.lus64 = c.allocN<double>(nv);
     L.perm = upload_ints(c, perm);
     L.v64 = c.allocN<double>((size_t)4 * (n > 0 ? n : 1));
+}
+
+// A P of level L (see mg_correct_kernel): for every block row, its coarse
+// block columns (aggregates of its columns, ascending) in slices of 32 rows,
+// and for every slot the A slots it sums.
+void build_ap(Core& c, Level& L, const std::vector<int>& aggb)
+{
+    const int nb = L.nb;
+    const int nsl = (nb + 31) / 32;
+    std::vector<int> alen(nb > 0 ? nb : 1, 0);
+    std::vector<int> rowq((size_t)nb * 16);  // coarse columns of each row (at most its A row length)
+    int kmax = 0;
+    bool ok = true;
+#pragma omp parallel for reduction(max : kmax) reduction(&& : ok) schedule(static)
+    for (int R = 0; R < nb; ++R) {
+        const int base = L.h_sp[R / 32] + (R % 32);
+        int q[64];
+        int nq = 0;
+        for (int k = 0; k < L.h_len[R]; ++k) {
+            const int P = aggb[L.h_col[base + 32 * k]];
+            bool seen = false;
+            for (int j = 0; j < nq; ++j) seen = seen || q[j] == P;
+            if (!seen && nq < 64) q[nq++] = P;
+        }
+        std::sort(q, q + nq);
+        if (nq > 16) ok = false;
+        alen[R] = nq;
+        kmax = std::max(kmax, nq);
+        for (int j = 0; j < nq && j < 16; ++j) rowq[(size_t)R * 16 + j] = q[j];
+    }
+    if (!ok) return;  // rows of more than 16 coarse columns: keep the plain up-leg
+    std::vector<int> asp(nsl + 1, 0);
+    for (int sl = 0; sl < nsl; ++sl) {
+        int w = 0;
+        for (int R = sl * 32; R < std::min(nb, sl * 32 + 32); ++R) w = std::max(w, alen[R]);
+        asp[sl + 1] = asp[sl] + 32 * w;
+    }
+    const int64_t slots = asp[nsl];
+    std::vector<int> acol(slots > 0 ? slots : 1, 0), cnt(slots + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (int R = 0; R < nb; ++R) {
+        const int abase = asp[R / 32] + (R % 32);
+        const int w = (asp[R / 32 + 1] - asp[R / 32]) / 32;
+        const int base = L.h_sp[R / 32] + (R % 32);
+        for (int j = 0; j < w; ++j) acol[abase + 32 * j] = j < alen[R] ? rowq[(size_t)R * 16 + j] : aggb[R];
+        for (int k = 0; k < L.h_len[R]; ++k) {
+            const int P = aggb[L.h_col[base + 32 * k]];
+            const int j = (int)(std::lower_bound(&rowq[(size_t)R * 16], &rowq[(size_t)R * 16] + alen[R], P) -
+                                &rowq[(size_t)R * 16]);
+            cnt[abase + 32 * j + 1]++;  // one writer per slot: slots belong to one row
+        }
+    }
+    for (int64_t q = 0; q < slots; ++q) cnt[q + 1] += cnt[q];
+    std::vector<int> gidx(cnt[slots] > 0 ? cnt[slots] : 1);
+#pragma omp parallel for schedule(static)
+    for (int R = 0; R < nb; ++R) {
+        const int abase = asp[R / 32] + (R % 32);
+        const int base = L.h_sp[R / 32] + (R % 32);
+        int fill[16] = {0};
+        for (int k = 0; k < L.h_len[R]; ++k) {
+            const int P = aggb[L.h_col[base + 32 * k]];
+            const int j = (int)(std::lower_bound(&rowq[(size_t)R * 16], &rowq[(size_t)R * 16] + alen[R], P) -
+                                &rowq[(size_t)R * 16]);
+            const int q = abase + 32 * j;
+            gidx[cnt[q] + fill[j]++] = base + 32 * k;
+        }
+    }
+    L.ap_slots = slots;
+    L.ap_kmax = kmax;
+    L.ap_sp = upload_ints(c, asp);
+    L.ap_col = upload_ints(c, acol);
+    L.ap_len = upload_ints(c, alen);
+    L.ap_gptr = upload_ints(c, cnt);
+    L.ap_gidx = upload_ints(c, gidx);
+    L.ap64 = c.allocN<double>((size_t)(slots > 0 ? slots : 1) * L.bs * L.bs);
 }
 
 std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
@@ -1880,6 +2020,7 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     const double t_copy = since();
     // levels small enough for the fused coarse cycle get slices of uniform width
     const int fuse_rows = c.param_i("linsolver_mg_fuse_rows", 40000);
+    const int ap_rows = c.param_i("linsolver_mg_ap_rows", 40000);
     order_level(c, A, natural, bs, n <= fuse_rows, an->levels[0], perm, iperm, vpos, an->ok);
     const double t_level0 = since();
     {
@@ -1968,7 +2109,11 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
                         if (aggp[R * bs + cc] != aggb[R] * bs + cc) fail(EQG_ERR_DEVICE, "aggregation splits a block");
                 }
                 Lf.aggb = upload_ints(c, aggb);
+                if (Lf.n > ap_rows) build_ap(c, Lf, aggb);
             }
+            Lf.h_sp.clear();
+            Lf.h_col.clear();
+            Lf.h_len.clear();
             Lf.mptr = upload_ints(c, mptr);
             Lf.midx = upload_ints(c, midx);
             if (max_members <= kMembers) {
@@ -2048,6 +2193,11 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             for (int l = an->tail_first; l < nl; ++l)
                 if (!an->levels[l].coarsest) an->tail_kmax = std::max(an->tail_kmax, an->levels[l].kmax);
     }
+    for (auto& L : an->levels) {
+        L.h_sp.clear();
+        L.h_col.clear();
+        L.h_len.clear();
+    }
     an->vec64 = c.allocN<double>((size_t)10 * vec_stride(n));
     an->scal = c.alloc(sizeof(KScal));
     an->partials = c.allocN<double>((size_t)kRedBlocks * 2);
@@ -2113,6 +2263,12 @@ template <>
 const double* level_inv<double>(const Level& L) { return L.inv64->as<double>(); }
 template <>
 const float* level_inv<float>(const Level& L) { return L.inv32->as<float>(); }
+template <class T>
+const T* level_ap(const Level& L);
+template <>
+const double* level_ap<double>(const Level& L) { return L.ap64->as<double>(); }
+template <>
+const float* level_ap<float>(const Level& L) { return L.ap32->as<float>(); }
 
 // Precision of a preconditioner application: vectors T, matrix values M.
 // [0] FP64, [1] FP32 (inner solve of "refine"), [2] FP64 vectors with FP32
@@ -2454,12 +2610,20 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
                  (const int*)L.midx->as<int>(), (const T*)t, rc, sc, skip);
     });
     vcycle<T, M>(c, an, l + 1, rc, zc, sc, skip);
-    // coarse correction z += P zc, then post-smoothing z += M^{-1} (r - A z)
-    WITH_BS(L.bs, launch(c, "mg_prolong", [&] {
-                launch_k(c, mg_prolong_kernel<BS, T>, blocksFor(L.nb), kThreads, L.nb, (const int*)L.aggb->as<int>(),
-                         (const T*)zc, z, an.mg_alpha, sc, skip);
-            }));
-    level_residual<T, M>(c, L, z, r, t, 0, sc, skip);
+    // coarse correction z += alpha P zc and its residual t = r - A z, then
+    // post-smoothing z += M^{-1} t
+    if (L.ap_slots > 0) {
+        WITH_BS(L.bs, WITH_KMAX(L.ap_kmax, launch(c, "mg_correct", [&] {
+                    launch_k(c, mg_correct_kernel<BS, KK, T, M>, blocksFor(L.nb), kThreads, L.nb, L.ap_view(),
+                             level_ap<M>(L), (const int*)L.aggb->as<int>(), (const T*)zc, z, t, an.mg_alpha, sc, skip);
+                })));
+    } else {
+        WITH_BS(L.bs, launch(c, "mg_prolong", [&] {
+                    launch_k(c, mg_prolong_kernel<BS, T>, blocksFor(L.nb), kThreads, L.nb,
+                             (const int*)L.aggb->as<int>(), (const T*)zc, z, an.mg_alpha, sc, skip);
+                }));
+        level_residual<T, M>(c, L, z, r, t, 0, sc, skip);
+    }
     ilu_apply<T, M>(c, L, t, w, z, sc, skip);
 }
 
@@ -2640,6 +2804,14 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
                                                                          C.as64->as<double>());
         });
     }
+    for (auto& L : an.levels)
+        if (L.ap_slots > 0) {
+            launch(c, "mg_ap_values", [&] {
+                ap_values_kernel<<<blocksFor(L.ap_slots * L.bs * L.bs), kThreads, 0, c.stream>>>(
+                    L.ap_slots, L.bs * L.bs, L.ap_gptr->as<int>(), L.ap_gidx->as<int>(), L.as64->as<double>(),
+                    L.ap64->as<double>());
+            });
+        }
     EQG_CUDA(cudaMemsetAsync(an.factor_status->ptr, 0, sizeof(int), c.stream));
     for (auto& L : an.levels) {
         if (L.coarsest) {
@@ -2660,6 +2832,7 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     if (mixed || refine) {
         for (auto& L : an.levels) {
             to_float(c, L.as64, L.as32, L.vals);
+            if (L.ap_slots > 0) to_float(c, L.ap64, L.ap32, L.ap_slots * L.bs * L.bs);
             if (L.coarsest) to_float(c, L.inv64, L.inv32, (int64_t)L.n * L.n);
             else to_float(c, L.lus64, L.lus32, L.vals);
             if (refine && !L.v32) L.v32 = c.allocN<float>((size_t)4 * (L.n > 0 ? L.n : 1));
