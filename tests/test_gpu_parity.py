@@ -10,6 +10,10 @@ from parity import assert_colls, assert_values
 
 pytestmark = pytest.mark.gpu
 
+# the V-cycle's up-leg through A P on every level outside the fused cycle,
+# and no fused levels (the defaults take it only above 40000 unknowns)
+AP_EVERYWHERE = dict(linsolver_mg_ap_rows=0, linsolver_mg_fuse_rows=0)
+
 
 def test_gpu_grid_4x3_golden(gpu_lib):
     kat.check_grid_4x3(gpu_lib)
@@ -62,14 +66,18 @@ def test_topology_parity(gpu_lib, oracle_lib, grid):
         assert np.array_equal(g.normal(g.allFaces())[d].value(), o.normal(o.allFaces())[d].value())
 
 
-@pytest.mark.parametrize("ordering,precond", [("multicolor", "multigrid"), ("multicolor", "ilu0"),
-                                              ("natural", "ilu0"), ("natural", "multigrid")])
-def test_heat_64x64_parity(gpu_lib, oracle_lib, ordering, precond):
-    """Implicit heat equation, 64x64, 20 steps: fields within 1e-9 relative."""
+@pytest.mark.parametrize("ordering,precond,extra", [("multicolor", "multigrid", {}), ("multicolor", "ilu0", {}),
+                                                    ("natural", "ilu0", {}), ("natural", "multigrid", {}),
+                                                    ("natural", "multigrid", AP_EVERYWHERE),
+                                                    ("multicolor", "multigrid", AP_EVERYWHERE)],
+                         ids=["mc-mg", "mc-ilu0", "nat-ilu0", "nat-mg", "nat-mg-ap", "mc-mg-ap"])
+def test_heat_64x64_parity(gpu_lib, oracle_lib, ordering, precond, extra):
+    """Implicit heat equation, 64x64, 20 steps: fields within 1e-9 relative
+    (scalar unknowns; with the A P up-leg on every launch-path level too)."""
     grid, case = programs.heat_case(64, 64, steps=20)
     params = dict(grid, abs_res_tol=1e-10, linsolver_residual_tolerance=1e-12)
     og = programs.heat_equation(Runtime(gpu_lib, dict(params, linsolver_ordering=ordering,
-                                                      linsolver_preconditioner=precond)), 0.3, 1.0, **case)
+                                                      linsolver_preconditioner=precond, **extra)), 0.3, 1.0, **case)
     oo = programs.heat_equation(Runtime(oracle_lib, params), 0.3, 1.0, **case)
     for step, (a, b) in enumerate(zip(og, oo)):
         assert np.max(np.abs(a - b) / np.abs(b)) <= 1e-9, "step %d" % step
@@ -136,7 +144,8 @@ def reaction_diffusion3(er, fields, rates, timesteps):
     return out
 
 
-@pytest.mark.parametrize("shape,precond", [((12, 10, 6), "multigrid"), ((12, 10, 6), "ilu0"), ((40, 30, None), "multigrid")])
+@pytest.mark.parametrize("shape,precond", [((12, 10, 6), "multigrid"), ((12, 10, 6), "ilu0"), ((40, 30, None), "multigrid"),
+                                           ((12, 10, 6), "multigrid-ap")])
 def test_three_species_blocks_parity(gpu_lib, oracle_lib, shape, precond):
     """A 3-unknowns-per-cell system (3 x 3 block ILU(0)): every species
     within 1e-9 relative of the FP64 oracle after every step."""
@@ -147,7 +156,9 @@ def test_three_species_blocks_parity(gpu_lib, oracle_lib, shape, precond):
     fields = [1.0 + rng.rand(n), 0.5 + rng.rand(n), 0.1 * rng.rand(n)]
     args = (fields, (2.0, 0.5, (1.0, 0.3, 0.05)), [0.1, 0.2, 0.2])
     params = dict(grid, abs_res_tol=1e-12, linsolver_residual_tolerance=1e-12, linsolver_max_iterations=5000)
-    og = reaction_diffusion3(Runtime(gpu_lib, dict(params, linsolver_preconditioner=precond)), *args)
+    extra = AP_EVERYWHERE if precond.endswith("-ap") else {}
+    og = reaction_diffusion3(Runtime(gpu_lib, dict(params, linsolver_preconditioner=precond.split("-")[0], **extra)),
+                             *args)
     oo = reaction_diffusion3(Runtime(oracle_lib, params), *args)
     for step, (g, o) in enumerate(zip(og, oo)):
         for k in range(3):
