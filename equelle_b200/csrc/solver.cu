@@ -2005,7 +2005,9 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     if (pre != "multigrid" && pre != "ilu0") fail(EQG_ERR_ARG, "linsolver_preconditioner must be multigrid or ilu0");
     // unknowns stacked as ncomp collections over all cells
     const int ncomp = (c.nc > 0 && n % c.nc == 0) ? n / c.nc : 0;
-    const bool mg_wanted = pre == "multigrid" && ncomp >= 1 && ncomp <= 8 && n > kCoarsest;
+    // coarsening stops at linsolver_mg_coarsest unknowns (at most kCoarsest)
+    const int coarsest = std::max(1, std::min(kCoarsest, c.param_i("linsolver_mg_coarsest", kCoarsest)));
+    const bool mg_wanted = pre == "multigrid" && ncomp >= 1 && ncomp <= 8 && n > coarsest;
     // Block ILU(0) sweeps with FP32 vectors (precision "refine") converge much
     // more slowly than scalar ones on the two-phase systems; with FP64
     // vectors, FP32 matrix values ("mixed") do not change the iteration
@@ -2159,7 +2161,7 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             Lc.gidx = upload_ints(c, gidx);
             Lc.gpos = upload_ints(c, cvpos);
             Lc.nnz = cnnz;
-            if (nc_unk <= kCoarsest || (ccx == 1 && ccy == 1 && ccz == 1)) {
+            if (nc_unk <= coarsest || (ccx == 1 && ccy == 1 && ccz == 1)) {
                 if (nc_unk > kCoarsest) {
                     an->multigrid = false;  // cannot coarsen further and too large to invert
                     an->levels.resize(1);

@@ -126,7 +126,9 @@ const char* eqg_backend_name(void);
  * linsolver_mg_alpha (factor of the coarse-grid correction z += alpha P zc;
  * 1.4 on 3D grids, 1.9 on 2D grids), linsolver_mg_ap_rows (40000: levels
  * with more unknowns correct their residual through A P instead of
- * recomputing r - A z), linsolver_pdl (1: the BiCGStab iteration's kernels
+ * recomputing r - A z), linsolver_mg_coarsest (128: coarsening stops at
+ * this many unknowns, at most 128; that level is solved with a dense
+ * inverse), linsolver_pdl (1: the BiCGStab iteration's kernels
  * as programmatic dependent launches; 0: plain launches), linsolver_mg_local (1: that kernel keeps its coarsest levels in one thread
  * block's shared memory while they fit in 200 KB; 0: off),
  * linsolver_tail_trace (0; 1: print the SM clock cycles of every step of the
