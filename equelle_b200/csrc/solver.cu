@@ -570,17 +570,19 @@ __device__ __forceinline__ void upper_rows(int r0, int r1, int first, const Sell
     }
 }
 
-// out = b - A x.  Block rows below r_zero get 0 without being computed:
-// after a full ILU(0) sweep their residual is zero (see vcycle).
-template <int B, int KM, class T, class M, bool CG, bool U = false>
+// out = b - A x.  Block rows below r_zero are not computed: after a full
+// ILU(0) sweep their residual is zero (see vcycle).  With ZW they get 0;
+// without, they are left as they are, for readers that skip them.
+template <int B, int KM, class T, class M, bool CG, bool U = false, bool ZW = true>
 __device__ __forceinline__ void residual_rows(int nb, int r_zero, const SellView& m, const M* __restrict__ a,
                                               const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ out,
                                               int tid, int nth)
 {
     for (int R = tid; R < nb; R += nth) {
         if (R < r_zero) {
+            if (ZW)
 #pragma unroll
-            for (int c = 0; c < B; ++c) out[R * B + c] = (T)0;
+                for (int c = 0; c < B; ++c) out[R * B + c] = (T)0;
             continue;
         }
         double acc[B];
@@ -601,9 +603,12 @@ __device__ __forceinline__ void residual_rows(int nb, int r_zero, const SellView
 // latency of that chain, not by its bytes.
 constexpr int kMembers = 8;
 
+// Members below t_zero (positions whose t is zero and was not written, see
+// residual_rows) are skipped: the same sums as adding their zeros.
 template <class T, bool CG>
 __device__ __forceinline__ void restrict_rows(int nc, const int* __restrict__ mptr, const int* __restrict__ midx,
-                                              const T* __restrict__ t, T* __restrict__ rc, int tid, int nth)
+                                              const T* __restrict__ t, int t_zero, T* __restrict__ rc, int tid,
+                                              int nth)
 {
     for (int P = tid; P < nc; P += nth) {
         double s = 0.0;
@@ -611,16 +616,17 @@ __device__ __forceinline__ void restrict_rows(int nc, const int* __restrict__ mp
         if (k1 - k0 <= kMembers) {
             int mi[kMembers];
 #pragma unroll
-            for (int j = 0; j < kMembers; ++j) mi[j] = k0 + j < k1 ? midx[k0 + j] : 0;
+            for (int j = 0; j < kMembers; ++j) mi[j] = k0 + j < k1 ? midx[k0 + j] : -1;
             double tv[kMembers];
 #pragma unroll
             for (int j = 0; j < kMembers; ++j)
-                tv[j] = k0 + j < k1 ? (double)(CG ? __ldcg(t + mi[j]) : t[mi[j]]) : 0.0;
+                tv[j] = mi[j] >= t_zero ? (double)(CG ? __ldcg(t + mi[j]) : t[mi[j]]) : 0.0;
 #pragma unroll
             for (int j = 0; j < kMembers; ++j)
-                if (k0 + j < k1) s += tv[j];
+                if (mi[j] >= t_zero) s += tv[j];
         } else {
-            for (int k = k0; k < k1; ++k) s += (double)(CG ? __ldcg(t + midx[k]) : t[midx[k]]);
+            for (int k = k0; k < k1; ++k)
+                if (midx[k] >= t_zero) s += (double)(CG ? __ldcg(t + midx[k]) : t[midx[k]]);
         }
         rc[P] = (T)s;
     }
@@ -1094,17 +1100,18 @@ __global__ void mg_residual_kernel(int nb, int r_zero, SellView m, const M* __re
     pdl_wait();
     if (mg_skip(sc, skip_if_s)) return;
     THREAD_RANGE;
-    residual_rows<B, KM, T, M, false>(nb, r_zero, m, a, x, b, out, tid, nth);
+    residual_rows<B, KM, T, M, false, false, false>(nb, r_zero, m, a, x, b, out, tid, nth);
 }
 
 template <class T>
 __global__ void mg_restrict_kernel(int nc, const int* __restrict__ mptr, const int* __restrict__ midx,
-                                   const T* __restrict__ t, T* __restrict__ rc, const KScal* sc, int skip_if_s)
+                                   const T* __restrict__ t, int t_zero, T* __restrict__ rc, const KScal* sc,
+                                   int skip_if_s)
 {
     pdl_wait();
     if (mg_skip(sc, skip_if_s)) return;
     THREAD_RANGE;
-    restrict_rows<T, false>(nc, mptr, midx, t, rc, tid, nth);
+    restrict_rows<T, false>(nc, mptr, midx, t, t_zero, rc, tid, nth);
 }
 
 template <int B, class T>
@@ -1121,13 +1128,14 @@ __global__ void mg_prolong_kernel(int nb, const int* __restrict__ aggb, const T*
 // piecewise-constant prolongation; blocks of each fine block row summed per
 // coarse block column, about 4 per row against 7 in A).  With t = r - A z
 // left by the down-leg:
-//   t -= alpha (A P) zc   (= r - A (z + alpha P zc), by linearity)
+//   t -= alpha (A P) zc   (= r - A (z + alpha P zc), by linearity; the
+//                          rows below r_zero of t are zero, not stored)
 //   z += alpha P zc       (as prolong_rows)
 // one pass over A P instead of the prolongation and a pass over A.
 template <int B, int KM, class T, class M>
-__global__ void mg_correct_kernel(int nb, SellView ap, const M* __restrict__ apv, const int* __restrict__ aggb,
-                                  const T* __restrict__ zc, T* __restrict__ z, T* __restrict__ t, double alpha,
-                                  const KScal* sc, int skip_if_s)
+__global__ void mg_correct_kernel(int nb, int r_zero, SellView ap, const M* __restrict__ apv,
+                                  const int* __restrict__ aggb, const T* __restrict__ zc, T* __restrict__ z,
+                                  T* __restrict__ t, double alpha, const KScal* sc, int skip_if_s)
 {
     pdl_wait();
     if (mg_skip(sc, skip_if_s)) return;
@@ -1138,7 +1146,12 @@ __global__ void mg_correct_kernel(int nb, SellView ap, const M* __restrict__ apv
         for (int c = 0; c < B; ++c) acc[c] = 0.0;
         bdot<B, KM, T, M>(ap, ap.slice_ptr[R >> 5], R & 31, 0, ap.len[R], apv, zc, zc, INT_MAX, acc);
         double tv[B];
-        load_bvec<B, T>(t, R, tv);
+        if (R < r_zero) {  // zero, not stored (residual_rows without ZW)
+#pragma unroll
+            for (int c = 0; c < B; ++c) tv[c] = 0.0;
+        } else {
+            load_bvec<B, T>(t, R, tv);
+        }
 #pragma unroll
         for (int c = 0; c < B; ++c) tv[c] -= alpha * acc[c];
         store_bvec<B, T>(t, R, tv);
@@ -2605,11 +2618,14 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     // lower part and were solved last, against the final z of every other
     // stage, with their rows of A unchanged by the factorization
     // (D_R^{-1} = A_RR^{-1}, U_RJ = A_RJ): their residual r - A z is zero.
+    // Those rows of t are not stored: the restriction skips them and the
+    // A P up-leg takes them as zero.
+    const int r_zero = L.stage_ptr.size() > 1 ? L.stage_ptr[1] : 0;
     ilu_apply<T, M>(c, L, r, z, nullptr, sc, skip);
-    level_residual<T, M>(c, L, z, r, t, L.stage_ptr.size() > 1 ? L.stage_ptr[1] : 0, sc, skip);
+    level_residual<T, M>(c, L, z, r, t, r_zero, sc, skip);
     launch(c, "mg_restrict", [&] {
         launch_k(c, mg_restrict_kernel<T>, blocksFor(C.n), kThreads, C.n, (const int*)L.mptr->as<int>(),
-                 (const int*)L.midx->as<int>(), (const T*)t, rc, sc, skip);
+                 (const int*)L.midx->as<int>(), (const T*)t, r_zero * L.bs, rc, sc, skip);
     });
     vcycle<T, M>(c, an, l + 1, rc, zc, sc, skip);
     // coarse correction z += alpha P zc and its residual t = r - A z, then
@@ -2618,7 +2634,7 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     // and the iterations per time step rose from 203 to 254 (128x128x64)
     if (L.ap_slots > 0 && sizeof(T) == sizeof(double)) {
         WITH_BS(L.bs, WITH_KMAX(L.ap_kmax, launch(c, "mg_correct", [&] {
-                    launch_k(c, mg_correct_kernel<BS, KK, T, M>, blocksFor(L.nb), kThreads, L.nb, L.ap_view(),
+                    launch_k(c, mg_correct_kernel<BS, KK, T, M>, blocksFor(L.nb), kThreads, L.nb, r_zero, L.ap_view(),
                              level_ap<M>(L), (const int*)L.aggb->as<int>(), (const T*)zc, z, t, an.mg_alpha, sc, skip);
                 })));
     } else {
@@ -2779,7 +2795,11 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         fail(EQG_ERR_ARG, "linsolver_precision must be double, mixed or refine");
     const double tol = c.param_d("linsolver_residual_tolerance", 1e-8);
     const int max_iter = c.param_i("linsolver_max_iterations", 1000);
-    const int check_every = std::max(1, c.param_i("linsolver_check_every", 8));
+    // iterations per graph launch between host convergence checks: after
+    // convergence the rest of a chunk still launches (its kernels return at
+    // once); on 128x128x64, 4 beat 8 and 16 (72.7, 73.3, 74.2 ms of Krylov
+    // time per step)
+    const int check_every = std::max(1, c.param_i("linsolver_check_every", 4));
 
     if (!p->analysis || p->analysis->natural != natural) p->analysis = analyse(c, *p, natural);
     c.pdl_launch = c.param_i("linsolver_pdl", 1) != 0;

@@ -118,7 +118,7 @@ const char* eqg_backend_name(void);
  * ilu0), linsolver_ordering (multicolor | natural),
  * linsolver_precision (double | mixed: FP32 preconditioner | refine: FP32
  * BiCGStab inside FP64 refinement), linsolver_inner_tolerance (1e-4) and
- * linsolver_max_sweeps (60) for refine, linsolver_check_every (8),
+ * linsolver_max_sweeps (60) for refine, linsolver_check_every (4),
  * linsolver_block (1: ncomp x ncomp block ILU(0) for 2 or 3 unknowns per
  * cell; 0: scalar ILU(0)), linsolver_mg_fuse_rows (40000: the V-cycle
  * levels up to this size run as one kernel; 0: none), linsolver_mg_cluster
