@@ -1795,6 +1795,8 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
     const int nb = n / bs;
     const int bb = bs * bs;
     const int64_t nnz = A.ptr[n];
+    const auto t0 = std::chrono::steady_clock::now();
+    auto ms = [&] { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); };
     // block graph (natural block numbering), sorted, with the diagonal
     HostCsr G;
     build_rows(nb, bs * max_row(A) + 1, G, [&](int R, int* buf) {
@@ -1816,7 +1818,9 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
         }
         if (!all) ok = false;
     }
+    const double tg = ms();
     const std::vector<int> key = stage_keys(G, natural);
+    const double tk = ms();
     const int nst = nb > 0 ? *std::max_element(key.begin(), key.end()) + 1 : 0;
     L.stage_ptr.assign(nst + 1, 0);
     for (int R = 0; R < nb; ++R) L.stage_ptr[key[R] + 1]++;
@@ -1835,6 +1839,7 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
             perm[R * bs + cc] = cc * nb + pb[R];
             iperm[cc * nb + pb[R]] = R * bs + cc;
         }
+    const double tp = ms();
     // permuted block rows: sorted permuted columns
     std::vector<int> pptr(nb + 1, 0), pcol(G.ptr[nb] > 0 ? G.ptr[nb] : 1);
     for (int R = 0; R < nb; ++R) pptr[R + 1] = pptr[R] + (G.ptr[pb[R] + 1] - G.ptr[pb[R]]);
@@ -1845,6 +1850,7 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
         for (int e = G.ptr[o]; e < G.ptr[o + 1]; ++e) pcol[w++] = ipb[G.col[e]];
         std::sort(pcol.begin() + pptr[R], pcol.begin() + pptr[R + 1]);
     }
+    const double tc = ms();
     // block sliced ELL, 32 block rows per slice
     const int nsl = (nb + 31) / 32;
     std::vector<int> sp(nsl + 1, 0), len(nb > 0 ? nb : 1), dk(nb > 0 ? nb : 1);
@@ -1877,6 +1883,7 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
         }
     }
     L.kmax = kmax;
+    const double ts = ms();
     // value position of every scalar entry of A, block row by block row
     vpos.assign(nnz > 0 ? nnz : 1, -1);
 #pragma omp parallel for schedule(static)
@@ -1894,6 +1901,7 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
             }
         }
     }
+    const double tv = ms();
     L.n = n;
     L.nb = nb;
     L.bs = bs;
@@ -1913,6 +1921,10 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
     L.lus64 = c.allocN<double>(nv);
     L.perm = upload_ints(c, perm);
     L.v64 = c.allocN<double>((size_t)4 * (n > 0 ? n : 1));
+    if (c.verbose > 2 && nb > 100000)
+        std::printf("        ordering of %d block rows: %.1f ms (block graph %.1f, stages %.1f, permutation %.1f, "
+                    "sorted columns %.1f, slices %.1f, value positions %.1f, uploads %.1f)\n",
+                    nb, ms(), tg, tk - tg, tp - tk, tc - tp, ts - tc, tv - ts, ms() - tv);
 }
 
 // A P of level L (see mg_correct_kernel): for every block row, its coarse
@@ -1922,11 +1934,12 @@ void build_ap(Core& c, Level& L, const std::vector<int>& aggb)
 {
     const int nb = L.nb;
     const int nsl = (nb + 31) / 32;
+    const int W = L.kmax;  // a row has at most as many coarse columns as blocks
+    if (W < 1 || W > 64) return;
     std::vector<int> alen(nb > 0 ? nb : 1, 0);
-    std::vector<int> rowq((size_t)nb * 16);  // coarse columns of each row (at most its A row length)
+    std::unique_ptr<int[]> rowq(new int[(size_t)nb * W]);  // coarse columns of each row, ascending
     int kmax = 0;
-    bool ok = true;
-#pragma omp parallel for reduction(max : kmax) reduction(&& : ok) schedule(static)
+#pragma omp parallel for reduction(max : kmax) schedule(static)
     for (int R = 0; R < nb; ++R) {
         const int base = L.h_sp[R / 32] + (R % 32);
         int q[64];
@@ -1938,12 +1951,10 @@ void build_ap(Core& c, Level& L, const std::vector<int>& aggb)
             if (!seen && nq < 64) q[nq++] = P;
         }
         std::sort(q, q + nq);
-        if (nq > 16) ok = false;
         alen[R] = nq;
         kmax = std::max(kmax, nq);
-        for (int j = 0; j < nq && j < 16; ++j) rowq[(size_t)R * 16 + j] = q[j];
+        for (int j = 0; j < nq; ++j) rowq[(size_t)R * W + j] = q[j];
     }
-    if (!ok) return;  // rows of more than 16 coarse columns: keep the plain up-leg
     std::vector<int> asp(nsl + 1, 0);
     for (int sl = 0; sl < nsl; ++sl) {
         int w = 0;
@@ -1957,11 +1968,11 @@ void build_ap(Core& c, Level& L, const std::vector<int>& aggb)
         const int abase = asp[R / 32] + (R % 32);
         const int w = (asp[R / 32 + 1] - asp[R / 32]) / 32;
         const int base = L.h_sp[R / 32] + (R % 32);
-        for (int j = 0; j < w; ++j) acol[abase + 32 * j] = j < alen[R] ? rowq[(size_t)R * 16 + j] : aggb[R];
+        for (int j = 0; j < w; ++j) acol[abase + 32 * j] = j < alen[R] ? rowq[(size_t)R * W + j] : aggb[R];
         for (int k = 0; k < L.h_len[R]; ++k) {
             const int P = aggb[L.h_col[base + 32 * k]];
-            const int j = (int)(std::lower_bound(&rowq[(size_t)R * 16], &rowq[(size_t)R * 16] + alen[R], P) -
-                                &rowq[(size_t)R * 16]);
+            const int j = (int)(std::lower_bound(&rowq[(size_t)R * W], &rowq[(size_t)R * W] + alen[R], P) -
+                                &rowq[(size_t)R * W]);
             cnt[abase + 32 * j + 1]++;  // one writer per slot: slots belong to one row
         }
     }
@@ -1971,11 +1982,11 @@ void build_ap(Core& c, Level& L, const std::vector<int>& aggb)
     for (int R = 0; R < nb; ++R) {
         const int abase = asp[R / 32] + (R % 32);
         const int base = L.h_sp[R / 32] + (R % 32);
-        int fill[16] = {0};
+        int fill[64] = {0};  // per coarse column of the row (at most W <= 64)
         for (int k = 0; k < L.h_len[R]; ++k) {
             const int P = aggb[L.h_col[base + 32 * k]];
-            const int j = (int)(std::lower_bound(&rowq[(size_t)R * 16], &rowq[(size_t)R * 16] + alen[R], P) -
-                                &rowq[(size_t)R * 16]);
+            const int j = (int)(std::lower_bound(&rowq[(size_t)R * W], &rowq[(size_t)R * W] + alen[R], P) -
+                                &rowq[(size_t)R * W]);
             const int q = abase + 32 * j;
             gidx[cnt[q] + fill[j]++] = base + 32 * k;
         }
@@ -2058,6 +2069,7 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
         HostCsr owned;
         std::vector<int> owned_perm, owned_vpos;
         for (;;) {
+            const double tl0 = since();
             const HostCsr& fine = *finep;
             const std::vector<int>& fperm = *fpermp;
             const std::vector<int>& fvpos = *fvposp;
@@ -2103,10 +2115,13 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             Lc.cz = ccz;
             std::vector<int> cperm, ciperm, cvpos;
             bool cok = true;
+            const double tl1 = since();
             order_level(c, C, natural, bs, nc_unk <= fuse_rows, Lc, cperm, ciperm, cvpos, cok);
+            const double tl2 = since();
             if (!cok) fail(EQG_ERR_DEVICE, "coarse level without a diagonal entry");
             // aggregation in permuted positions, and aggregate members
             std::vector<int> aggp(fine.n);
+#pragma omp parallel for schedule(static)
             for (int pf = 0; pf < fine.n; ++pf) aggp[pf] = ciperm[agg_nat[fperm[pf]]];
             std::vector<int> mptr(nc_unk + 1, 0), midx(fine.n);
             for (int pf = 0; pf < fine.n; ++pf) mptr[aggp[pf] + 1]++;
@@ -2118,11 +2133,13 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             {
                 // per block row: unknown R*bs + c aggregates onto coarse R'*bs + c
                 std::vector<int> aggb(Lf.nb);
+                bool whole = true;
+#pragma omp parallel for schedule(static) reduction(&& : whole)
                 for (int R = 0; R < Lf.nb; ++R) {
                     aggb[R] = aggp[R * bs] / bs;
-                    for (int cc = 0; cc < bs; ++cc)
-                        if (aggp[R * bs + cc] != aggb[R] * bs + cc) fail(EQG_ERR_DEVICE, "aggregation splits a block");
+                    for (int cc = 0; cc < bs; ++cc) whole = whole && aggp[R * bs + cc] == aggb[R] * bs + cc;
                 }
+                if (!whole) fail(EQG_ERR_DEVICE, "aggregation splits a block");
                 Lf.aggb = upload_ints(c, aggb);
                 if (Lf.n > ap_rows) build_ap(c, Lf, aggb);
             }
@@ -2133,10 +2150,12 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             Lf.midx = upload_ints(c, midx);
             if (max_members <= kMembers) {
                 std::vector<int> mpad((size_t)nc_unk * kMembers, -1);
+#pragma omp parallel for schedule(static)
                 for (int P = 0; P < nc_unk; ++P)
                     for (int k = mptr[P]; k < mptr[P + 1]; ++k) mpad[(size_t)P * kMembers + (k - mptr[P])] = midx[k];
                 Lf.mpad = upload_ints(c, mpad);
             }
+            const double tl3 = since();
             // Galerkin gather: for every coarse entry, the value positions of
             // the fine entries that aggregate onto it, in ascending fine-entry
             // order.  A coarse row's entries come only from its members' rows,
@@ -2174,6 +2193,10 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
             Lc.gidx = upload_ints(c, gidx);
             Lc.gpos = upload_ints(c, cvpos);
             Lc.nnz = cnnz;
+            if (c.verbose > 2)
+                std::printf("        coarse level of %d unknowns: %.1f ms (pattern %.1f, ordering %.1f, aggregation "
+                            "and A P %.1f, Galerkin lists %.1f)\n",
+                            nc_unk, since() - tl0, tl1 - tl0, tl2 - tl1, tl3 - tl2, since() - tl3);
             if (nc_unk <= coarsest || (ccx == 1 && ccy == 1 && ccz == 1)) {
                 if (nc_unk > kCoarsest) {
                     an->multigrid = false;  // cannot coarsen further and too large to invert
