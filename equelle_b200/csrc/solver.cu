@@ -1803,7 +1803,11 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
         int len = 0;
         for (int cc = 0; cc < bs; ++cc) {
             const int u = cc * nb + R;
-            for (int e = A.ptr[u]; e < A.ptr[u + 1]; ++e) buf[len++] = A.col[e] % nb;
+            for (int e = A.ptr[u]; e < A.ptr[u + 1]; ++e) {
+                int cell = A.col[e];
+                while (cell >= nb) cell -= nb;  // column mod nb, at most bs - 1 subtractions
+                buf[len++] = cell;
+            }
         }
         buf[len++] = R;
         return len;
@@ -1894,10 +1898,14 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
         for (int cu = 0; cu < bs; ++cu) {
             const int u = cu * nb + Rn;
             for (int e = A.ptr[u]; e < A.ptr[u + 1]; ++e) {
-                const int v = A.col[e];
-                const int k = find_small(row, rl, ipb[v % nb]);
+                int cell = A.col[e], cv = 0;  // column = cv nb + cell, cv < bs (no division)
+                while (cell >= nb) {
+                    cell -= nb;
+                    ++cv;
+                }
+                const int k = find_small(row, rl, ipb[cell]);
                 const int64_t slot0 = sp[R / 32] + 32 * k;
-                vpos[e] = (int)((slot0 + R % 32) * bb + cu * bs + v / nb);
+                vpos[e] = (int)((slot0 + R % 32) * bb + cu * bs + cv);
             }
         }
     }
