@@ -1660,9 +1660,8 @@ struct SolverAnalysis {
     int tail_kmax = 0;
     int tail_cluster[3] = {0, 0, 0};
     // per precision: first fused level kept in block 0's shared memory
-    // (index into the fused levels; their count: none) and its bytes
+    // (index into the fused levels; their count: none)
     int tail_local[3] = {0, 0, 0};
-    int tail_smem[3] = {0, 0, 0};
     int last_mode = 0;  // precision of the last solve (pc_mode)
     Buf tail_trace;  // SM clock after each step of the last fused cycle
     // CUDA graphs of `chunk` BiCGStab iterations: [0] FP64, [1] FP32, [2] FP64
@@ -2469,7 +2468,8 @@ void prepare_tail(Core& c, SolverAnalysis& an)
     int& cl = an.tail_cluster[mode];
     const int bs = an.levels[an.tail_first].bs;
     if (!cl) WITH_BS(bs, WITH_KMAX(an.tail_kmax, cl = tail_cluster_size<BS, KK, T, M>(c)));
-    an.tail_local[mode] = plan_local<T, M>(c, an, an.tail_smem[mode], nullptr);
+    int bytes = 0;
+    an.tail_local[mode] = plan_local<T, M>(c, an, bytes, nullptr);
     an.last_mode = mode;
 }
 
