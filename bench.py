@@ -37,6 +37,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SPMV_KERNEL = "bicg_spmv_omega"
+# DRAM bytes (read + write) that ncu measured for one launch of that kernel
+# (2 x 2 FP64 blocks, --set full, two-phase 128x128x48: 242.5 MB) against its
+# algorithmic bytes (237.0 MB).  Both scale with the number of blocks, so a
+# launch of the same layout on another grid moves this ratio times its
+# algorithmic bytes.
+SPMV_TRAFFIC_RATIO = 242.5 / 237.0
 
 
 def parse():
@@ -296,8 +302,13 @@ def main():
     k_ms = kt / launches
     achieved = kbytes / (k_ms / 1000.0) / 1e9 if k_ms > 0 else 0.0
     peak, peak_kind = peaks()
+    # the captured layout: 3D two-phase, FP64 2 x 2 blocks, rows of up to 7 blocks
+    same_layout = a.workload == "twophase3d" and bsz == 2 and a.precision != "refine"
     roofline = {"kernel": SPMV_KERNEL, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": SPMV_TRAFFIC_RATIO * kbytes if same_layout else None,
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel on the "
+                                   "128x128x48 case, scaled by blocks" if same_layout else "not captured"),
                 "algorithmic_bytes_per_launch": kbytes, "launches": kl,
                 "avg_launch_ms": k_ms}
 
