@@ -37,6 +37,23 @@ def test_oracle_exports_header(oracle_lib):
     assert oracle_lib.eqg_backend_name() == b"cpu-oracle"
 
 
+def test_device_library_exports_other_headers():
+    """libeqg.so also exports what the other headers under include/ declare
+    (the allocation-free entry point, which the oracle does not have)."""
+    path = os.path.join(ROOT, "equelle_b200", "lib", "libeqg.so")
+    if not os.path.exists(path):
+        pytest.fail("libeqg.so not built: run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    inc = os.path.join(ROOT, "include")
+    names = []
+    for h in sorted(os.listdir(inc)):
+        if h.endswith(".h") and h != "eqg.h":
+            names += re.findall(r"\b(eqg_\w+)\s*\(", open(os.path.join(inc, h)).read())
+    assert names, "no declarations parsed"
+    for name in sorted(set(names)):
+        assert hasattr(lib, name), name
+
+
 def test_device_library_exports_header():
     """libeqg.so loads without a GPU and exports the whole ABI."""
     path = os.path.join(ROOT, "equelle_b200", "lib", "libeqg.so")
