@@ -54,7 +54,7 @@ def _stale(target, sources):
 def build_library(force=False, verbose=False):
     os.makedirs(OBJ_DIR, exist_ok=True)
     os.makedirs(LIB_DIR, exist_ok=True)
-    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(INCLUDE_DIR, "eqg.h")]
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE_DIR, "*.h"))
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     jobs = []
     objs = []

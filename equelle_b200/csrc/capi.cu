@@ -472,21 +472,32 @@ int eqg_runtime_kernel_profile(const eqg_runtime* rt, char* buf, int64_t len, in
     return guarded(__func__, [&] {
         need(rt, "runtime");
         const Core& c = *rt->core;
-        std::map<std::string, std::pair<int64_t, double>> agg;
+        // per kernel name: launches, ms, algorithmic bytes, launches that
+        // stated their bytes
+        struct Agg {
+            int64_t launches = 0, with_bytes = 0;
+            double ms = 0.0, bytes = 0.0;
+        };
+        std::map<std::string, Agg> agg;
         for (auto& pr : c.timer_pairs) {
             float f = 0.f;
             EQG_CUDA(cudaEventSynchronize(pr.b));
             EQG_CUDA(cudaEventElapsedTime(&f, pr.a, pr.b));
             auto& e = agg[pr.name];
-            e.first++;
-            e.second += f;
+            e.launches++;
+            e.ms += f;
+            if (pr.bytes >= 0) {
+                e.bytes += pr.bytes;
+                e.with_bytes++;
+            }
         }
         std::string js = "{";
         for (auto& kv : agg) {
             if (js.size() > 1) js += ", ";
             char tmp[256];
-            std::snprintf(tmp, sizeof(tmp), "\"%s\": [%lld, %.6f]", kv.first.c_str(), (long long)kv.second.first,
-                          kv.second.second);
+            std::snprintf(tmp, sizeof(tmp), "\"%s\": [%lld, %.6f, %.0f, %lld]", kv.first.c_str(),
+                          (long long)kv.second.launches, kv.second.ms, kv.second.bytes,
+                          (long long)kv.second.with_bytes);
             js += tmp;
         }
         js += "}";

@@ -509,6 +509,7 @@ void build_grid(Core& c, eqg_set** builtin)
         m->n_out = n_out;
         m->n_src = n_src;
         m->max_row = max_row;
+        m->nnz = nnz;
         m->ptr = c.allocN<int32_t>((size_t)n_out + 1);
         m->src = c.allocN<int32_t>(nnz > 0 ? nnz : 1);
         m->w = c.allocN<double>(nnz > 0 ? nnz : 1);
@@ -548,6 +549,7 @@ void build_grid(Core& c, eqg_set** builtin)
                                                                                cnt->as<int64_t>(), nullptr, nullptr,
                                                                                nullptr); });
         const int64_t nnz = counts_to_rowptr(c, cnt, c.nc, m->ptr);
+        m->nnz = nnz;
         m->src = c.allocN<int32_t>(nnz > 0 ? nnz : 1);
         m->w = c.allocN<double>(nnz > 0 ? nnz : 1);
         launch(c, "div_interior_fill", [&] { div_interior_kernel<true><<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, ipos->as<int32_t>(), nullptr,

@@ -81,6 +81,7 @@ struct OpMatrix {
     uint64_t id = 0;
     int n_out = 0, n_src = 0;
     int max_row = 0;
+    int64_t nnz = 0;
     Buf ptr;   // int32[n_out+1]
     Buf src;   // int32[nnz], ascending within a row
     Buf w;     // double[nnz]
@@ -192,6 +193,7 @@ struct Core {
     struct TimedLaunch {
         const char* name;
         cudaEvent_t a, b;
+        double bytes;  // algorithmic bytes of the launch (< 0: not stated)
     };
     std::vector<TimedLaunch> timer_pairs;
     PhaseClock residual_clock, factor_clock, krylov_clock;
@@ -289,8 +291,10 @@ void lazy_forget(eqg_mask* m);
 
 // Launches a kernel through `f`, checks the launch, and brackets it with
 // CUDA events on the runtime stream when `name` is the timed kernel.
+// `bytes`: the launch's algorithmic bytes (the data its operation must read
+// and write at least once), reported with the timings (< 0: not stated).
 template <class F>
-inline void launch(Core& c, const char* name, F&& f)
+inline void launch(Core& c, const char* name, F&& f, double bytes = -1.0)
 {
     const bool timed = !c.timed_kernel.empty() && (c.timed_kernel == name || c.timed_kernel == "*");
     cudaEvent_t a = nullptr, b = nullptr;
@@ -303,7 +307,7 @@ inline void launch(Core& c, const char* name, F&& f)
     c.checkLaunch(name);
     if (timed) {
         cudaEventRecord(b, c.stream);
-        c.timer_pairs.push_back({name, a, b});
+        c.timer_pairs.push_back({name, a, b, bytes});
     }
 }
 

@@ -412,9 +412,13 @@ template <int KMAX>
 void spgemm_numeric(Core& c, const OpMatrix& m, const Pattern& jp, const double* jv, const Pattern& op, double* ov)
 {
     if (m.n_out <= 0) return;
+    // algorithmic bytes: M (row pointers, sources, weights), the Jacobian
+    // operand and the output pattern (row pointers, columns, values) once
+    const double bytes = 4.0 * (m.n_out + 1) + 12.0 * m.nnz + 4.0 * (jp.rows + 1) + 12.0 * jp.nnz +
+                         4.0 * (op.rows + 1) + 12.0 * op.nnz;
     launch(c, "spgemm_numeric", [&] { spgemm_numeric_kernel<KMAX><<<blocksFor(m.n_out), kThreads, 0, c.stream>>>(
         m.n_out, m.ptr->as<int>(), m.src->as<int>(), m.w->as<double>(), jp.rowptr->as<int>(), jp.colind->as<int>(),
-        jv, op.rowptr->as<int>(), op.colind->as<int>(), ov); });
+        jv, op.rowptr->as<int>(), op.colind->as<int>(), ov); }, bytes);
 }
 
 int kmax_for(int max_row)
@@ -438,6 +442,7 @@ OpMatrixP opmat_from_host(Core& c, int n_out, int n_src, const std::vector<int32
     m->n_out = n_out;
     m->n_src = n_src;
     for (int i = 0; i < n_out; ++i) m->max_row = std::max(m->max_row, ptr[i + 1] - ptr[i]);
+    m->nnz = (int64_t)src.size();
     m->ptr = c.allocN<int32_t>(ptr.size());
     m->src = c.allocN<int32_t>(src.empty() ? 1 : src.size());
     m->w = c.allocN<double>(w.empty() ? 1 : w.size());
@@ -471,6 +476,7 @@ OpMatrixP opmat_from_map(Core& c, const int32_t* map_dev, int n_out, int n_src, 
     std::memcpy(&herr, c.pinned, 4);
     if (herr) fail(EQG_ERR_ARG, "index map points outside its source collection");
     if (!allow_missing && nnz != n_out) fail(EQG_ERR_ARG, "index map has unmatched entries");
+    m->nnz = nnz;
     m->src = c.allocN<int32_t>(nnz > 0 ? nnz : 1);
     m->w = c.allocN<double>(nnz > 0 ? nnz : 1);
     if (n_out > 0) {
@@ -484,7 +490,8 @@ void opmat_apply_values(Core& c, const OpMatrix& m, const double* x, double* y)
 {
     if (m.n_out <= 0) return;
     launch(c, "opmat_apply", [&] { opmat_apply_kernel<<<blocksFor(m.n_out), kThreads, 0, c.stream>>>(m.n_out, m.ptr->as<int>(), m.src->as<int>(),
-                                                                     m.w->as<double>(), x, y); });
+                                                                     m.w->as<double>(), x, y); },
+           4.0 * (m.n_out + 1) + 12.0 * m.nnz + 8.0 * m.n_src + 8.0 * m.n_out);
 }
 
 PatternP pattern_identity(Core& c, int n)
@@ -602,10 +609,17 @@ void jacobian_elementwise(Core& c, const JacArgs& a, const Pattern& out, double*
     Rule r{a.rule, a.va, a.vb, a.vout, a.mask, a.s};
     const bool flat = (!a.pa || a.pa->id == out.id) && (!a.pb || a.pb->id == out.id);
     if (out.nnz <= 0) return;
+    // algorithmic bytes: the operand Jacobians' values and the output's once,
+    // the output's row pointers, the per-row operand values the rule uses;
+    // operands on other patterns add their column indices and the output's
+    const int64_t na = a.pa ? a.pa->nnz : 0, nbv = a.pb ? a.pb->nnz : 0;
+    const double per_row = 8.0 * ((a.va ? 1 : 0) + (a.vb ? 1 : 0) + (a.vout ? 1 : 0)) + (a.mask ? 1.0 : 0.0);
+    const double bytes = 8.0 * (na + nbv + out.nnz) + 4.0 * (out.rows + 1) + per_row * out.rows +
+                         (flat ? 0.0 : 4.0 * (na + nbv + out.nnz));
     if (flat) {
         pattern_build_rowidx(c, const_cast<Pattern&>(out));
         launch(c, "jac_flat", [&] { ew_flat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(r, out.rowidx->as<int>(), a.pa ? a.ja : nullptr,
-                                                                      a.pb ? a.jb : nullptr, jout, out.nnz); });
+                                                                      a.pb ? a.jb : nullptr, jout, out.nnz); }, bytes);
     } else if (out.nnz < (int64_t)INT_MAX / 2) {
         // through position maps kept with the output pattern
         Pattern& o = const_cast<Pattern&>(out);
@@ -625,12 +639,12 @@ void jacobian_elementwise(Core& c, const JacArgs& a, const Pattern& out, double*
             ew_mapped_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(
                 r, out.rowidx->as<int>(), maps->as<int>(), maps->as<int>() + out.nnz, a.pa ? a.ja : nullptr,
                 a.pb ? a.jb : nullptr, jout, out.nnz);
-        });
+        }, bytes);
     } else {
         launch(c, "jac_merge", [&] { ew_merge_kernel<<<blocksFor(out.rows), kThreads, 0, c.stream>>>(
             r, out.rows, a.pa ? a.pa->rowptr->as<int>() : nullptr, a.pa ? a.pa->colind->as<int>() : nullptr,
             a.pa ? a.ja : nullptr, a.pb ? a.pb->rowptr->as<int>() : nullptr, a.pb ? a.pb->colind->as<int>() : nullptr,
-            a.pb ? a.jb : nullptr, out.rowptr->as<int>(), out.colind->as<int>(), jout); });
+            a.pb ? a.jb : nullptr, out.rowptr->as<int>(), out.colind->as<int>(), jout); }, bytes);
     }
 }
 

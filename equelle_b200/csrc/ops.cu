@@ -274,7 +274,7 @@ double run_reduce(Core& c, const double* a, int64_t n)
 {
     double* partials = c.red_partials->as<double>();
     const int nb = blocksFor(n, kThreads, kRedBlocks);
-    launch(c, "reduce_partials", [&] { reduce_partials_kernel<OP, SQUARE><<<nb, kThreads, 0, c.stream>>>(a, n, partials); });
+    launch(c, "reduce_partials", [&] { reduce_partials_kernel<OP, SQUARE><<<nb, kThreads, 0, c.stream>>>(a, n, partials); }, 8.0 * n);
     launch(c, "reduce_final", [&] { reduce_final_kernel<OP, SQUARE><<<1, kThreads, 0, c.stream>>>(partials, nb, partials + kRedBlocks); });
     EQG_CUDA(cudaMemcpyAsync(c.pinned, partials + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
@@ -286,7 +286,7 @@ double run_reduce(Core& c, const double* a, int64_t n)
 void k_fill(Core& c, double* out, double v, int64_t n)
 {
     if (n <= 0) return;
-    launch(c, "fill", [&] { fill_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(out, v, n); });
+    launch(c, "fill", [&] { fill_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(out, v, n); }, 8.0 * n);
 }
 
 void k_fill_i32(Core& c, int32_t* out, int32_t v, int64_t n)
@@ -300,10 +300,10 @@ void k_binary(Core& c, int op, const double* a, const double* b, double* out, in
     if (n <= 0) return;
     const int nb = blocksFor(n);
     switch (op) {
-    case EW_ADD: launch(c, "binary", [&] { binary_kernel<EW_ADD><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }); break;
-    case EW_SUB: launch(c, "binary", [&] { binary_kernel<EW_SUB><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }); break;
-    case EW_MUL: launch(c, "binary", [&] { binary_kernel<EW_MUL><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }); break;
-    case EW_DIV: launch(c, "binary", [&] { binary_kernel<EW_DIV><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }); break;
+    case EW_ADD: launch(c, "binary", [&] { binary_kernel<EW_ADD><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }, 24.0 * n); break;
+    case EW_SUB: launch(c, "binary", [&] { binary_kernel<EW_SUB><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }, 24.0 * n); break;
+    case EW_MUL: launch(c, "binary", [&] { binary_kernel<EW_MUL><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }, 24.0 * n); break;
+    case EW_DIV: launch(c, "binary", [&] { binary_kernel<EW_DIV><<<nb, kThreads, 0, c.stream>>>(a, b, out, n); }, 24.0 * n); break;
     default: fail(EQG_ERR_ARG, "unknown binary operator");
     }
 }
@@ -311,37 +311,37 @@ void k_binary(Core& c, int op, const double* a, const double* b, double* out, in
 void k_binary_scalar(Core& c, int op, const double* a, double s, int scalar_left, double* out, int64_t n)
 {
     if (n <= 0) return;
-    launch(c, "binary_scalar", [&] { binary_scalar_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, s, scalar_left, out, n); });
+    launch(c, "binary_scalar", [&] { binary_scalar_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, s, scalar_left, out, n); }, 16.0 * n);
 }
 
 void k_unary_value(Core& c, int op, const double* a, double* out, int64_t n)
 {
     if (n <= 0) return;
-    launch(c, "unary", [&] { unary_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, out, n); });
+    launch(c, "unary", [&] { unary_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, out, n); }, 16.0 * n);
 }
 
 void k_compare(Core& c, int op, const double* a, const double* b, uint8_t* out, int64_t n)
 {
     if (n <= 0) return;
-    launch(c, "compare", [&] { compare_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, b, out, n); });
+    launch(c, "compare", [&] { compare_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, b, out, n); }, 17.0 * n);
 }
 
 void k_compare_scalar(Core& c, int op, const double* a, double s, int scalar_left, uint8_t* out, int64_t n)
 {
     if (n <= 0) return;
-    launch(c, "compare_scalar", [&] { compare_scalar_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, s, scalar_left, out, n); });
+    launch(c, "compare_scalar", [&] { compare_scalar_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, s, scalar_left, out, n); }, 9.0 * n);
 }
 
 void k_select_value(Core& c, const uint8_t* m, const double* a, const double* b, double* out, int64_t n)
 {
     if (n <= 0) return;
-    launch(c, "select", [&] { select_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(m, a, b, out, n); });
+    launch(c, "select", [&] { select_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(m, a, b, out, n); }, 25.0 * n);
 }
 
 void k_mask_logic(Core& c, int op, const uint8_t* a, const uint8_t* b, uint8_t* out, int64_t n)
 {
     if (n <= 0) return;
-    launch(c, "mask_logic", [&] { mask_logic_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, b, out, n); });
+    launch(c, "mask_logic", [&] { mask_logic_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(op, a, b, out, n); }, 3.0 * n);
 }
 
 void k_set_select(Core& c, const uint8_t* m, const int32_t* a, const int32_t* b, int32_t* out, int64_t n)
@@ -373,7 +373,7 @@ void k_gather_f64(Core& c, const double* data, const int32_t* idx, int stride, i
                   int32_t* err)
 {
     if (n <= 0) return;
-    launch(c, "gather_f64", [&] { gather_f64_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(data, idx, stride, comp, out, n, err); });
+    launch(c, "gather_f64", [&] { gather_f64_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(data, idx, stride, comp, out, n, err); }, 20.0 * n);
 }
 
 void k_normal(Core& c, const int32_t* faces, double* out, int comp, int64_t n, int32_t* err)
@@ -419,7 +419,7 @@ double k_two_norm(Core& c, const double* a, int64_t n)
 {
     double* partials = c.red_partials->as<double>();
     const int nb = blocksFor(n, kThreads, kRedBlocks);
-    launch(c, "norm_partials", [&] { reduce_partials_kernel<EQG_SUM, true><<<nb, kThreads, 0, c.stream>>>(a, n, partials); });
+    launch(c, "norm_partials", [&] { reduce_partials_kernel<EQG_SUM, true><<<nb, kThreads, 0, c.stream>>>(a, n, partials); }, 8.0 * n);
     launch(c, "norm_final", [&] { reduce_final_kernel<EQG_SUM, true><<<1, kThreads, 0, c.stream>>>(partials, nb, partials + kRedBlocks); });
     EQG_CUDA(cudaMemcpyAsync(c.pinned, partials + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     c.sync();

@@ -1611,6 +1611,9 @@ struct Level {
     int cx = 1, cy = 1, cz = 1;    // cells of this level's grid
     bool coarsest = false;
     std::vector<int> stage_ptr;    // stages (colours or wavefronts) of block rows, permuted order
+    // blocks left and right of the diagonal in the rows of each stage
+    // (algorithmic bytes of the sweeps)
+    std::vector<int64_t> stage_lower, stage_upper;
     Buf perm;                      // permuted unknown position -> natural unknown
     Buf gptr, gidx, gpos;          // Galerkin gather from the finer level's values (levels > 0)
     Buf aggb;                      // coarse block row of each block row (next coarser level)
@@ -1618,6 +1621,7 @@ struct Level {
     // longest row, slices, coarse block columns, row lengths, and the A slots
     // summed into each slot (gptr/gidx); levels above linsolver_mg_ap_rows
     int64_t ap_slots = 0;
+    int64_t ap_blocks = 0;         // coarse block columns over all rows (without padding)
     int ap_kmax = 0;
     Buf ap_sp, ap_col, ap_len, ap_gptr, ap_gidx, ap64, ap32;
     SellView ap_view() const
@@ -1923,6 +1927,17 @@ void order_level(Core& c, const HostCsr& A, bool natural, int bs, bool uniform, 
     L.h_len = len;
     L.sell_len = upload_ints(c, len);
     L.sell_dk = upload_ints(c, dk);
+    {
+        const int nst = (int)L.stage_ptr.size() - 1;
+        L.stage_lower.assign(nst > 0 ? nst : 0, 0);
+        L.stage_upper.assign(nst > 0 ? nst : 0, 0);
+        for (int st = 0; st < nst; ++st)
+            for (int R = L.stage_ptr[st]; R < L.stage_ptr[st + 1]; ++R) {
+                const int d = dk[R] >= 0 ? dk[R] : 0;
+                L.stage_lower[st] += d;
+                L.stage_upper[st] += std::max(0, len[R] - d - 1);
+            }
+    }
     const size_t nv = (size_t)(L.vals > 0 ? L.vals : 1);
     L.as64 = c.allocN<double>(nv);
     L.lus64 = c.allocN<double>(nv);
@@ -2000,6 +2015,8 @@ void build_ap(Core& c, Level& L, const std::vector<int>& aggb)
     }
     L.ap_slots = slots;
     L.ap_kmax = kmax;
+    L.ap_blocks = 0;
+    for (int R = 0; R < nb; ++R) L.ap_blocks += alen[R];
     L.ap_sp = upload_ints(c, asp);
     L.ap_col = upload_ints(c, acol);
     L.ap_len = upload_ints(c, alen);
@@ -2434,6 +2451,16 @@ int plan_local(Core& c, const SolverAnalysis& an, int& bytes, TailParams<T, M>* 
     return lf;
 }
 
+// Algorithmic bytes of the solver launches (reported with kernel timings):
+// every matrix block the step needs read once (its B^2 values and 4-byte
+// column), 4 bytes of row data per block row read (its length or diagonal
+// position), every vector element the step needs read or written once.
+template <class M>
+double block_bytes(const Level& L, int64_t blocks)
+{
+    return (double)blocks * (double)(sizeof(M) * L.bs * L.bs + 4);
+}
+
 // Launches kernel k on the runtime stream.  With c.pdl_launch it is a
 // programmatic dependent launch: its blocks may be scheduled while the
 // kernel before it on the stream finishes, which hides the launch latency
@@ -2536,9 +2563,17 @@ void launch_tail(Core& c, const SolverAnalysis& an, const T* r, T* z, const KSca
     attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = c.pdl_launch ? 2 : 1;
+    // algorithmic bytes: every fused level's matrix, factors and index
+    // arrays once (the data the bulk prefetch fetches) and its four vectors
+    double tail_bytes = 0.0;
+    for (size_t l = an.tail_first; l < an.levels.size(); ++l) {
+        const Level& L = an.levels[l];
+        tail_bytes += (L.coarsest ? (double)L.n * L.n : 2.0 * L.vals) * sizeof(M) + 4.0 * L.sell_size +
+                      8.0 * L.nb + 4.0 * L.n * sizeof(T);
+    }
     WITH_BS(an.levels[an.tail_first].bs, WITH_KMAX(an.tail_kmax, launch(c, "mg_tail", [&] {
                 EQG_CUDA(cudaLaunchKernelEx(&cfg, mg_tail_kernel<BS, KK, T, M>, p, r, z, sc, skip_if_s));
-            })));
+            }, tail_bytes)));
 }
 
 // Prints the steps of the last fused coarse cycle (linsolver_tail_trace=1):
@@ -2597,20 +2632,31 @@ void ilu_apply(Core& c, const Level& L, const T* b, T* out, T* zadd, const KScal
     const int ns = (int)L.stage_ptr.size() - 1;
     if (ns <= 0) return;
     const int r_first = L.stage_ptr[1];
+    // algorithmic bytes of a stage: its off-diagonal blocks on the swept
+    // side, its inverted diagonal blocks where rows finish, 4 bytes per row
+    // (diagonal position), its rows of b or y read and of out written, the
+    // other stages' values it gathers (counted as one vector of the stage's
+    // size) and zadd read and written where rows finish
+    const double vrow = (double)L.bs * sizeof(T);
     for (int s = 1; s < ns; ++s) {
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
         const int last = s == ns - 1;
+        const double bytes = block_bytes<M>(L, L.stage_lower[s]) +
+                             (last ? (double)(r1 - r0) * L.bs * L.bs * sizeof(M) : 0.0) +
+                             (r1 - r0) * (4.0 + vrow * ((last && zadd) ? 5.0 : 3.0));
         WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "bilu_lower", [&] {
                     launch_k(c, bilu_lower_kernel<BS, KK, T, M>, blocksFor(r1 - r0), kThreads, r0, r1, r_first, last,
                              L.view(), lu, b, out, last ? zadd : nullptr, sc, skip_if_s);
-                })));
+                }, bytes)));
     }
     for (int s = ns >= 2 ? ns - 2 : 0; s >= 0; --s) {
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
+        const double bytes = block_bytes<M>(L, L.stage_upper[s]) + (double)(r1 - r0) * L.bs * L.bs * sizeof(M) +
+                             (r1 - r0) * (8.0 + vrow * (zadd ? 5.0 : 3.0));
         WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "bilu_upper", [&] {
                     launch_k(c, bilu_upper_kernel<BS, KK, T, M>, blocksFor(r1 - r0), kThreads, r0, r1, (int)(s == 0),
                              L.view(), lu, b, out, zadd, sc, skip_if_s);
-                })));
+                }, bytes)));
     }
 }
 
@@ -2619,10 +2665,17 @@ template <class T, class M>
 void level_residual(Core& c, const Level& L, const T* x, const T* b, T* out, int r_zero, const KScal* sc,
                     int skip_if_s)
 {
+    // rows from r_zero: their blocks and lengths, b read and out written;
+    // x read once
+    const int64_t skipped = r_zero > 0 && !L.stage_lower.empty()
+                                ? L.stage_lower[0] + L.stage_upper[0] + (L.stage_ptr[1] - L.stage_ptr[0])
+                                : 0;
+    const double bytes = block_bytes<M>(L, L.blocks - skipped) +
+                         (L.nb - r_zero) * (4.0 + 2.0 * L.bs * sizeof(T)) + (double)L.n * sizeof(T);
     WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "mg_residual", [&] {
                 launch_k(c, mg_residual_kernel<BS, KK, T, M>, blocksFor(L.nb), kThreads, L.nb, r_zero, L.view(),
                          level_a<M>(L), x, b, out, sc, skip_if_s);
-            })));
+            }, bytes)));
 }
 
 // z = V-cycle(r) on level l.
@@ -2637,7 +2690,7 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     if (L.coarsest) {
         launch(c, "mg_dense_apply", [&] {
             launch_k(c, dense_apply_kernel<T, M>, 1, kThreads, L.n, level_inv<M>(L), r, z, sc, skip);
-        });
+        }, (double)L.n * L.n * sizeof(M) + 2.0 * L.n * sizeof(T));
         return;
     }
     const Level& C = an.levels[l + 1];
@@ -2657,22 +2710,26 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     launch(c, "mg_restrict", [&] {
         launch_k(c, mg_restrict_kernel<T>, blocksFor(C.n), kThreads, C.n, (const int*)L.mptr->as<int>(),
                  (const int*)L.midx->as<int>(), (const T*)t, r_zero * L.bs, rc, sc, skip);
-    });
+    }, (double)(L.n - r_zero * L.bs) * sizeof(T) + (double)C.n * sizeof(T) + 4.0 * (C.n + 1) + 4.0 * L.n);
     vcycle<T, M>(c, an, l + 1, rc, zc, sc, skip);
     // coarse correction z += alpha P zc and its residual t = r - A z, then
     // post-smoothing z += M^{-1} t.  Through A P with FP64 vectors only: with
     // the FP32 vectors of "refine" the updated residual drifts from r - A z
     // and the iterations per time step rose from 203 to 254 (128x128x64)
     if (L.ap_slots > 0 && sizeof(T) == sizeof(double)) {
+        // A P blocks and row lengths, aggregates, zc once, z and t (rows
+        // from r_zero) read and written
+        const double bytes = block_bytes<M>(L, L.ap_blocks) + 8.0 * L.nb + (double)C.n * sizeof(T) +
+                             2.0 * L.n * sizeof(T) + 2.0 * (L.n - r_zero * L.bs) * sizeof(T);
         WITH_BS(L.bs, WITH_KMAX(L.ap_kmax, launch(c, "mg_correct", [&] {
                     launch_k(c, mg_correct_kernel<BS, KK, T, M>, blocksFor(L.nb), kThreads, L.nb, r_zero, L.ap_view(),
                              level_ap<M>(L), (const int*)L.aggb->as<int>(), (const T*)zc, z, t, an.mg_alpha, sc, skip);
-                })));
+                }, bytes)));
     } else {
         WITH_BS(L.bs, launch(c, "mg_prolong", [&] {
                     launch_k(c, mg_prolong_kernel<BS, T>, blocksFor(L.nb), kThreads, L.nb,
                              (const int*)L.aggb->as<int>(), (const T*)zc, z, an.mg_alpha, sc, skip);
-                }));
+                }, 4.0 * L.nb + (double)C.n * sizeof(T) + 2.0 * L.n * sizeof(T)));
         level_residual<T, M>(c, L, z, r, t, 0, sc, skip);
     }
     ilu_apply<T, M>(c, L, t, w, z, sc, skip);
@@ -2712,31 +2769,33 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double 
     unsigned int* cnt = an.counter->as<unsigned int>();
     const int nb = blocksFor(n, kThreads, kRedBlocks);
     const int nbr = blocksFor(L0.nb, kThreads, kRedBlocks);
+    const double vb = (double)n * sizeof(T);  // one vector
+    const double spmv_bytes = block_bytes<T>(L0, L0.blocks) + 4.0 * L0.nb + 3.0 * vb;
     launch(c, "bicg_init", [&] {
         bicg_init_kernel<T><<<nb, kThreads, 0, c.stream>>>(v.b, v.r, v.rhat, v.p, v.v, v.x, n, part, cnt, sc, tol * tol);
-    });
+    }, 6.0 * vb);
     auto iteration = [&] {
         launch(c, "bicg_p", [&] {
             launch_k(c, bicg_p_kernel<T>, blocksFor(n), kThreads, (const T*)v.r, (const T*)v.v, v.p, n,
                      (const KScal*)sc);
-        });
+        }, 4.0 * vb);
         apply_pc<T>(c, an, v.p, v.ph, sc, 0, pc32);
         WITH_BS(L0.bs, WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_alpha", [&] {
                     launch_k(c, bicg_spmv_alpha_kernel<BS, KK, T>, nbr, kThreads, L0.view(), a, (const T*)v.ph,
                              (const T*)v.rhat, v.v, L0.nb, part, cnt, sc);
-                })));
+                }, spmv_bytes)));
         launch(c, "bicg_s", [&] {
             launch_k(c, bicg_s_kernel<T>, nb, kThreads, (const T*)v.r, (const T*)v.v, v.s, n, part, cnt, sc);
-        });
+        }, 3.0 * vb);
         apply_pc<T>(c, an, v.s, v.sh, sc, 1, pc32);
         WITH_BS(L0.bs, WITH_KMAX(L0.kmax, launch(c, "bicg_spmv_omega", [&] {
                     launch_k(c, bicg_spmv_omega_kernel<BS, KK, T>, nbr, kThreads, L0.view(), a, (const T*)v.sh,
                              (const T*)v.s, v.t, L0.nb, part, cnt, sc);
-                })));
+                }, spmv_bytes)));
         launch(c, "bicg_xr", [&] {
             launch_k(c, bicg_xr_kernel<T>, nb, kThreads, (const T*)v.ph, (const T*)v.sh, (const T*)v.s,
                      (const T*)v.t, (const T*)v.rhat, v.x, v.r, n, part, cnt, sc);
-        });
+        }, 8.0 * vb);
     };
     // Graph of `check_every` iterations, captured once per analysis and
     // precision; kernel arguments are fixed (buffers of the analysis,
@@ -2797,10 +2856,15 @@ void factor_level(Core& c, const Level& L, int* status)
     const int ns = (int)L.stage_ptr.size() - 1;
     for (int s = 0; s < ns; ++s) {
         const int r0 = L.stage_ptr[s], r1 = L.stage_ptr[s + 1];
+        // the stage's blocks read and written, the upper blocks of the rows
+        // they eliminate read once (counted as the stage's own upper blocks)
+        const int64_t stage_blocks = L.stage_lower[s] + L.stage_upper[s] + (r1 - r0);
+        const double bytes = block_bytes<double>(L, stage_blocks) + 8.0 * L.bs * L.bs * stage_blocks +
+                             block_bytes<double>(L, L.stage_upper[s]) + 8.0 * (r1 - r0);
         WITH_BS(L.bs, launch(c, "bilu_factor", [&] {
                     bilu_factor_stage_kernel<BS><<<blocksFor(r1 - r0), kThreads, 0, c.stream>>>(
                         r0, r1, L.view(), L.lus64->as<double>(), status);
-                }));
+                }, bytes));
     }
 }
 
@@ -2808,7 +2872,8 @@ void to_float(Core& c, const Buf& src, Buf& dst, int64_t n)
 {
     if (!dst) dst = c.allocN<float>((size_t)(n > 0 ? n : 1));
     launch(c, "to_float",
-           [&] { to_float_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(src->as<double>(), dst->as<float>(), n); });
+           [&] { to_float_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(src->as<double>(), dst->as<float>(), n); },
+           12.0 * n);
 }
 
 }  // namespace
@@ -2848,16 +2913,18 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     launch(c, "gather_values", [&] {
         gather_values_kernel<<<blocksFor(L0.vals), kThreads, 0, c.stream>>>(jval, an.vmap->as<int>(),
                                                                             L0.as64->as<double>(), L0.vals);
-    });
+    }, 12.0 * L0.vals + 8.0 * an.nnz);
     for (size_t l = 1; l < an.levels.size(); ++l) {
         const Level& F = an.levels[l - 1];
         const Level& C = an.levels[l];
         EQG_CUDA(cudaMemsetAsync(C.as64->ptr, 0, (size_t)C.vals * sizeof(double), c.stream));
+        // the finer level's entries and their gather indices once, the
+        // coarse entries (list bounds, position, value) once
         launch(c, "mg_galerkin", [&] {
             galerkin_kernel<<<blocksFor(C.nnz), kThreads, 0, c.stream>>>(C.nnz, C.gptr->as<int>(), C.gidx->as<int>(),
                                                                          C.gpos->as<int>(), F.as64->as<double>(),
                                                                          C.as64->as<double>());
-        });
+        }, 12.0 * F.nnz + 16.0 * C.nnz);
     }
     for (auto& L : an.levels)
         if (L.ap_slots > 0) {
@@ -2865,7 +2932,7 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
                 ap_values_kernel<<<blocksFor(L.ap_slots * L.bs * L.bs), kThreads, 0, c.stream>>>(
                     L.ap_slots, L.bs * L.bs, L.ap_gptr->as<int>(), L.ap_gidx->as<int>(), L.as64->as<double>(),
                     L.ap64->as<double>());
-            });
+            }, block_bytes<double>(L, L.blocks) + 8.0 * L.ap_slots + 8.0 * L.bs * L.bs * L.ap_slots);
         }
     EQG_CUDA(cudaMemsetAsync(an.factor_status->ptr, 0, sizeof(int), c.stream));
     for (auto& L : an.levels) {
@@ -2876,14 +2943,15 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
                                               (int)smem));
                 dense_inverse_kernel<BS><<<1, 1024, smem, c.stream>>>(L.nb, L.view(), L.as64->as<double>(),
                                                                      L.inv64->as<double>(), an.factor_status->as<int>());
-            }));
+            }, 16.0 * L.n * L.n));
         } else {
             factor_level(c, L, an.factor_status->as<int>());
         }
     }
     Vecs<double> v = vecs<double>(an.vec64->as<double>(), n);
     launch(c, "permute",
-           [&] { permute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(rhs, L0.perm->as<int>(), v.b, n); });
+           [&] { permute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(rhs, L0.perm->as<int>(), v.b, n); },
+           20.0 * n);
     if (mixed || refine) {
         for (auto& L : an.levels) {
             to_float(c, L.as64, L.as32, L.vals);
@@ -2920,13 +2988,14 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         k_fill(c, v.x, 0.0, n);
         Buf rr_dev = c.allocN<double>(2);
         launch(c, "sumsq",
-               [&] { sumsq_kernel<<<nb, kThreads, 0, c.stream>>>(v.b, n, part, cnt, rr_dev->as<double>()); });
+               [&] { sumsq_kernel<<<nb, kThreads, 0, c.stream>>>(v.b, n, part, cnt, rr_dev->as<double>()); },
+               8.0 * n);
         auto residual = [&] {
             WITH_BS(L0.bs, WITH_KMAX(L0.kmax, launch(c, "residual", [&] {
                         residual_kernel<BS, KK><<<nbr, kThreads, 0, c.stream>>>(
                             L0.view(), L0.as64->as<double>(), v.x, v.b, v.r, w.b, L0.nb, part, cnt,
                             rr_dev->as<double>() + 1);
-                    })));
+                    }, block_bytes<double>(L0, L0.blocks) + 4.0 * L0.nb + 28.0 * n)));
         };
         residual();
         EQG_CUDA(cudaMemcpyAsync(c.pinned, rr_dev->ptr, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -2941,7 +3010,7 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
             total_iter += inner.iterations;
             ++sweeps;
             launch(c, "add_float",
-                   [&] { add_float_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, w.x, n); });
+                   [&] { add_float_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, w.x, n); }, 20.0 * n);
             residual();
             EQG_CUDA(cudaMemcpyAsync(c.pinned, rr_dev->as<double>() + 1, sizeof(double), cudaMemcpyDeviceToHost,
                                      c.stream));
@@ -2958,7 +3027,8 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     c.krylov_clock.stop(c.stream);
     report_tail_trace(c, an);
     launch(c, "unpermute",
-           [&] { unpermute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, L0.perm->as<int>(), xout, n); });
+           [&] { unpermute_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(v.x, L0.perm->as<int>(), xout, n); },
+           20.0 * n);
     res.block_size = L0.bs;
     res.blocks = L0.blocks;
     return res;

@@ -147,10 +147,13 @@ int eqg_runtime_grid_info(const eqg_runtime* rt, eqg_grid_info* out);
 int eqg_runtime_synchronize(eqg_runtime* rt);
 int eqg_runtime_stats(const eqg_runtime* rt, eqg_stats* out);
 int eqg_runtime_reset_stats(eqg_runtime* rt);
-/* Device time per kernel name, as JSON {"name": [launches, ms], ...}, of
- * the launches timed under the parameter time_kernel (a name, or "*" for
- * every kernel).  Writes at most len bytes (NUL terminated) and the size
- * needed to *needed. */
+/* Device time per kernel name, as JSON
+ * {"name": [launches, ms, bytes, launches_with_bytes], ...}, of the
+ * launches timed under the parameter time_kernel (a name, or "*" for every
+ * kernel); bytes sums the algorithmic bytes (data the launch's operation
+ * must read and write at least once) of the launches that state them.
+ * Writes at most len bytes (NUL terminated) and the size needed to
+ * *needed. */
 int eqg_runtime_kernel_profile(const eqg_runtime* rt, char* buf, int64_t len, int64_t* needed);
 /* Timing marks: records an event on the runtime's stream (device clock for
  * the product, host steady clock for the oracle) and returns its id. */

@@ -3,12 +3,12 @@
  *
  * It has no counterpart in the reference (sintefmath/equelle has no device
  * code on this path).  It exists for callers that cannot call cudaMalloc:
- * code running inside a CUDA stream capture that must not add allocation
- * nodes, programs whose memory is budgeted up front by an external pool,
- * and plugins loaded into a host application that owns every device
- * allocation.  Such a caller passes device pointers for the input and the
- * output; the reduction's scratch (one partial sum per block of 256
- * elements) lives in a fixed array inside the library.
+ * plugins loaded into a host application whose own memory pool owns every
+ * device allocation, and programs whose device memory is budgeted once, up
+ * front, so that no allocation may happen while they run.  Such a caller
+ * passes device pointers for the input and the output; the reduction's
+ * scratch (one partial sum per block of 256 elements) lives in a fixed
+ * array inside the library.
  */
 #ifndef EQG_NOALLOC_H
 #define EQG_NOALLOC_H

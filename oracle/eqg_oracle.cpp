@@ -224,6 +224,7 @@ Csr csr_transpose(const Csr& a)
 std::vector<double> csr_apply(const Csr& a, const std::vector<double>& x)
 {
     std::vector<double> y(a.rows, 0.0);
+#pragma omp parallel for schedule(static) if (a.rows > 4096)
     for (int64_t i = 0; i < a.rows; ++i) {
         double s = 0.0;
         for (int64_t e = a.ptr[i]; e < a.ptr[i + 1]; ++e) s += a.val[e] * x[a.col[e]];
@@ -509,7 +510,36 @@ HelperOps build_ops(const Grid& g)
 struct Ilu0 {
     Csr lu;                     // L (unit, strictly lower) and U in one pattern
     std::vector<int64_t> diag;  // position of the diagonal in each row
+    // Built with OpenMP only: rows grouped by wavefront level of the forward
+    // (L) and backward (U) solves, so that rows of one level run in
+    // parallel with the same per-row operations as the serial loops.
+    std::vector<int64_t> fwd_ptr, fwd_rows, bwd_ptr, bwd_rows;
 };
+
+#ifdef _OPENMP
+// Rows in wavefront levels: level(i) = 1 + max level of the rows it reads.
+void wavefronts(const Ilu0& f, bool lower, std::vector<int64_t>& ptr, std::vector<int64_t>& rows)
+{
+    const Csr& m = f.lu;
+    const int64_t n = m.rows;
+    std::vector<int64_t> lev(n, 0);
+    int64_t nl = 0;
+    for (int64_t k = 0; k < n; ++k) {
+        const int64_t i = lower ? k : n - 1 - k;
+        int64_t l = 0;
+        const int64_t e0 = lower ? m.ptr[i] : f.diag[i] + 1, e1 = lower ? f.diag[i] : m.ptr[i + 1];
+        for (int64_t e = e0; e < e1; ++e) l = std::max(l, lev[m.col[e]] + 1);
+        lev[i] = l;
+        nl = std::max(nl, l + 1);
+    }
+    ptr.assign(nl + 1, 0);
+    for (int64_t i = 0; i < n; ++i) ptr[lev[i] + 1]++;
+    for (int64_t l = 0; l < nl; ++l) ptr[l + 1] += ptr[l];
+    rows.resize(n);
+    std::vector<int64_t> pos(ptr.begin(), ptr.end() - 1);
+    for (int64_t i = 0; i < n; ++i) rows[pos[lev[i]]++] = i;
+}
+#endif
 
 bool ilu0_factor(const Csr& a, Ilu0& f)
 {
@@ -539,6 +569,10 @@ bool ilu0_factor(const Csr& a, Ilu0& f)
         for (int64_t e = m.ptr[i]; e < m.ptr[i + 1]; ++e) where[m.col[e]] = -1;
         if (m.val[f.diag[i]] == 0.0) return false;
     }
+#ifdef _OPENMP
+    wavefronts(f, true, f.fwd_ptr, f.fwd_rows);
+    wavefronts(f, false, f.bwd_ptr, f.bwd_rows);
+#endif
     return true;
 }
 
@@ -547,6 +581,29 @@ void ilu0_apply(const Ilu0& f, const std::vector<double>& b, std::vector<double>
     const Csr& m = f.lu;
     const int64_t n = m.rows;
     x.resize(n);
+#ifdef _OPENMP
+#pragma omp parallel
+    {
+        for (size_t l = 0; l + 1 < f.fwd_ptr.size(); ++l) {
+#pragma omp for schedule(static)
+            for (int64_t k = f.fwd_ptr[l]; k < f.fwd_ptr[l + 1]; ++k) {
+                const int64_t i = f.fwd_rows[k];
+                double s = b[i];
+                for (int64_t e = m.ptr[i]; e < f.diag[i]; ++e) s -= m.val[e] * x[m.col[e]];
+                x[i] = s;
+            }
+        }
+        for (size_t l = 0; l + 1 < f.bwd_ptr.size(); ++l) {
+#pragma omp for schedule(static)
+            for (int64_t k = f.bwd_ptr[l]; k < f.bwd_ptr[l + 1]; ++k) {
+                const int64_t i = f.bwd_rows[k];
+                double s = x[i];
+                for (int64_t e = f.diag[i] + 1; e < m.ptr[i + 1]; ++e) s -= m.val[e] * x[m.col[e]];
+                x[i] = s / m.val[f.diag[i]];
+            }
+        }
+    }
+#else
     for (int64_t i = 0; i < n; ++i) {
         double s = b[i];
         for (int64_t e = m.ptr[i]; e < f.diag[i]; ++e) s -= m.val[e] * x[m.col[e]];
@@ -557,12 +614,15 @@ void ilu0_apply(const Ilu0& f, const std::vector<double>& b, std::vector<double>
         for (int64_t e = f.diag[i] + 1; e < m.ptr[i + 1]; ++e) s -= m.val[e] * x[m.col[e]];
         x[i] = s / m.val[f.diag[i]];
     }
+#endif
 }
 
 double dot(const std::vector<double>& a, const std::vector<double>& b)
 {
     double s = 0.0;
-    for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+    const int64_t n = (int64_t)a.size();
+#pragma omp parallel for schedule(static) reduction(+ : s) if (n > 4096)
+    for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
     return s;
 }
 
@@ -622,12 +682,14 @@ SolveReport bicgstab_ilu0(const Csr& a, const std::vector<double>& b, std::vecto
         const double rho_new = dot(rhat, r);
         if (rho_new == 0.0) break;
         const double beta = (rho_new / rho) * (alpha / omega);
+#pragma omp parallel for schedule(static) if (n > 4096)
         for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
         ilu0_apply(prec, p, ph);
         v = csr_apply(a, ph);
         const double rv = dot(rhat, v);
         if (rv == 0.0) break;
         alpha = rho_new / rv;
+#pragma omp parallel for schedule(static) if (n > 4096)
         for (int64_t i = 0; i < n; ++i) s[i] = r[i] - alpha * v[i];
         const double snorm = std::sqrt(dot(s, s));
         rep.iterations = it;
@@ -642,6 +704,7 @@ SolveReport bicgstab_ilu0(const Csr& a, const std::vector<double>& b, std::vecto
         const double tt = dot(t, t);
         if (tt == 0.0) break;
         omega = dot(t, s) / tt;
+#pragma omp parallel for schedule(static) if (n > 4096)
         for (int64_t i = 0; i < n; ++i) {
             x[i] += alpha * ph[i] + omega * sh[i];
             r[i] = s[i] - omega * t[i];

@@ -98,4 +98,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("EQUELLE_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <sintefmath/equelle checkout> (or set EQUELLE_REFERENCE)")
+    main(ref)
