@@ -19,6 +19,7 @@
 
 namespace eqg {
 void build_grid(Core& c, eqg_set** builtin);
+void build_grid_from_file(Core& c, const std::string& path, eqg_set** builtin);
 void set_last_error(const std::string& msg);
 }
 
@@ -343,8 +344,6 @@ int eqg_runtime_create(int nparams, const char* const* keys, const char* const* 
         rt->core = std::make_shared<Core>();
         Core& c = *rt->core;
         for (int i = 0; i < nparams; ++i) c.params[keys[i]] = values[i];
-        if (c.params.count("grid_filename"))
-            fail(EQG_ERR_UNSUPPORTED, "grid_filename: unstructured grid input is not supported");
         c.dim = c.param_i("grid_dim", 2);
         c.nx = c.param_i("nx", 6);
         c.ny = c.param_i("ny", 1);
@@ -359,7 +358,8 @@ int eqg_runtime_create(int nparams, const char* const* keys, const char* const* 
         c.timed_kernel = c.param_s("time_kernel", "");
         c.red_partials = c.allocN<double>((size_t)kRedBlocks * 4);
         c.red_counter = c.allocN<unsigned int>(1);
-        build_grid(c, rt->builtin);
+        if (c.params.count("grid_filename")) build_grid_from_file(c, c.params["grid_filename"], rt->builtin);
+        else build_grid(c, rt->builtin);
         for (auto* s : rt->builtin) {
             s->core = rt->core;
             s->id = c.newId();

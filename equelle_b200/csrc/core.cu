@@ -16,7 +16,14 @@
 
 #include <cub/cub.cuh>
 
+#include <algorithm>
+#include <cctype>
+#include <cerrno>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <sstream>
+#include <vector>
 
 namespace eqg {
 
@@ -426,6 +433,82 @@ Buf compact_indices(Core& c, const uint8_t* flags, int64_t n, int64_t& count)
     return out;
 }
 
+namespace {
+
+// The six built-in index sets from the face-interior and cell-boundary
+// flags; returns the interior faces (ascending) and their count.
+Buf make_index_sets(Core& c, const Buf& face_interior, const Buf& cell_boundary, eqg_set** builtin, int64_t& n_if)
+{
+    const int64_t nc64 = c.nc, nf64 = c.nf;
+    // index sets
+    auto make = [&](int entity, Buf idx, int64_t n, bool identity) {
+        auto* s = new eqg_set;
+        s->entity = entity;
+        s->n = n;
+        s->idx = idx;
+        s->identity = identity;
+        s->sorted = 1;
+        return s;
+    };
+    Buf all_c = c.allocN<int32_t>(nc64), all_f = c.allocN<int32_t>(nf64);
+    launch(c, "iota", [&] { iota_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(all_c->as<int32_t>(), nc64); });
+    launch(c, "iota", [&] { iota_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(all_f->as<int32_t>(), nf64); });
+    int64_t n_bc = 0, n_ic = 0, n_bf = 0;
+    n_if = 0;
+    Buf bc = compact_indices(c, cell_boundary->as<uint8_t>(), nc64, n_bc);
+    Buf not_b = c.allocN<uint8_t>(nc64 > nf64 ? nc64 : nf64);
+    launch(c, "negate", [&] { negate_u8_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(cell_boundary->as<uint8_t>(), not_b->as<uint8_t>(),
+                                                                 nc64); });
+    Buf ic = compact_indices(c, not_b->as<uint8_t>(), nc64, n_ic);
+    Buf iff = compact_indices(c, face_interior->as<uint8_t>(), nf64, n_if);
+    launch(c, "negate", [&] { negate_u8_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(face_interior->as<uint8_t>(), not_b->as<uint8_t>(),
+                                                                 nf64); });
+    Buf bf = compact_indices(c, not_b->as<uint8_t>(), nf64, n_bf);
+    c.nif = (int)n_if;
+    builtin[EQG_ALL_CELLS] = make(EQG_CELLS, all_c, nc64, true);
+    builtin[EQG_BOUNDARY_CELLS] = make(EQG_CELLS, bc, n_bc, false);
+    builtin[EQG_INTERIOR_CELLS] = make(EQG_CELLS, ic, n_ic, false);
+    builtin[EQG_ALL_FACES] = make(EQG_FACES, all_f, nf64, true);
+    builtin[EQG_BOUNDARY_FACES] = make(EQG_FACES, bf, n_bf, false);
+    builtin[EQG_INTERIOR_FACES] = make(EQG_FACES, iff, n_if, false);
+
+    return iff;
+}
+
+OpMatrixP new_opmatrix(Core& c, int n_out, int n_src, int max_row, int64_t nnz)
+{
+    auto m = std::make_shared<OpMatrix>();
+    m->id = c.newId();
+    m->n_out = n_out;
+    m->n_src = n_src;
+    m->max_row = max_row;
+    m->nnz = nnz;
+    m->ptr = c.allocN<int32_t>((size_t)n_out + 1);
+    m->src = c.allocN<int32_t>(nnz > 0 ? nnz : 1);
+    m->w = c.allocN<double>(nnz > 0 ? nnz : 1);
+    return m;
+}
+
+// grad = -ngrad and ngrad over the interior faces, from face_cells.
+void make_grad_ops(Core& c, const Buf& iff, int64_t n_if)
+{
+    c.grad = new_opmatrix(c, c.nif, c.nc, 2, 2 * n_if);
+    c.ngrad = new_opmatrix(c, c.nif, c.nc, 2, 2 * n_if);
+    if (c.nif > 0) {
+        launch(c, "grad_op", [&] { grad_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(c.nif, iff->as<int32_t>(), c.face_cells->as<int32_t>(),
+                                                                -1.0, c.grad->ptr->as<int32_t>(),
+                                                                c.grad->src->as<int32_t>(), c.grad->w->as<double>()); });
+        launch(c, "ngrad_op", [&] { grad_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(c.nif, iff->as<int32_t>(), c.face_cells->as<int32_t>(),
+                                                                1.0, c.ngrad->ptr->as<int32_t>(),
+                                                                c.ngrad->src->as<int32_t>(), c.ngrad->w->as<double>()); });
+    } else {
+        k_fill_i32(c, c.grad->ptr->as<int32_t>(), 0, 1);
+        k_fill_i32(c, c.ngrad->ptr->as<int32_t>(), 0, 1);
+    }
+}
+
+}  // namespace
+
 void build_grid(Core& c, eqg_set** builtin)
 {
     if (c.dim != 2 && c.dim != 3) fail(EQG_ERR_ARG, "Cannot handle " + std::to_string(c.dim) + " dimensions.");
@@ -471,64 +554,10 @@ void build_grid(Core& c, eqg_set** builtin)
                                                              c.cell_centroids->as<double>(),
                                                              cell_boundary->as<uint8_t>()); });
 
-    // index sets
-    auto make = [&](int entity, Buf idx, int64_t n, bool identity) {
-        auto* s = new eqg_set;
-        s->entity = entity;
-        s->n = n;
-        s->idx = idx;
-        s->identity = identity;
-        s->sorted = 1;
-        return s;
-    };
-    Buf all_c = c.allocN<int32_t>(nc64), all_f = c.allocN<int32_t>(nf64);
-    launch(c, "iota", [&] { iota_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(all_c->as<int32_t>(), nc64); });
-    launch(c, "iota", [&] { iota_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(all_f->as<int32_t>(), nf64); });
-    int64_t n_bc = 0, n_ic = 0, n_bf = 0, n_if = 0;
-    Buf bc = compact_indices(c, cell_boundary->as<uint8_t>(), nc64, n_bc);
-    Buf not_b = c.allocN<uint8_t>(nc64 > nf64 ? nc64 : nf64);
-    launch(c, "negate", [&] { negate_u8_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(cell_boundary->as<uint8_t>(), not_b->as<uint8_t>(),
-                                                                 nc64); });
-    Buf ic = compact_indices(c, not_b->as<uint8_t>(), nc64, n_ic);
-    Buf iff = compact_indices(c, face_interior->as<uint8_t>(), nf64, n_if);
-    launch(c, "negate", [&] { negate_u8_kernel<<<blocksFor(nf64), kThreads, 0, c.stream>>>(face_interior->as<uint8_t>(), not_b->as<uint8_t>(),
-                                                                 nf64); });
-    Buf bf = compact_indices(c, not_b->as<uint8_t>(), nf64, n_bf);
-    c.nif = (int)n_if;
-    builtin[EQG_ALL_CELLS] = make(EQG_CELLS, all_c, nc64, true);
-    builtin[EQG_BOUNDARY_CELLS] = make(EQG_CELLS, bc, n_bc, false);
-    builtin[EQG_INTERIOR_CELLS] = make(EQG_CELLS, ic, n_ic, false);
-    builtin[EQG_ALL_FACES] = make(EQG_FACES, all_f, nf64, true);
-    builtin[EQG_BOUNDARY_FACES] = make(EQG_FACES, bf, n_bf, false);
-    builtin[EQG_INTERIOR_FACES] = make(EQG_FACES, iff, n_if, false);
-
-    // helper operators
-    auto opm = [&](int n_out, int n_src, int max_row, int64_t nnz) {
-        auto m = std::make_shared<OpMatrix>();
-        m->id = c.newId();
-        m->n_out = n_out;
-        m->n_src = n_src;
-        m->max_row = max_row;
-        m->nnz = nnz;
-        m->ptr = c.allocN<int32_t>((size_t)n_out + 1);
-        m->src = c.allocN<int32_t>(nnz > 0 ? nnz : 1);
-        m->w = c.allocN<double>(nnz > 0 ? nnz : 1);
-        return m;
-    };
-    c.grad = opm(c.nif, c.nc, 2, 2 * n_if);
-    c.ngrad = opm(c.nif, c.nc, 2, 2 * n_if);
-    if (c.nif > 0) {
-        launch(c, "grad_op", [&] { grad_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(c.nif, iff->as<int32_t>(), c.face_cells->as<int32_t>(),
-                                                                -1.0, c.grad->ptr->as<int32_t>(),
-                                                                c.grad->src->as<int32_t>(), c.grad->w->as<double>()); });
-        launch(c, "ngrad_op", [&] { grad_kernel<<<blocksFor(n_if), kThreads, 0, c.stream>>>(c.nif, iff->as<int32_t>(), c.face_cells->as<int32_t>(),
-                                                                1.0, c.ngrad->ptr->as<int32_t>(),
-                                                                c.ngrad->src->as<int32_t>(), c.ngrad->w->as<double>()); });
-    } else {
-        k_fill_i32(c, c.grad->ptr->as<int32_t>(), 0, 1);
-        k_fill_i32(c, c.ngrad->ptr->as<int32_t>(), 0, 1);
-    }
-    c.div_full = opm(c.nc, c.nf, 2 * c.dim, (int64_t)2 * c.dim * nc64);
+    int64_t n_if = 0;
+    Buf iff = make_index_sets(c, face_interior, cell_boundary, builtin, n_if);
+    make_grad_ops(c, iff, n_if);
+    c.div_full = new_opmatrix(c, c.nc, c.nf, 2 * c.dim, (int64_t)2 * c.dim * nc64);
     launch(c, "div_full_op", [&] { div_full_kernel<<<blocksFor(nc64), kThreads, 0, c.stream>>>(d, c.div_full->ptr->as<int32_t>(),
                                                                 c.div_full->src->as<int32_t>(),
                                                                 c.div_full->w->as<double>()); });
@@ -558,6 +587,235 @@ void build_grid(Core& c, eqg_set** builtin)
                                                                               m->w->as<double>()); });
         c.div_interior = m;
     }
+    c.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Grids read from a file (parameter grid_filename; the reference builds
+// Opm::GridManager(grid_filename), EquelleRuntimeCPU.cpp:20-24).
+//
+// The file holds the arrays of an UnstructuredGrid that the runtime uses, as
+// whitespace-separated text, each array after its keyword:
+//
+//   eqg-grid 1
+//   dimensions <2|3>  cells <nc>  faces <nf>
+//   face_cells      2 nf integers: first and second cell of each face (-1: outside)
+//   cell_facepos    nc + 1 integers: cell c's faces are cell_faces[facepos[c] .. facepos[c+1])
+//   cell_faces      facepos[nc] integers
+//   face_areas      nf reals
+//   face_centroids  dim nf reals, face by face (x y [z] of face 0, then face 1, ...)
+//   face_normals    dim nf reals, face by face, scaled by the face area, from the
+//                   first cell toward the second
+//   cell_volumes    nc reals
+//   cell_centroids  dim nc reals, cell by cell
+//
+// equelle_b200/grids.py writes it.  Every face must have at least one cell
+// and two different cells when it has two, and each cell's face list must
+// hold exactly the faces that name the cell.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct FileGrid {
+    int dim = 0;
+    int64_t nc = 0, nf = 0;
+    std::vector<int32_t> face_cells, cell_facepos, cell_faces;
+    std::vector<double> face_areas, face_centroids, face_normals, cell_volumes, cell_centroids;
+};
+
+class GridTokens {
+public:
+    GridTokens(const std::string& path) : path_(path)
+    {
+        std::ifstream f(path.c_str(), std::ios::binary);
+        if (!f) fail(EQG_ERR_ARG, "Failed to read grid from file " + path);
+        std::ostringstream ss;
+        ss << f.rdbuf();
+        text_ = ss.str();
+        p_ = text_.c_str();
+    }
+    std::string word()
+    {
+        skip();
+        const char* b = p_;
+        while (*p_ && !std::isspace((unsigned char)*p_)) ++p_;
+        return std::string(b, p_);
+    }
+    void expect(const char* key)
+    {
+        const std::string w = word();
+        if (w != key) fail(EQG_ERR_ARG, "grid file " + path_ + ": expected '" + key + "', found '" + w + "'");
+    }
+    long long integer()
+    {
+        skip();
+        char* e = nullptr;
+        errno = 0;
+        const long long v = std::strtoll(p_, &e, 10);
+        if (e == p_ || errno) fail(EQG_ERR_ARG, "grid file " + path_ + ": expected an integer");
+        p_ = e;
+        return v;
+    }
+    double real()
+    {
+        skip();
+        char* e = nullptr;
+        const double v = std::strtod(p_, &e);
+        if (e == p_) fail(EQG_ERR_ARG, "grid file " + path_ + ": expected a number");
+        p_ = e;
+        return v;
+    }
+    template <class T>
+    void ints(const char* key, int64_t n, std::vector<T>& out)
+    {
+        expect(key);
+        out.resize(n);
+        for (int64_t i = 0; i < n; ++i) out[i] = (T)integer();
+    }
+    void reals(const char* key, int64_t n, std::vector<double>& out)
+    {
+        expect(key);
+        out.resize(n);
+        for (int64_t i = 0; i < n; ++i) out[i] = real();
+    }
+
+private:
+    void skip()
+    {
+        while (*p_ && std::isspace((unsigned char)*p_)) ++p_;
+    }
+    std::string path_, text_;
+    const char* p_ = nullptr;
+};
+
+FileGrid read_grid_file(const std::string& path)
+{
+    GridTokens t(path);
+    FileGrid g;
+    t.expect("eqg-grid");
+    if (t.integer() != 1) fail(EQG_ERR_ARG, "grid file " + path + ": unknown format version");
+    t.expect("dimensions");
+    g.dim = (int)t.integer();
+    t.expect("cells");
+    g.nc = t.integer();
+    t.expect("faces");
+    g.nf = t.integer();
+    if (g.dim != 2 && g.dim != 3) fail(EQG_ERR_ARG, "Cannot handle " + std::to_string(g.dim) + " dimensions.");
+    if (g.nc < 1 || g.nf < 1 || 2 * g.nf > (int64_t)INT32_MAX || g.nc > (int64_t)INT32_MAX)
+        fail(EQG_ERR_ARG, "grid file " + path + ": cell or face count out of range");
+    t.ints("face_cells", 2 * g.nf, g.face_cells);
+    t.ints("cell_facepos", g.nc + 1, g.cell_facepos);
+    if (g.cell_facepos[0] != 0) fail(EQG_ERR_ARG, "grid file " + path + ": cell_facepos must start at 0");
+    for (int64_t c = 0; c < g.nc; ++c)
+        if (g.cell_facepos[c + 1] < g.cell_facepos[c])
+            fail(EQG_ERR_ARG, "grid file " + path + ": cell_facepos must not decrease");
+    t.ints("cell_faces", g.cell_facepos[g.nc], g.cell_faces);
+    t.reals("face_areas", g.nf, g.face_areas);
+    t.reals("face_centroids", g.dim * g.nf, g.face_centroids);
+    t.reals("face_normals", g.dim * g.nf, g.face_normals);
+    t.reals("cell_volumes", g.nc, g.cell_volumes);
+    t.reals("cell_centroids", g.dim * g.nc, g.cell_centroids);
+    // topology checks: faces name valid, distinct cells; each cell's list
+    // holds exactly the faces naming it
+    std::vector<int64_t> named(g.nc, 0);
+    for (int64_t f = 0; f < g.nf; ++f) {
+        const int32_t a = g.face_cells[2 * f], b = g.face_cells[2 * f + 1];
+        if (a < -1 || a >= g.nc || b < -1 || b >= g.nc || (a < 0 && b < 0) || a == b)
+            fail(EQG_ERR_ARG, "grid file " + path + ": face " + std::to_string(f) + " has invalid cells");
+        if (a >= 0) named[a]++;
+        if (b >= 0) named[b]++;
+    }
+    for (int64_t c = 0; c < g.nc; ++c) {
+        if (g.cell_facepos[c + 1] - g.cell_facepos[c] != named[c])
+            fail(EQG_ERR_ARG, "grid file " + path + ": face list of cell " + std::to_string(c) +
+                                 " does not match face_cells");
+        for (int32_t k = g.cell_facepos[c]; k < g.cell_facepos[c + 1]; ++k) {
+            const int32_t f = g.cell_faces[k];
+            if (f < 0 || f >= g.nf || (g.face_cells[2 * (int64_t)f] != c && g.face_cells[2 * (int64_t)f + 1] != c))
+                fail(EQG_ERR_ARG, "grid file " + path + ": face list of cell " + std::to_string(c) +
+                                     " does not match face_cells");
+        }
+    }
+    return g;
+}
+
+// face by face (f dim + d) -> component-major (d n + f)
+std::vector<double> component_major(const std::vector<double>& v, int dim, int64_t n)
+{
+    std::vector<double> out(v.size());
+    for (int64_t i = 0; i < n; ++i)
+        for (int d = 0; d < dim; ++d) out[(size_t)d * n + i] = v[(size_t)i * dim + d];
+    return out;
+}
+
+template <class T>
+Buf upload(Core& c, const std::vector<T>& v)
+{
+    Buf b = c.allocN<T>(v.empty() ? 1 : v.size());
+    if (!v.empty()) EQG_CUDA(cudaMemcpyAsync(b->ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+    return b;
+}
+
+}  // namespace
+
+void build_grid_from_file(Core& c, const std::string& path, eqg_set** builtin)
+{
+    const FileGrid g = read_grid_file(path);
+    c.cartesian = false;
+    c.dim = g.dim;
+    c.nx = c.ny = c.nz = 0;
+    c.dx = c.dy = c.dz = 0.0;
+    c.nc = (int)g.nc;
+    c.nf = (int)g.nf;
+    c.face_cells = upload(c, g.face_cells);
+    c.face_areas = upload(c, g.face_areas);
+    c.face_centroids = upload(c, component_major(g.face_centroids, g.dim, g.nf));
+    c.face_normals = upload(c, component_major(g.face_normals, g.dim, g.nf));
+    c.cell_volumes = upload(c, g.cell_volumes);
+    c.cell_centroids = upload(c, component_major(g.cell_centroids, g.dim, g.nc));
+    // interior faces: two cells; boundary cells: a face with an outside side
+    // (EquelleRuntimeCPU::boundaryCell, EquelleRuntimeCPU.cpp:94-104)
+    std::vector<uint8_t> interior(g.nf), boundary(g.nc, 0);
+    for (int64_t f = 0; f < g.nf; ++f) {
+        const int32_t a = g.face_cells[2 * f], b = g.face_cells[2 * f + 1];
+        interior[f] = (a >= 0 && b >= 0) ? 1 : 0;
+        if (!interior[f]) boundary[a >= 0 ? a : b] = 1;
+    }
+    Buf face_interior = upload(c, interior), cell_boundary = upload(c, boundary);
+    int64_t n_if = 0;
+    Buf iff = make_index_sets(c, face_interior, cell_boundary, builtin, n_if);
+    make_grad_ops(c, iff, n_if);
+    // fulldiv = fullngrad^T and div = ngrad^T: row c holds the faces of cell
+    // c in ascending order, +1 where c is the face's first cell, -1 where it
+    // is the second (the transpose of a face-by-face matrix has its columns
+    // in ascending order)
+    std::vector<int32_t> ipos(g.nf, -1);
+    {
+        int32_t k = 0;
+        for (int64_t f = 0; f < g.nf; ++f)
+            if (interior[f]) ipos[f] = k++;
+    }
+    std::vector<int32_t> fptr(g.nc + 1, 0), fsrc, iptr(g.nc + 1, 0), isrc;
+    std::vector<double> fw, iw;
+    int max_row = 0;
+    for (int64_t cc = 0; cc < g.nc; ++cc) {
+        std::vector<int32_t> faces(g.cell_faces.begin() + g.cell_facepos[cc],
+                                   g.cell_faces.begin() + g.cell_facepos[cc + 1]);
+        std::sort(faces.begin(), faces.end());
+        max_row = std::max(max_row, (int)faces.size());
+        for (int32_t f : faces) {
+            const double sign = g.face_cells[2 * (int64_t)f] == cc ? 1.0 : -1.0;
+            fsrc.push_back(f);
+            fw.push_back(sign);
+            if (ipos[f] >= 0) {
+                isrc.push_back(ipos[f]);
+                iw.push_back(sign);
+            }
+        }
+        fptr[cc + 1] = (int32_t)fsrc.size();
+        iptr[cc + 1] = (int32_t)isrc.size();
+    }
+    c.div_full = opmat_from_host(c, c.nc, c.nf, fptr, fsrc, fw);
+    c.div_interior = opmat_from_host(c, c.nc, c.nif, iptr, isrc, iw);
     c.sync();
 }
 

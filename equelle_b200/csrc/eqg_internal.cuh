@@ -155,7 +155,9 @@ struct Core {
     int dim = 2, nx = 6, ny = 1, nz = 1;
     double dx = 1, dy = 1, dz = 1;
     int nc = 0, nf = 0, nif = 0;
+    bool cartesian = true;  // false: read from a grid file (grid_filename); nx = ny = nz = 0
     Buf face_cells;      // int32[2*nf]
+    Buf face_normals;    // double[dim*nf], area-scaled (component-major); grids read from a file only
     Buf face_areas;      // double[nf]
     Buf face_centroids;  // double[dim*nf] (component-major: d*nf + f)
     Buf cell_volumes;    // double[nc]

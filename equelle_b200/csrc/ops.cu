@@ -177,6 +177,29 @@ __global__ void normal_kernel(const int32_t* faces, const double* areas, double*
     }
 }
 
+// Unit normal component of grids read from a file: the area-scaled normal
+// over its Euclidean norm (EquelleRuntimeCPU::normal,
+// EquelleRuntimeCPU.cpp:295-314), the squares summed in component order.
+__global__ void normal_file_kernel(const int32_t* faces, const double* normals, double* out, int comp, int dim,
+                                   int nf, int64_t n, int32_t* err)
+{
+    GRID_STRIDE(i, n)
+    {
+        const int32_t f = faces[i];
+        if (f < 0 || f >= nf) {
+            *err = 1;
+            out[i] = 0.0;
+            continue;
+        }
+        double nn = 0.0;
+        for (int d = 0; d < dim; ++d) {
+            const double v = normals[(int64_t)d * nf + f];
+            nn += v * v;
+        }
+        out[i] = normals[(int64_t)comp * nf + f] / sqrt(nn);
+    }
+}
+
 // Position of each key in a strictly ascending array (binary search), or in
 // the identity enumeration 0..identity_n-1 when sorted == nullptr.
 __global__ void locate_kernel(const int32_t* sorted, int64_t n_sorted, const int32_t* keys, int32_t* pos,
@@ -379,6 +402,13 @@ void k_gather_f64(Core& c, const double* data, const int32_t* idx, int stride, i
 void k_normal(Core& c, const int32_t* faces, double* out, int comp, int64_t n, int32_t* err)
 {
     if (n <= 0) return;
+    if (!c.cartesian) {
+        launch(c, "normal", [&] {
+            normal_file_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(faces, c.face_normals->as<double>(), out, comp,
+                                                                       c.dim, c.nf, n, err);
+        });
+        return;
+    }
     const int fx = (c.nx + 1) * c.ny * c.nz;
     const int fy = c.nx * (c.ny + 1) * c.nz;
     launch(c, "normal", [&] { normal_kernel<<<blocksFor(n), kThreads, 0, c.stream>>>(faces, c.face_areas->as<double>(), out, comp, c.dim, c.nf,

@@ -2055,7 +2055,8 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     const int ncomp = (c.nc > 0 && n % c.nc == 0) ? n / c.nc : 0;
     // coarsening stops at linsolver_mg_coarsest unknowns (at most kCoarsest)
     const int coarsest = std::max(1, std::min(kCoarsest, c.param_i("linsolver_mg_coarsest", kCoarsest)));
-    const bool mg_wanted = pre == "multigrid" && ncomp >= 1 && ncomp <= 8 && n > coarsest;
+    // (the aggregation is geometric: Cartesian grids only)
+    const bool mg_wanted = pre == "multigrid" && c.cartesian && ncomp >= 1 && ncomp <= 8 && n > coarsest;
     // Block ILU(0) sweeps with FP32 vectors (precision "refine") converge much
     // more slowly than scalar ones on the two-phase systems; with FP64
     // vectors, FP32 matrix values ("mixed") do not change the iteration

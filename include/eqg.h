@@ -136,8 +136,13 @@ const char* eqg_backend_name(void);
  * defer value-only elementwise operations and evaluate them in batches),
  * host_threads (0: OpenMP's default for the solver analysis), time_kernel
  * (a kernel name, or "*", to time with CUDA events) and device (CUDA device
- * index; default: the calling thread's current device).  grid_filename is
- * rejected with EQG_ERR_UNSUPPORTED.
+ * index; default: the calling thread's current device).  grid_filename
+ * (instead of grid_dim, nx, ...) reads the grid from a file: the arrays of an
+ * UnstructuredGrid (face_cells, cell_facepos, cell_faces, face areas,
+ * centroids and area-scaled normals, cell volumes and centroids) as text
+ * after the header "eqg-grid 1" (layout: equelle_b200/grids.py, which writes
+ * it); such a grid reports nx = ny = nz = 0, and its linear solves use block
+ * ILU(0) (the multigrid preconditioner coarsens Cartesian grids only).
  * Replaces EquelleRuntimeCPU::EquelleRuntimeCPU(const ParameterGroup&)
  * and createGridManager (backends/serial/src/EquelleRuntimeCPU.cpp:20-65). */
 int eqg_runtime_create(int nparams, const char* const* keys, const char* const* values,

@@ -44,6 +44,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -449,6 +450,74 @@ Grid build_grid(int dim, int nx, int ny, int nz, double dx, double dy, double dz
     return g;
 }
 
+// A grid read from a file (grid_filename; the reference's
+// Opm::GridManager(grid_filename), EquelleRuntimeCPU.cpp:20-24): the
+// UnstructuredGrid arrays after the header "eqg-grid 1", each after its
+// keyword, as whitespace-separated text (the layout equelle_b200/grids.py
+// writes).  nx = ny = nz = 0 mark it as not Cartesian.
+Grid read_grid_file(const std::string& path)
+{
+    std::ifstream in(path.c_str());
+    if (!in) fail(EQG_ERR_ARG, "Failed to read grid from file " + path);
+    auto expect = [&](const char* key) {
+        std::string w;
+        in >> w;
+        if (w != key) fail(EQG_ERR_ARG, "grid file " + path + ": expected '" + key + "', found '" + w + "'");
+    };
+    auto number = [&](auto& v) {
+        if (!(in >> v)) fail(EQG_ERR_ARG, "grid file " + path + ": expected a number");
+    };
+    Grid g;
+    int version = 0;
+    expect("eqg-grid");
+    number(version);
+    if (version != 1) fail(EQG_ERR_ARG, "grid file " + path + ": unknown format version");
+    expect("dimensions");
+    number(g.dim);
+    expect("cells");
+    number(g.nc);
+    expect("faces");
+    number(g.nf);
+    if (g.dim != 2 && g.dim != 3) fail(EQG_ERR_ARG, "Cannot handle " + std::to_string(g.dim) + " dimensions.");
+    if (g.nc < 1 || g.nf < 1) fail(EQG_ERR_ARG, "grid file " + path + ": cell or face count out of range");
+    g.nx = g.ny = g.nz = 0;
+    g.dx = g.dy = g.dz = 0.0;
+    auto read_ints = [&](const char* key, int64_t n, auto& v) {
+        expect(key);
+        v.resize(n);
+        for (auto& x : v) number(x);
+    };
+    auto read_reals = [&](const char* key, int64_t n, std::vector<double>& v) {
+        expect(key);
+        v.resize(n);
+        for (auto& x : v) number(x);
+    };
+    read_ints("face_cells", 2 * g.nf, g.face_cells);
+    read_ints("cell_facepos", g.nc + 1, g.cell_facepos);
+    for (int64_t c = 0; c < g.nc; ++c)
+        if (g.cell_facepos[c + 1] < g.cell_facepos[c] || g.cell_facepos[0] != 0)
+            fail(EQG_ERR_ARG, "grid file " + path + ": bad cell_facepos");
+    read_ints("cell_faces", g.cell_facepos[g.nc], g.cell_faces);
+    read_reals("face_areas", g.nf, g.face_areas);
+    read_reals("face_centroids", g.dim * g.nf, g.face_centroids);
+    read_reals("face_normals", g.dim * g.nf, g.face_normals);
+    read_reals("cell_volumes", g.nc, g.cell_volumes);
+    read_reals("cell_centroids", g.dim * g.nc, g.cell_centroids);
+    for (int64_t f = 0; f < g.nf; ++f) {
+        const int32_t a = g.face_cells[2 * f], b = g.face_cells[2 * f + 1];
+        if (a < -1 || a >= g.nc || b < -1 || b >= g.nc || (a < 0 && b < 0) || a == b)
+            fail(EQG_ERR_ARG, "grid file " + path + ": face " + std::to_string(f) + " has invalid cells");
+    }
+    for (int64_t c = 0; c < g.nc; ++c)
+        for (int64_t k = g.cell_facepos[c]; k < g.cell_facepos[c + 1]; ++k) {
+            const int32_t f = g.cell_faces[k];
+            if (f < 0 || f >= g.nf || (g.face_cells[2 * (int64_t)f] != c && g.face_cells[2 * (int64_t)f + 1] != c))
+                fail(EQG_ERR_ARG, "grid file " + path + ": face list of cell " + std::to_string(c) +
+                                      " does not match face_cells");
+        }
+    return g;
+}
+
 // HelperOps, construction as in backends/cuda/src/deviceHelperOps.cpp:84-148.
 struct HelperOps {
     std::vector<int32_t> internal_faces;
@@ -837,13 +906,15 @@ int eqg_runtime_create(int nparams, const char* const* keys, const char* const* 
         need(out, "out");
         auto rt = std::make_unique<eqg_runtime>();
         for (int i = 0; i < nparams; ++i) rt->params[keys[i]] = values[i];
-        if (rt->params.count("grid_filename"))
-            fail(EQG_ERR_UNSUPPORTED, "grid_filename: unstructured grid input is not supported");
-        const int dim = param_i(rt.get(), "grid_dim", 2);
-        if (dim != 2 && dim != 3) fail(EQG_ERR_ARG, "Cannot handle " + std::to_string(dim) + " dimensions.");
-        rt->grid = build_grid(dim, param_i(rt.get(), "nx", 6), param_i(rt.get(), "ny", 1),
-                              param_i(rt.get(), "nz", 1), param_d(rt.get(), "dx", 1.0),
-                              param_d(rt.get(), "dy", 1.0), param_d(rt.get(), "dz", 1.0));
+        if (rt->params.count("grid_filename")) {
+            rt->grid = read_grid_file(rt->params["grid_filename"]);
+        } else {
+            const int dim = param_i(rt.get(), "grid_dim", 2);
+            if (dim != 2 && dim != 3) fail(EQG_ERR_ARG, "Cannot handle " + std::to_string(dim) + " dimensions.");
+            rt->grid = build_grid(dim, param_i(rt.get(), "nx", 6), param_i(rt.get(), "ny", 1),
+                                  param_i(rt.get(), "nz", 1), param_d(rt.get(), "dx", 1.0),
+                                  param_d(rt.get(), "dy", 1.0), param_d(rt.get(), "dz", 1.0));
+        }
         rt->ops = build_ops(rt->grid);
         rt->verbose = param_i(rt.get(), "verbose", 0);
         rt->max_iter = param_i(rt.get(), "max_iter", 10);
