@@ -84,6 +84,7 @@ Core::~Core()
     div_interior.reset();
     div_full.reset();
     face_cells.reset();
+    face_normals.reset();
     face_areas.reset();
     face_centroids.reset();
     cell_volumes.reset();

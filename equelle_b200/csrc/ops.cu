@@ -191,10 +191,12 @@ __global__ void normal_file_kernel(const int32_t* faces, const double* normals, 
             out[i] = 0.0;
             continue;
         }
+        // separately rounded products and sums (no fused multiply-add), as
+        // the reference's Eigen row norm computes them
         double nn = 0.0;
         for (int d = 0; d < dim; ++d) {
             const double v = normals[(int64_t)d * nf + f];
-            nn += v * v;
+            nn = __dadd_rn(nn, __dmul_rn(v, v));
         }
         out[i] = normals[(int64_t)comp * nf + f] / sqrt(nn);
     }
