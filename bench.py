@@ -39,13 +39,15 @@ sys.path.insert(0, ROOT)
 SPMV_KERNEL = "bicg_spmv_omega"
 # DRAM bytes (read + write) that ncu measured for one launch of a kernel
 # against its algorithmic bytes, on the FP64 2 x 2 block layout of the
-# two-phase 128x128x48 case (profiles/solver_kernels_twophase_128x128x48.md).
+# two-phase 128x128x48 case (profiles/solver_kernels_twophase_128x128x48.md,
+# profiles/bilu_upper_kernel_twophase_128x128x48.md).
 # Both scale with the number of blocks, so a launch of the same layout on
 # another grid moves this ratio times its algorithmic bytes.
 TRAFFIC_RATIO = {
     "bicg_spmv_omega": 242.5 / 237.0,
     "mg_residual": 245.5 / 237.0,
     "bilu_lower": 114.8 / 118.5,
+    "bilu_upper": 116.6 / 118.5,
 }
 
 # Kernels of one BiCGStab iteration (its V-cycles, SpMVs and vector steps),
