@@ -72,8 +72,12 @@ def parse():
                     default="twophase3d")
     ap.add_argument("--instances", type=int, default=64, help="batched: number of instances")
     ap.add_argument("--requests", type=int, default=48, help="serve: requests per arrival rate")
-    ap.add_argument("--rates", default="50,200,1000", help="serve: Poisson arrival rates (req/s)")
+    ap.add_argument("--rates", default="50,200,1000,2000", help="serve: Poisson arrival rates (req/s)")
     ap.add_argument("--slots", type=int, default=32, help="batched/serve: instances on the GPU at once")
+    ap.add_argument("--seq-sample", type=int, default=128,
+                    help="batched: instances of the sequential FP64 arm (the first ones of the same seeded set)")
+    ap.add_argument("--side-max", type=int, default=None, help="batched/serve: largest grid side")
+    ap.add_argument("--max-steps", type=int, default=None, help="serve: most time steps of a request")
     ap.add_argument("--nx", type=int)
     ap.add_argument("--ny", type=int)
     ap.add_argument("--nz", type=int)
@@ -561,8 +565,15 @@ def main_many(a, rp):
                 "errors": sum(1 for r in recs if r.error)}
 
     if a.workload == "batched":
-        reqs = serve.make_requests(a.instances, seed=1, programs=("twophase",), side=(32, 512), steps=(a.steps, a.steps))
-        seq = summary(*serve.Server(slots=1).run(prepared(reqs, "double"), realtime=False))
+        side_max = a.side_max or 512
+        reqs = serve.make_requests(a.instances, seed=1, programs=("twophase",), side=(32, side_max),
+                                   steps=(a.steps, a.steps))
+        # the sequential plain-FP64 arm on the first seq_sample instances of
+        # the same seeded set (instance-steps/s)
+        seq_reqs = serve.make_requests(min(a.seq_sample, a.instances), seed=1, programs=("twophase",),
+                                       side=(32, side_max), steps=(a.steps, a.steps))
+        seq = summary(*serve.Server(slots=1).run(prepared(seq_reqs, "double"), realtime=False))
+        bat64 = summary(*serve.Server(slots=a.slots).run(prepared(reqs, "double"), realtime=False))
         with ClockSampler(rp.local_rank) as clk:
             bat = summary(*serve.Server(slots=a.slots).run(prepared(reqs, "mixed"), realtime=False))
         value = rp.throughput(bat["instance_steps"], 1000.0 * rp.max(bat["wall_s"]))
@@ -570,20 +581,24 @@ def main_many(a, rp):
                 "steps": a.steps, "warmup": 0, "ms_per_step": 1000.0 * bat["wall_s"] / bat["instance_steps"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
                 "data": "synthetic (seeded log-permeability per instance, corner wells)",
-                "config": {"workload": "%d 2D two-phase instances, sides log-uniform in [32, 512], %d steps each, "
+                "config": {"workload": "%d 2D two-phase instances, sides log-uniform in [32, %d], %d steps each, "
                                        "%d on the GPU at once (own runtime, stream and host thread each)"
-                                       % (a.instances, a.steps, a.slots), "precision": "mixed (batched), "
-                                       "double (sequential)", "parallelism": "replicas"},
-                "batched": bat, "sequential_fp64": seq,
+                                       % (a.instances, side_max, a.steps, a.slots),
+                           "precision": "mixed (batched), double (sequential and batched_fp64)",
+                           "sequential_sample": "the first %d of the same instances" % len(seq_reqs),
+                           "parallelism": "replicas"},
+                "batched": bat, "batched_fp64": bat64, "sequential_fp64": seq,
                 "speedup_vs_sequential": bat["instance_steps_per_s"] / seq["instance_steps_per_s"],
+                "speedup_vs_sequential_same_precision": bat64["instance_steps_per_s"] / seq["instance_steps_per_s"],
                 "clocks": clk.summary()}
     else:
         rates = [float(x) for x in a.rates.split(",")]
         per_rate = {}
-        base = serve.make_requests(a.requests, seed=2, side=(64, 512), steps=(10, 30))
+        side_max, max_steps = a.side_max or 1024, a.max_steps or 100
+        base = serve.make_requests(a.requests, seed=2, side=(64, side_max), steps=(10, max_steps))
         seq = summary(*serve.Server(slots=1).run(prepared(base, "double"), realtime=False))
         for lam in rates:
-            reqs = serve.make_requests(a.requests, seed=2, rate=lam, side=(64, 512), steps=(10, 30))
+            reqs = serve.make_requests(a.requests, seed=2, rate=lam, side=(64, side_max), steps=(10, max_steps))
             recs, wall = serve.Server(slots=a.slots).run(prepared(reqs, "mixed"), realtime=True)
             per_rate["%g" % lam] = summary(recs, wall)
         top = per_rate["%g" % rates[-1]]
@@ -591,8 +606,8 @@ def main_many(a, rp):
                 "unit": "requests/s",
                 "n_gpus": world, "steps": a.requests, "warmup": 0, "ms_per_step": 1000.0 / top["requests_per_s"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
-                "data": "synthetic (seeded requests: heat or 2D two-phase, sides log-uniform in [64, 512], "
-                        "10-30 steps)",
+                "data": "synthetic (seeded requests: heat or 2D two-phase, sides log-uniform in [64, %d], "
+                        "10-%d steps)" % (side_max, max_steps),
                 "config": {"workload": "serving loop, Poisson arrivals at %s req/s, %d requests per rate, up to %d on "
                                        "the GPU at once, admission under 150 GB" % (a.rates, a.requests, a.slots),
                            "parallelism": "replicas"},

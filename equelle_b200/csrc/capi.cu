@@ -1238,7 +1238,20 @@ int eqg_span_superset(eqg_runtime* rt, const eqg_coll* a, int64_t start, int64_t
         need(a, "collection");
         if (start < 0 || start + a->n > total) fail(EQG_ERR_ARG, "span out of range");
         OpMatrixP m = span_matrix(*rt->core, MAP_SUPERSET, start, a->n, a->n, total);
-        *out = apply_operator(rt->core, *m, a);
+        Core& c = *rt->core;
+        if (!a->pat || c.param_i("span_share", 1) == 0) {
+            *out = apply_operator(rt->core, *m, a);
+            return;
+        }
+        // The superset only inserts empty Jacobian rows: the product keeps
+        // every entry, in order, with weight 1, so the result shares the
+        // operand's Jacobian values (collections are immutable) under the
+        // superset pattern.
+        Buf val = c.allocN<double>(total > 0 ? total : 1);
+        opmat_apply_values(c, *m, coll_values(c, a), val->as<double>());
+        PatternP p = pattern_spgemm(c, *m, a->pat, false);
+        if (p->nnz != a->pat->nnz) fail(EQG_ERR_DEVICE, "span superset changed the number of Jacobian entries");
+        *out = new_coll(rt->core, total, val, p, a->jval);
     });
 }
 

@@ -413,6 +413,95 @@ __global__ void negate_u8_kernel(const uint8_t* a, uint8_t* out, int64_t n)
     GRID_STRIDE(i, n) out[i] = !a[i];
 }
 
+// ---------------------------------------------------------------------------
+// Cartesian stencils: ngrad/grad over the interior faces and fulldiv/div
+// over the cells, applied to values by face and cell index arithmetic
+// instead of through their CSR operator matrices.  Interior faces come in
+// ascending face order: x faces with 0 < i < nx (i fastest), then y faces
+// with 0 < j < ny, then z faces with 0 < k < nz.  Each value is the CSR
+// row's sum in its order (ascending column), with the weights +-1:
+//   ngrad x (face) = x[first] - x[second], grad = -ngrad;
+//   div f (cell)   = sum over the cell's faces in ascending face order of
+//                    -f (the cell is the face's second cell) or +f (first).
+// ---------------------------------------------------------------------------
+struct InteriorCounts {
+    int64_t x, y, z;
+};
+
+__host__ __device__ inline InteriorCounts interior_counts(const Dims& d)
+{
+    InteriorCounts n;
+    n.x = (int64_t)(d.nx - 1) * d.ny * d.nz;
+    n.y = (int64_t)d.nx * (d.ny - 1) * d.nz;
+    n.z = d.dim == 3 ? (int64_t)d.nx * d.ny * (d.nz - 1) : 0;
+    return n;
+}
+
+__global__ void stencil_grad_kernel(Dims d, InteriorCounts ni, int first_minus_second, const double* __restrict__ x,
+                                    double* __restrict__ y, int64_t n)
+{
+    GRID_STRIDE(t, n)
+    {
+        int64_t c0, step;
+        if (t < ni.x) {
+            const int64_t i = t % (d.nx - 1) + 1, r = t / (d.nx - 1);
+            c0 = (i - 1) + (int64_t)d.nx * r;
+            step = 1;
+        } else if (t < ni.x + ni.y) {
+            const int64_t u = t - ni.x, i = u % d.nx, r = u / d.nx;
+            const int64_t j = r % (d.ny - 1) + 1, k = r / (d.ny - 1);
+            c0 = i + (int64_t)d.nx * ((j - 1) + (int64_t)d.ny * k);
+            step = d.nx;
+        } else {
+            const int64_t u = t - ni.x - ni.y, i = u % d.nx, r = u / d.nx;
+            const int64_t j = r % d.ny, k = r / d.ny + 1;
+            c0 = i + (int64_t)d.nx * (j + (int64_t)d.ny * (k - 1));
+            step = (int64_t)d.nx * d.ny;
+        }
+        const double a = x[c0], b = x[c0 + step];
+        y[t] = first_minus_second ? a - b : b - a;
+    }
+}
+
+template <bool INTERIOR>
+__global__ void stencil_div_kernel(Dims d, InteriorCounts ni, const double* __restrict__ f, double* __restrict__ y)
+{
+    GRID_STRIDE(c, d.nc)
+    {
+        const int64_t i = c % d.nx, r = c / d.nx, j = r % d.ny, k = r / d.ny;
+        double acc = 0.0;
+        if (!INTERIOR) {
+            const int64_t xl = i + (int64_t)(d.nx + 1) * (j + (int64_t)d.ny * k);
+            const int64_t yl = d.fx + i + (int64_t)d.nx * (j + (int64_t)(d.ny + 1) * k);
+            acc = acc - f[xl];
+            acc = acc + f[xl + 1];
+            acc = acc - f[yl];
+            acc = acc + f[yl + d.nx];
+            if (d.dim == 3) {
+                const int64_t zl = (int64_t)d.fx + d.fy + i + (int64_t)d.nx * (j + (int64_t)d.ny * k);
+                acc = acc - f[zl];
+                acc = acc + f[zl + (int64_t)d.nx * d.ny];
+            }
+        } else {
+            // interior position of the x face at i (0 < i < nx), of the y face
+            // at j (0 < j < ny), of the z face at k (0 < k < nz)
+            const int64_t xr = (int64_t)(d.nx - 1) * (j + (int64_t)d.ny * k);
+            if (i > 0) acc = acc - f[(i - 1) + xr];
+            if (i < d.nx - 1) acc = acc + f[i + xr];
+            const int64_t yr = ni.x + i + (int64_t)d.nx * ((int64_t)(d.ny - 1) * k);
+            if (j > 0) acc = acc - f[yr + (int64_t)d.nx * (j - 1)];
+            if (j < d.ny - 1) acc = acc + f[yr + (int64_t)d.nx * j];
+            if (d.dim == 3) {
+                const int64_t zr = ni.x + ni.y + i + (int64_t)d.nx * j;
+                const int64_t plane = (int64_t)d.nx * d.ny;
+                if (k > 0) acc = acc - f[zr + plane * (k - 1)];
+                if (k < d.nz - 1) acc = acc + f[zr + plane * k];
+            }
+        }
+        y[c] = acc;
+    }
+}
+
 }  // namespace
 
 // Indices i in [0, n) with flags[i] != 0, ascending.
@@ -588,7 +677,63 @@ void build_grid(Core& c, eqg_set** builtin)
                                                                               m->w->as<double>()); });
         c.div_interior = m;
     }
+    c.grad->stencil = STENCIL_GRAD;
+    c.ngrad->stencil = STENCIL_NGRAD;
+    c.div_full->stencil = STENCIL_DIV_FULL;
+    c.div_interior->stencil = STENCIL_DIV_INTERIOR;
     c.sync();
+}
+
+namespace {
+
+Dims core_dims(const Core& c)
+{
+    Dims d;
+    d.dim = c.dim;
+    d.nx = c.nx;
+    d.ny = c.ny;
+    d.nz = c.nz;
+    d.dx = c.dx;
+    d.dy = c.dy;
+    d.dz = c.dz;
+    d.fx = (c.nx + 1) * c.ny * c.nz;
+    d.fy = c.nx * (c.ny + 1) * c.nz;
+    d.fz = c.dim == 3 ? c.nx * c.ny * (c.nz + 1) : 0;
+    d.nf = c.nf;
+    d.nc = c.nc;
+    return d;
+}
+
+}  // namespace
+
+bool stencil_apply_values(Core& c, int kind, const double* x, double* y)
+{
+    if (!c.cartesian) return false;
+    const Dims d = core_dims(c);
+    const InteriorCounts ni = interior_counts(d);
+    switch (kind) {
+    case STENCIL_GRAD:
+    case STENCIL_NGRAD:
+        if (c.nif <= 0) return true;
+        // the interior face values written, two cell values read per face
+        launch(c, "stencil_grad", [&] {
+            stencil_grad_kernel<<<blocksFor(c.nif), kThreads, 0, c.stream>>>(d, ni, kind == STENCIL_NGRAD ? 1 : 0, x,
+                                                                           y, c.nif);
+        }, 8.0 * c.nif + 8.0 * c.nc);
+        return true;
+    case STENCIL_DIV_FULL:
+        launch(c, "stencil_div", [&] {
+            stencil_div_kernel<false><<<blocksFor(c.nc), kThreads, 0, c.stream>>>(d, ni, x, y);
+        }, 8.0 * c.nf + 8.0 * c.nc);
+        return true;
+    case STENCIL_DIV_INTERIOR:
+        launch(c, "stencil_div", [&] {
+            stencil_div_kernel<true><<<blocksFor(c.nc), kThreads, 0, c.stream>>>(d, ni, x, y);
+        }, 8.0 * c.nif + 8.0 * c.nc);
+        return true;
+    default:
+        return false;
+    }
 }
 
 // ---------------------------------------------------------------------------

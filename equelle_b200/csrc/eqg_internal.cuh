@@ -72,6 +72,16 @@ struct Pattern {
     // for a union pattern: per pair of operand patterns (ids), the position
     // of each entry in either operand (-1: absent), int32[2 nnz]
     std::map<std::pair<uint64_t, uint64_t>, Buf> merge_maps;
+    // for a pattern made as M J (gradient, divergence, On, Extend, spans):
+    // per entry, the positions of J's entries that add into it (see
+    // spgemm_plan_kernel), int32[nnz+1] bounds and int32 packed positions
+    Buf plan_start, plan_contrib;
+    int64_t plan_entries = 0;
+    // for a union pattern whose operands have entries in disjoint row
+    // ranges, the one with the lower rows first: the union's entries are
+    // those of concat_first, then those of concat_second (ids; 0: not such
+    // a union)
+    uint64_t concat_first = 0, concat_second = 0;
     std::shared_ptr<SolverAnalysis> analysis;  // linear-solver analysis, built on demand
 };
 using PatternP = std::shared_ptr<Pattern>;
@@ -82,6 +92,9 @@ struct OpMatrix {
     int n_out = 0, n_src = 0;
     int max_row = 0;
     int64_t nnz = 0;
+    // a helper operator of the Cartesian grid that the stencil kernels apply
+    // to values by face and cell index arithmetic (STENCIL_*; 0: none)
+    int stencil = 0;
     Buf ptr;   // int32[n_out+1]
     Buf src;   // int32[nnz], ascending within a row
     Buf w;     // double[nnz]
@@ -355,9 +368,14 @@ OpMatrixP opmat_from_map(Core& c, const int32_t* map_dev, int n_out, int n_src, 
 OpMatrixP opmat_from_host(Core& c, int n_out, int n_src, const std::vector<int32_t>& ptr,
                           const std::vector<int32_t>& src, const std::vector<double>& w);
 void opmat_apply_values(Core& c, const OpMatrix& m, const double* x, double* y);
+// Helper operators of Cartesian grids applied to values without their CSR
+// arrays (core.cu); false when `kind` is not one of them.
+enum StencilKind { STENCIL_NONE = 0, STENCIL_GRAD, STENCIL_NGRAD, STENCIL_DIV_FULL, STENCIL_DIV_INTERIOR };
+bool stencil_apply_values(Core& c, int kind, const double* x, double* y);
 PatternP pattern_identity(Core& c, int n);
 Buf ones(Core& c, int64_t n);
-PatternP pattern_spgemm(Core& c, const OpMatrix& m, const PatternP& j);
+// with_plan: also build the output's position plan (spgemm_plan_kernel)
+PatternP pattern_spgemm(Core& c, const OpMatrix& m, const PatternP& j, bool with_plan = true);
 void spgemm_values(Core& c, const OpMatrix& m, const Pattern& jp, const double* jv, const Pattern& op,
                    double* ov);
 PatternP pattern_union(Core& c, const PatternP& a, const PatternP& b);

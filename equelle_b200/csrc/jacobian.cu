@@ -134,6 +134,62 @@ __global__ void spgemm_numeric_kernel(int n_out, const int* __restrict__ mptr, c
     }
 }
 
+// Position plan of M*J for one output pattern: for every output entry, the
+// entries of J that the K-way merge adds into it, in the merge's order
+// (stream t of M's row ascending), packed as t << kPlanShift | position in
+// J.  Built once with the output pattern; the numeric product then runs one
+// thread per output entry, with the same operations in the same order as
+// spgemm_numeric_kernel.
+constexpr int kPlanShift = 27;
+constexpr int kPlanMask = (1 << kPlanShift) - 1;
+
+template <int KMAX, bool COUNT>
+__global__ void spgemm_plan_kernel(int n_out, const int* __restrict__ mptr, const int* __restrict__ msrc,
+                                   const int* __restrict__ jptr, const int* __restrict__ jcol,
+                                   const int* __restrict__ optr, const int* __restrict__ ocol,
+                                   int64_t* __restrict__ cnt, const int* __restrict__ start,
+                                   int* __restrict__ contrib)
+{
+    GRID_STRIDE(i, n_out)
+    {
+        Streams<KMAX> s;
+        s.load((int)i, mptr, msrc, nullptr, jptr);
+        const int p1 = optr[i + 1];
+        for (int p = optr[i]; p < p1; ++p) {
+            const int c = ocol[p];
+            int n = 0;
+            const int o = COUNT ? 0 : start[p];
+#pragma unroll
+            for (int t = 0; t < KMAX; ++t) {
+                if (s.pos[t] < s.end[t] && jcol[s.pos[t]] == c) {
+                    if (!COUNT) contrib[o + n] = (t << kPlanShift) | s.pos[t];
+                    ++n;
+                    ++s.pos[t];
+                }
+            }
+            if (COUNT) cnt[p] = n;
+        }
+    }
+}
+
+__global__ void spgemm_planned_kernel(int64_t nnz, const int* __restrict__ rowidx, const int* __restrict__ mptr,
+                                      const double* __restrict__ mw, const int* __restrict__ start,
+                                      const int* __restrict__ contrib, const double* __restrict__ jval,
+                                      double* __restrict__ oval)
+{
+    GRID_STRIDE(e, nnz)
+    {
+        const int m0 = mptr[rowidx[e]];
+        const int k1 = start[e + 1];
+        double acc = 0.0;
+        for (int k = start[e]; k < k1; ++k) {
+            const int q = contrib[k];
+            acc += mw[m0 + (q >> kPlanShift)] * jval[q & kPlanMask];
+        }
+        oval[e] = acc;
+    }
+}
+
 // y = M x, each row accumulated from 0.0 over ascending source entries.
 __global__ void opmat_apply_kernel(int n_out, const int* __restrict__ mptr, const int* __restrict__ msrc,
                                    const double* __restrict__ mw, const double* __restrict__ x,
@@ -294,6 +350,14 @@ __global__ void ew_merge_kernel(Rule r, int rows, const int* __restrict__ aptr, 
     }
 }
 
+// out = [x (n1 values), y (n2 values)]: the sum of two Jacobians whose
+// entries lie in disjoint row ranges (each entry 1.0 * its one operand).
+__global__ void concat_kernel(const double* __restrict__ x, int64_t n1, const double* __restrict__ y, int64_t n2,
+                              double* __restrict__ out)
+{
+    GRID_STRIDE(e, n1 + n2) out[e] = e < n1 ? x[e] : y[e - n1];
+}
+
 // Position in each operand of every entry of the union pattern (-1: absent),
 // built once per operand pattern pair.
 __global__ void merge_map_kernel(int rows, const int* __restrict__ aptr, const int* __restrict__ acol,
@@ -409,9 +473,44 @@ void spgemm_symbolic(Core& c, const OpMatrix& m, const Pattern& j, Pattern& out)
 }
 
 template <int KMAX>
+void spgemm_build_plan(Core& c, const OpMatrix& m, const Pattern& j, Pattern& out)
+{
+    if (m.n_out <= 0 || out.nnz <= 0) return;
+    Buf cnt = c.allocN<int64_t>((size_t)out.nnz);
+    const int nb = blocksFor(m.n_out);
+    launch(c, "spgemm_plan_count", [&] {
+        spgemm_plan_kernel<KMAX, true><<<nb, kThreads, 0, c.stream>>>(
+            m.n_out, m.ptr->as<int>(), m.src->as<int>(), j.rowptr->as<int>(), j.colind->as<int>(),
+            out.rowptr->as<int>(), out.colind->as<int>(), cnt->as<int64_t>(), nullptr, nullptr);
+    });
+    const int64_t total = counts_to_rowptr(c, cnt, (int)out.nnz, out.plan_start);
+    out.plan_entries = total;
+    out.plan_contrib = c.allocN<int>(total > 0 ? total : 1);
+    launch(c, "spgemm_plan_fill", [&] {
+        spgemm_plan_kernel<KMAX, false><<<nb, kThreads, 0, c.stream>>>(
+            m.n_out, m.ptr->as<int>(), m.src->as<int>(), j.rowptr->as<int>(), j.colind->as<int>(),
+            out.rowptr->as<int>(), out.colind->as<int>(), nullptr, out.plan_start->as<int>(),
+            out.plan_contrib->as<int>());
+    });
+    pattern_build_rowidx(c, out);
+}
+
+template <int KMAX>
 void spgemm_numeric(Core& c, const OpMatrix& m, const Pattern& jp, const double* jv, const Pattern& op, double* ov)
 {
     if (m.n_out <= 0) return;
+    if (op.plan_start) {
+        // algorithmic bytes: the output's row indices and plan, the
+        // contributing Jacobian values and M's row pointers and weights, the
+        // output values
+        const double bytes = 16.0 * op.nnz + 12.0 * op.plan_entries + 4.0 * (m.n_out + 1) + 8.0 * m.nnz;
+        launch(c, "spgemm_planned", [&] {
+            spgemm_planned_kernel<<<blocksFor(op.nnz), kThreads, 0, c.stream>>>(
+                op.nnz, op.rowidx->as<int>(), m.ptr->as<int>(), m.w->as<double>(), op.plan_start->as<int>(),
+                op.plan_contrib->as<int>(), jv, ov);
+        }, bytes);
+        return;
+    }
     // algorithmic bytes: M (row pointers, sources, weights), the Jacobian
     // operand and the output pattern (row pointers, columns, values) once
     const double bytes = 4.0 * (m.n_out + 1) + 12.0 * m.nnz + 4.0 * (jp.rows + 1) + 12.0 * jp.nnz +
@@ -489,6 +588,7 @@ OpMatrixP opmat_from_map(Core& c, const int32_t* map_dev, int n_out, int n_src, 
 void opmat_apply_values(Core& c, const OpMatrix& m, const double* x, double* y)
 {
     if (m.n_out <= 0) return;
+    if (m.stencil && c.param_i("stencil_ops", 1) != 0 && stencil_apply_values(c, m.stencil, x, y)) return;
     launch(c, "opmat_apply", [&] { opmat_apply_kernel<<<blocksFor(m.n_out), kThreads, 0, c.stream>>>(m.n_out, m.ptr->as<int>(), m.src->as<int>(),
                                                                      m.w->as<double>(), x, y); },
            4.0 * (m.n_out + 1) + 12.0 * m.nnz + 8.0 * m.n_src + 8.0 * m.n_out);
@@ -523,7 +623,7 @@ Buf ones(Core& c, int64_t n)
     return b;
 }
 
-PatternP pattern_spgemm(Core& c, const OpMatrix& m, const PatternP& j)
+PatternP pattern_spgemm(Core& c, const OpMatrix& m, const PatternP& j, bool with_plan)
 {
     if (m.n_src != j->rows) fail(EQG_ERR_ARG, "operator/Jacobian shape mismatch");
     const auto key = std::make_tuple(1, m.id, j->id, (int64_t)0);
@@ -543,6 +643,17 @@ PatternP pattern_spgemm(Core& c, const OpMatrix& m, const PatternP& j)
     case 6: spgemm_symbolic<6>(c, m, *j, *p); break;
     case 8: spgemm_symbolic<8>(c, m, *j, *p); break;
     default: spgemm_symbolic<16>(c, m, *j, *p); break;
+    }
+    // the position plan, when positions and streams fit its packing
+    if (with_plan && c.param_i("spgemm_plan", 1) != 0 && j->nnz <= kPlanMask && p->nnz < (int64_t)INT_MAX / 2) {
+        switch (kmax_for(m.max_row)) {
+        case 1: spgemm_build_plan<1>(c, m, *j, *p); break;
+        case 2: spgemm_build_plan<2>(c, m, *j, *p); break;
+        case 4: spgemm_build_plan<4>(c, m, *j, *p); break;
+        case 6: spgemm_build_plan<6>(c, m, *j, *p); break;
+        case 8: spgemm_build_plan<8>(c, m, *j, *p); break;
+        default: spgemm_build_plan<16>(c, m, *j, *p); break;
+        }
     }
     c.patterns_built++;
     c.pattern_cache[key] = p;
@@ -589,6 +700,32 @@ PatternP pattern_union(Core& c, const PatternP& a, const PatternP& b)
         launch(c, "union_fill", [&] { union_kernel<true><<<nb, kThreads, 0, c.stream>>>(p->rows, a->rowptr->as<int>(), a->colind->as<int>(),
                                                          b->rowptr->as<int>(), b->colind->as<int>(), nullptr,
                                                          p->rowptr->as<int>(), p->colind->as<int>()); });
+        // operands with entries in disjoint row ranges (the stacked
+        // residuals of a system): the union lists one operand's entries, then
+        // the other's
+        std::vector<int> ra(p->rows + 1), rb(p->rows + 1);
+        EQG_CUDA(cudaMemcpyAsync(ra.data(), a->rowptr->ptr, ra.size() * 4, cudaMemcpyDeviceToHost, c.stream));
+        EQG_CUDA(cudaMemcpyAsync(rb.data(), b->rowptr->ptr, rb.size() * 4, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        auto first_row = [&](const std::vector<int>& r) {
+            for (int i = 0; i < p->rows; ++i)
+                if (r[i + 1] > r[i]) return i;
+            return p->rows;
+        };
+        auto last_row = [&](const std::vector<int>& r) {
+            for (int i = p->rows - 1; i >= 0; --i)
+                if (r[i + 1] > r[i]) return i;
+            return -1;
+        };
+        if (a->nnz > 0 && b->nnz > 0) {
+            if (last_row(ra) < first_row(rb)) {
+                p->concat_first = a->id;
+                p->concat_second = b->id;
+            } else if (last_row(rb) < first_row(ra)) {
+                p->concat_first = b->id;
+                p->concat_second = a->id;
+            }
+        }
     }
     c.patterns_built++;
     c.pattern_cache[key] = p;
@@ -616,6 +753,18 @@ void jacobian_elementwise(Core& c, const JacArgs& a, const Pattern& out, double*
     const double per_row = 8.0 * ((a.va ? 1 : 0) + (a.vb ? 1 : 0) + (a.vout ? 1 : 0)) + (a.mask ? 1.0 : 0.0);
     const double bytes = 8.0 * (na + nbv + out.nnz) + 4.0 * (out.rows + 1) + per_row * out.rows +
                          (flat ? 0.0 : 4.0 * (na + nbv + out.nnz));
+    if (a.rule == JR_ADD && a.pa && a.pb && out.concat_first && c.param_i("jac_concat", 1) != 0 &&
+        ((a.pa->id == out.concat_first && a.pb->id == out.concat_second) ||
+         (a.pb->id == out.concat_first && a.pa->id == out.concat_second))) {
+        const bool a_first = a.pa->id == out.concat_first;
+        const double* x = a_first ? a.ja : a.jb;
+        const double* y = a_first ? a.jb : a.ja;
+        const int64_t n1 = a_first ? a.pa->nnz : a.pb->nnz, n2 = out.nnz - n1;
+        launch(c, "jac_concat", [&] {
+            concat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(x, n1, y, n2, jout);
+        }, 16.0 * out.nnz);
+        return;
+    }
     if (flat) {
         pattern_build_rowidx(c, const_cast<Pattern&>(out));
         launch(c, "jac_flat", [&] { ew_flat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(r, out.rowidx->as<int>(), a.pa ? a.ja : nullptr,

@@ -49,8 +49,15 @@
 #include <chrono>
 #include <climits>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
 #include <numeric>
+#include <sstream>
+#include <string>
 
 #include <omp.h>
 
@@ -410,6 +417,31 @@ __global__ void gather_values_kernel(const double* __restrict__ src, const int* 
     {
         const int e = map[p];
         dst[p] = e >= 0 ? src[e] : 0.0;
+    }
+}
+
+// The same gather, one block row per thread over its slots: a thread's
+// loads stay in the few Jacobian rows of its block row (the unknowns of one
+// cell), which L1 then serves, and a warp's stores at one slot position are
+// one contiguous segment.
+template <int BB>
+__global__ void gather_rows_kernel(int nb, const int* __restrict__ slice_ptr, const double* __restrict__ src,
+                                   const int* __restrict__ map, double* __restrict__ dst)
+{
+    // every lane of the last slice, also past the last row (its slots are
+    // padding: zero)
+    GRID_STRIDE(r, ((int64_t)nb + 31) & ~(int64_t)31)
+    {
+        const int R = (int)r, lane = R & 31;
+        const int s0 = slice_ptr[R >> 5], width = (slice_ptr[(R >> 5) + 1] - s0) >> 5;
+        for (int k = 0; k < width; ++k) {
+            const int64_t q = (int64_t)(s0 + (k << 5) + lane) * BB;
+#pragma unroll
+            for (int e = 0; e < BB; ++e) {
+                const int j = map[q + e];
+                dst[q + e] = j >= 0 ? src[j] : 0.0;
+            }
+        }
     }
 }
 
@@ -1638,6 +1670,7 @@ struct Level {
     int64_t blocks = 0;            // block entries of the pattern (without padding)
     int kmax = 0;                  // longest block row
     int width = 0;                 // slots per row of every slice when uniform (else 0)
+    int threads = kThreads;        // threads per block of this level's launch-per-step kernels (autotuned)
     Buf sell_ptr, sell_col, sell_len, sell_dk;
     Buf as64, lus64, as32, lus32;  // matrix, block ILU(0) factors (inverted diagonal blocks)
     Buf v64, v32;                  // 4 work vectors: r, z, t, w
@@ -1667,6 +1700,7 @@ struct SolverAnalysis {
     // (index into the fused levels; their count: none)
     int tail_local[3] = {0, 0, 0};
     int last_mode = 0;  // precision of the last solve (pc_mode)
+    bool tuned[3] = {false, false, false};  // launch shapes chosen, per precision (autotune)
     Buf tail_trace;  // SM clock after each step of the last fused cycle
     // CUDA graphs of `chunk` BiCGStab iterations: [0] FP64, [1] FP32, [2] FP64
     // with an FP32 preconditioner
@@ -2646,7 +2680,8 @@ void ilu_apply(Core& c, const Level& L, const T* b, T* out, T* zadd, const KScal
                              (last ? (double)(r1 - r0) * L.bs * L.bs * sizeof(M) : 0.0) +
                              (r1 - r0) * (4.0 + vrow * ((last && zadd) ? 5.0 : 3.0));
         WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "bilu_lower", [&] {
-                    launch_k(c, bilu_lower_kernel<BS, KK, T, M>, blocksFor(r1 - r0), kThreads, r0, r1, r_first, last,
+                    launch_k(c, bilu_lower_kernel<BS, KK, T, M>, blocksFor(r1 - r0, L.threads), L.threads, r0, r1,
+                             r_first, last,
                              L.view(), lu, b, out, last ? zadd : nullptr, sc, skip_if_s);
                 }, bytes)));
     }
@@ -2655,7 +2690,8 @@ void ilu_apply(Core& c, const Level& L, const T* b, T* out, T* zadd, const KScal
         const double bytes = block_bytes<M>(L, L.stage_upper[s]) + (double)(r1 - r0) * L.bs * L.bs * sizeof(M) +
                              (r1 - r0) * (8.0 + vrow * (zadd ? 5.0 : 3.0));
         WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "bilu_upper", [&] {
-                    launch_k(c, bilu_upper_kernel<BS, KK, T, M>, blocksFor(r1 - r0), kThreads, r0, r1, (int)(s == 0),
+                    launch_k(c, bilu_upper_kernel<BS, KK, T, M>, blocksFor(r1 - r0, L.threads), L.threads, r0, r1,
+                             (int)(s == 0),
                              L.view(), lu, b, out, zadd, sc, skip_if_s);
                 }, bytes)));
     }
@@ -2674,7 +2710,8 @@ void level_residual(Core& c, const Level& L, const T* x, const T* b, T* out, int
     const double bytes = block_bytes<M>(L, L.blocks - skipped) +
                          (L.nb - r_zero) * (4.0 + 2.0 * L.bs * sizeof(T)) + (double)L.n * sizeof(T);
     WITH_BS(L.bs, WITH_KMAX(L.kmax, launch(c, "mg_residual", [&] {
-                launch_k(c, mg_residual_kernel<BS, KK, T, M>, blocksFor(L.nb), kThreads, L.nb, r_zero, L.view(),
+                launch_k(c, mg_residual_kernel<BS, KK, T, M>, blocksFor(L.nb, L.threads), L.threads, L.nb, r_zero,
+                         L.view(),
                          level_a<M>(L), x, b, out, sc, skip_if_s);
             }, bytes)));
 }
@@ -2709,7 +2746,7 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
     ilu_apply<T, M>(c, L, r, z, nullptr, sc, skip);
     level_residual<T, M>(c, L, z, r, t, r_zero, sc, skip);
     launch(c, "mg_restrict", [&] {
-        launch_k(c, mg_restrict_kernel<T>, blocksFor(C.n), kThreads, C.n, (const int*)L.mptr->as<int>(),
+        launch_k(c, mg_restrict_kernel<T>, blocksFor(C.n, L.threads), L.threads, C.n, (const int*)L.mptr->as<int>(),
                  (const int*)L.midx->as<int>(), (const T*)t, r_zero * L.bs, rc, sc, skip);
     }, (double)(L.n - r_zero * L.bs) * sizeof(T) + (double)C.n * sizeof(T) + 4.0 * (C.n + 1) + 4.0 * L.n);
     vcycle<T, M>(c, an, l + 1, rc, zc, sc, skip);
@@ -2723,12 +2760,13 @@ void vcycle(Core& c, const SolverAnalysis& an, size_t l, const T* r, T* z, const
         const double bytes = block_bytes<M>(L, L.ap_blocks) + 8.0 * L.nb + (double)C.n * sizeof(T) +
                              2.0 * L.n * sizeof(T) + 2.0 * (L.n - r_zero * L.bs) * sizeof(T);
         WITH_BS(L.bs, WITH_KMAX(L.ap_kmax, launch(c, "mg_correct", [&] {
-                    launch_k(c, mg_correct_kernel<BS, KK, T, M>, blocksFor(L.nb), kThreads, L.nb, r_zero, L.ap_view(),
+                    launch_k(c, mg_correct_kernel<BS, KK, T, M>, blocksFor(L.nb, L.threads), L.threads, L.nb, r_zero,
+                             L.ap_view(),
                              level_ap<M>(L), (const int*)L.aggb->as<int>(), (const T*)zc, z, t, an.mg_alpha, sc, skip);
                 }, bytes)));
     } else {
         WITH_BS(L.bs, launch(c, "mg_prolong", [&] {
-                    launch_k(c, mg_prolong_kernel<BS, T>, blocksFor(L.nb), kThreads, L.nb,
+                    launch_k(c, mg_prolong_kernel<BS, T>, blocksFor(L.nb, L.threads), L.threads, L.nb,
                              (const int*)L.aggb->as<int>(), (const T*)zc, z, an.mg_alpha, sc, skip);
                 }, 4.0 * L.nb + (double)C.n * sizeof(T) + 2.0 * L.n * sizeof(T)));
         level_residual<T, M>(c, L, z, r, t, 0, sc, skip);
@@ -2755,6 +2793,174 @@ void apply_pc(Core& c, const SolverAnalysis& an, const T* in, T* out, const KSca
         }
     }
     precondition<T, T>(c, an, in, out, sc, skip_if_s);
+}
+
+// ---- autotuning of launch shapes ---------------------------------------------
+// Per Jacobian pattern and precision, the threads per block of every
+// launch-per-step V-cycle level's kernels (128, 256 or 512) and the cluster
+// size of the fused coarse cycle (the largest the device schedules, half or
+// a quarter of it) are chosen by timing preconditioner applications on the
+// solve's right-hand side (CUDA events on the runtime stream), before the
+// first BiCGStab iteration and its graph capture; one level at a time, then
+// the cluster.  A row's operations do not depend on the launch shape, so the
+// results are the same for every choice.  Choices are kept for the process,
+// keyed by device, system and hierarchy sizes and precision, and read from
+// and written to the JSON file linsolver_tune_file (or $EQG_TUNE_FILE) when
+// one is named.  linsolver_autotune=0 keeps 256 threads and the largest
+// cluster.
+struct TuneChoice {
+    std::vector<int> threads;
+    int cluster = 0;
+};
+std::mutex g_tune_mutex;
+std::map<std::string, TuneChoice> g_tune_cache;
+std::map<std::string, bool> g_tune_files_read;
+
+// The file holds one entry per line:
+//   "<key>": {"threads": [t0, t1, ...], "cluster": c},
+void tune_file_read(const std::string& path)
+{
+    std::ifstream f(path.c_str());
+    std::string line;
+    while (std::getline(f, line)) {
+        const size_t k0 = line.find('"'), k1 = line.find('"', k0 + 1);
+        const size_t a0 = line.find('['), a1 = line.find(']');
+        const size_t c0 = line.find("\"cluster\":");
+        if (k0 == std::string::npos || k1 == std::string::npos || a0 == std::string::npos ||
+            a1 == std::string::npos || c0 == std::string::npos)
+            continue;
+        TuneChoice t;
+        std::string nums = line.substr(a0 + 1, a1 - a0 - 1);
+        for (char& ch : nums)
+            if (ch == ',') ch = ' ';
+        std::istringstream in(nums);
+        int v = 0;
+        while (in >> v) t.threads.push_back(v);
+        t.cluster = std::atoi(line.c_str() + c0 + 10);
+        g_tune_cache.emplace(line.substr(k0 + 1, k1 - k0 - 1), t);
+    }
+}
+
+void tune_file_write(const std::string& path)
+{
+    const std::string tmp = path + ".tmp";
+    {
+        std::ofstream f(tmp.c_str());
+        f << "{\n";
+        size_t i = 0;
+        for (auto& kv : g_tune_cache) {
+            f << "\"" << kv.first << "\": {\"threads\": [";
+            for (size_t j = 0; j < kv.second.threads.size(); ++j) f << (j ? ", " : "") << kv.second.threads[j];
+            f << "], \"cluster\": " << kv.second.cluster << "}" << (++i < g_tune_cache.size() ? "," : "") << "\n";
+        }
+        f << "}\n";
+    }
+    std::rename(tmp.c_str(), path.c_str());
+}
+
+template <class T, class M>
+void autotune(Core& c, SolverAnalysis& an, const T* b, T* out, const KScal* sc)
+{
+    const int mode = pc_mode<T, M>();
+    if (an.tuned[mode]) return;
+    an.tuned[mode] = true;
+    if (c.param_i("linsolver_autotune", 1) == 0) return;
+    // levels with launch-per-step kernels: all but the fused ones and a
+    // dense coarsest level
+    std::vector<int> lv;
+    for (size_t l = 0; l < an.levels.size(); ++l) {
+        if (an.multigrid && an.tail_first >= 0 && (int)l >= an.tail_first) break;
+        if (an.levels[l].coarsest) break;
+        lv.push_back((int)l);
+        if (!an.multigrid) break;
+    }
+    cudaDeviceProp prop;
+    EQG_CUDA(cudaGetDeviceProperties(&prop, c.device));
+    std::ostringstream key;
+    key << prop.name << "; n " << an.n << "; nnz " << an.nnz << "; bs " << an.levels[0].bs << "; levels";
+    for (auto& L : an.levels) key << " " << L.n;
+    key << "; fused from " << an.tail_first << "; precision " << mode;
+    std::string file = c.param_s("linsolver_tune_file", "");
+    if (file.empty() && std::getenv("EQG_TUNE_FILE")) file = std::getenv("EQG_TUNE_FILE");
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        if (!file.empty() && !g_tune_files_read[file]) {
+            tune_file_read(file);
+            g_tune_files_read[file] = true;
+        }
+        auto it = g_tune_cache.find(key.str());
+        if (it != g_tune_cache.end() && it->second.threads.size() == lv.size()) {
+            for (size_t i = 0; i < lv.size(); ++i) an.levels[lv[i]].threads = it->second.threads[i];
+            if (an.tail_first >= 0 && it->second.cluster > 0 && it->second.cluster <= an.tail_cluster[mode])
+                an.tail_cluster[mode] = it->second.cluster;
+            return;
+        }
+    }
+    // tuning launches are not part of a kernel profile
+    const std::string timed = c.timed_kernel;
+    c.timed_kernel.clear();
+    cudaEvent_t e0, e1;
+    EQG_CUDA(cudaEventCreate(&e0));
+    EQG_CUDA(cudaEventCreate(&e1));
+    auto measure = [&] {
+        precondition<T, M>(c, an, b, out, sc, 0);
+        float best = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {
+            EQG_CUDA(cudaEventRecord(e0, c.stream));
+            for (int k = 0; k < 4; ++k) precondition<T, M>(c, an, b, out, sc, 0);
+            EQG_CUDA(cudaEventRecord(e1, c.stream));
+            EQG_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            EQG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            best = std::min(best, ms);
+        }
+        return best;
+    };
+    float cur = measure();
+    const float first = cur;
+    for (int l : lv) {
+        Level& L = an.levels[l];
+        int best_t = L.threads;
+        for (int t : {128, 256, 512}) {
+            if (t == best_t) continue;
+            L.threads = t;
+            const float ms = measure();
+            if (ms < cur) {
+                cur = ms;
+                best_t = t;
+            }
+        }
+        L.threads = best_t;
+    }
+    int& cl = an.tail_cluster[mode];
+    if (an.tail_first >= 0 && cl > 1) {
+        const int top = cl;
+        int best_c = cl;
+        for (int cand : {top / 2, top / 4}) {
+            if (cand < 2) continue;
+            cl = cand;
+            const float ms = measure();
+            if (ms < cur) {
+                cur = ms;
+                best_c = cand;
+            }
+        }
+        cl = best_c;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c.timed_kernel = timed;
+    TuneChoice t;
+    for (int l : lv) t.threads.push_back(an.levels[l].threads);
+    t.cluster = an.tail_first >= 0 ? cl : 0;
+    if (c.verbose > 2) {
+        std::printf("        autotune: %.3f -> %.3f ms per V-cycle; threads per level:", first / 4, cur / 4);
+        for (int v : t.threads) std::printf(" %d", v);
+        std::printf("; cluster %d\n", t.cluster);
+    }
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key.str()] = t;
+    if (!file.empty()) tune_file_write(file);
 }
 
 // BiCGStab on the permuted system with values a; v.b holds the right-hand
@@ -2798,6 +3004,16 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double 
                      (const T*)v.t, (const T*)v.rhat, v.x, v.r, n, part, cnt, sc);
         }, 8.0 * vb);
     };
+    // launch shapes of the preconditioner, once per analysis and precision
+    // (before the graph capture below)
+    if (an.multigrid || an.levels[0].n > 0) {
+        if constexpr (sizeof(T) == sizeof(double)) {
+            if (pc32) autotune<double, float>(c, an, v.b, v.ph, sc);
+            else autotune<double, double>(c, an, v.b, v.ph, sc);
+        } else {
+            autotune<float, float>(c, an, v.b, v.ph, sc);
+        }
+    }
     // Graph of `check_every` iterations, captured once per analysis and
     // precision; kernel arguments are fixed (buffers of the analysis,
     // scalars in device memory).  Kernel timing (time_kernel) needs one
@@ -2912,8 +3128,23 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     c.factor_clock.start(c.stream);
     const Level& L0 = an.levels[0];
     launch(c, "gather_values", [&] {
-        gather_values_kernel<<<blocksFor(L0.vals), kThreads, 0, c.stream>>>(jval, an.vmap->as<int>(),
-                                                                            L0.as64->as<double>(), L0.vals);
+        // gather_rows=1: one block row per thread (measured slower on the
+        // 128x128x64 Jacobian: 0.74 against 0.64 ms per gather)
+        if (c.param_i("gather_rows", 0) != 0) {
+            const int* sp = L0.sell_ptr->as<int>();
+            if (L0.bs == 1)
+                gather_rows_kernel<1><<<blocksFor(L0.nb + 32), kThreads, 0, c.stream>>>(L0.nb, sp, jval, an.vmap->as<int>(),
+                                                                                  L0.as64->as<double>());
+            else if (L0.bs == 2)
+                gather_rows_kernel<4><<<blocksFor(L0.nb + 32), kThreads, 0, c.stream>>>(L0.nb, sp, jval, an.vmap->as<int>(),
+                                                                                  L0.as64->as<double>());
+            else
+                gather_rows_kernel<9><<<blocksFor(L0.nb + 32), kThreads, 0, c.stream>>>(L0.nb, sp, jval, an.vmap->as<int>(),
+                                                                                  L0.as64->as<double>());
+        } else {
+            gather_values_kernel<<<blocksFor(L0.vals), kThreads, 0, c.stream>>>(jval, an.vmap->as<int>(),
+                                                                                L0.as64->as<double>(), L0.vals);
+        }
     }, 12.0 * L0.vals + 8.0 * an.nnz);
     for (size_t l = 1; l < an.levels.size(); ++l) {
         const Level& F = an.levels[l - 1];
