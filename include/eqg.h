@@ -134,7 +134,14 @@ const char* eqg_backend_name(void);
  * linsolver_tail_trace (0; 1: print the SM clock cycles of every step of the
  * last fused cycle after each linear solve), lazy (0; 1:
  * defer value-only elementwise operations and evaluate them in batches),
- * host_threads (0: OpenMP's default for the solver analysis), time_kernel
+ * host_threads (0: OpenMP's default for the solver analysis),
+ * linsolver_autotune (1: choose threads per block of the launch-per-step
+ * V-cycle levels and the fused cycle's cluster size by timing, once per
+ * Jacobian pattern and precision; 0: 256 and the largest cluster),
+ * linsolver_tune_file (a JSON file caching those choices; default
+ * $EQG_TUNE_FILE, else none), spgemm_plan / span_share / jac_concat /
+ * stencil_ops (1; 0 switches off an assembly fast path, for comparisons),
+ * gather_rows (0), time_kernel
  * (a kernel name, or "*", to time with CUDA events) and device (CUDA device
  * index; default: the calling thread's current device).  grid_filename
  * (instead of grid_dim, nx, ...) reads the grid from a file: the arrays of an
