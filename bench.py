@@ -562,7 +562,8 @@ def main_many(a, rp):
         return {"requests": len(recs), "instance_steps": steps, "wall_s": wall,
                 "instance_steps_per_s": steps / wall, "requests_per_s": len(recs) / wall,
                 "latency_p50_s": serve.percentile(lat, 50), "latency_p99_s": serve.percentile(lat, 99),
-                "errors": sum(1 for r in recs if r.error)}
+                "errors": sum(1 for r in recs if r.error),
+                "error_samples": ["%s %d cells: %s" % (r.program, r.cells, r.error[:160]) for r in recs if r.error][:4]}
 
     if a.workload == "batched":
         side_max = a.side_max or 512

@@ -3171,8 +3171,12 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
         if (L.coarsest) {
             WITH_BS(L.bs, launch(c, "mg_dense_inverse", [&] {
                 const size_t smem = ((size_t)L.n * L.n + L.n) * sizeof(double);
+                // one value for every call: runtimes on other host threads set
+                // the same attribute of the same kernel, and a smaller value
+                // set between this call's set and its launch would fail it
+                const size_t most = ((size_t)kCoarsest * kCoarsest + kCoarsest) * sizeof(double);
                 EQG_CUDA(cudaFuncSetAttribute(dense_inverse_kernel<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)smem));
+                                              (int)std::max(smem, most)));
                 dense_inverse_kernel<BS><<<1, 1024, smem, c.stream>>>(L.nb, L.view(), L.as64->as<double>(),
                                                                      L.inv64->as<double>(), an.factor_status->as<int>());
             }, 16.0 * L.n * L.n));
