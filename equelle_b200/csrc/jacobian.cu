@@ -26,9 +26,6 @@ namespace {
 #define GRID_STRIDE(i, n) \
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
-// entries per thread per round of the *_ilp kernels
-constexpr int kIlp = 4;
-
 // ---------------------------------------------------------------------------
 // Conservative product M*J by K-way merge of the selected rows of J.
 // ---------------------------------------------------------------------------
@@ -193,46 +190,6 @@ __global__ void spgemm_planned_kernel(int64_t nnz, const int* __restrict__ rowid
     }
 }
 
-// spgemm_planned_kernel four entries per thread per round; the first two
-// contributions of each entry loaded with its plan, the rest in its loop.
-__global__ void spgemm_planned_ilp_kernel(int64_t nnz, const int* __restrict__ rowidx, const int* __restrict__ mptr,
-                                          const double* __restrict__ mw, const int* __restrict__ start,
-                                          const int* __restrict__ contrib, const double* __restrict__ jval,
-                                          double* __restrict__ oval)
-{
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < nnz; e0 += kIlp * stride) {
-        int m0[kIlp], k0[kIlp], k1[kIlp];
-#pragma unroll
-        for (int u = 0; u < kIlp; ++u) {
-            const int64_t e = e0 + u * stride;
-            const bool ok = e < nnz;
-            m0[u] = ok ? mptr[rowidx[e]] : 0;
-            k0[u] = ok ? start[e] : 0;
-            k1[u] = ok ? start[e + 1] : 0;
-        }
-        int q0[kIlp];
-        double v0[kIlp];
-#pragma unroll
-        for (int u = 0; u < kIlp; ++u) {
-            q0[u] = k0[u] < k1[u] ? contrib[k0[u]] : 0;
-            v0[u] = k0[u] < k1[u] ? jval[q0[u] & kPlanMask] : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < kIlp; ++u) {
-            const int64_t e = e0 + u * stride;
-            if (e >= nnz) break;
-            double acc = 0.0;
-            if (k0[u] < k1[u]) acc += mw[m0[u] + (q0[u] >> kPlanShift)] * v0[u];
-            for (int k = k0[u] + 1; k < k1[u]; ++k) {
-                const int q = contrib[k];
-                acc += mw[m0[u] + (q >> kPlanShift)] * jval[q & kPlanMask];
-            }
-            oval[e] = acc;
-        }
-    }
-}
-
 // y = M x, each row accumulated from 0.0 over ascending source entries.
 __global__ void opmat_apply_kernel(int n_out, const int* __restrict__ mptr, const int* __restrict__ msrc,
                                    const double* __restrict__ mw, const double* __restrict__ x,
@@ -369,39 +326,6 @@ __global__ void ew_flat_kernel(Rule r, const int* __restrict__ rowidx, const dou
     }
 }
 
-// The same, kIlp entries per thread per round (e, e + stride, ...): every
-// entry's index loads are issued before its value loads, so a thread keeps
-// independent load chains in flight.  Same operations per entry.
-
-__global__ void ew_flat_ilp_kernel(Rule r, const int* __restrict__ rowidx, const double* __restrict__ ja,
-                                   const double* __restrict__ jb, double* __restrict__ out, int64_t nnz)
-{
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < nnz; e0 += kIlp * stride) {
-        int row[kIlp];
-        double a[kIlp], b[kIlp];
-#pragma unroll
-        for (int u = 0; u < kIlp; ++u) {
-            const int64_t e = e0 + u * stride;
-            const bool ok = e < nnz;
-            row[u] = ok ? rowidx[e] : 0;
-            a[u] = ok && ja ? ja[e] : 0.0;
-            b[u] = ok && jb ? jb[e] : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < kIlp; ++u) {
-            const int64_t e = e0 + u * stride;
-            if (e >= nnz) break;
-            double wa, wb, post;
-            rule_weights(r, row[u], wa, wb, post);
-            double acc = 0.0;
-            if (ja) acc += wa * a[u];
-            if (jb) acc += wb * b[u];
-            out[e] = post * acc;
-        }
-    }
-}
-
 // Operands on different patterns: merge each row into the union pattern.
 __global__ void ew_merge_kernel(Rule r, int rows, const int* __restrict__ aptr, const int* __restrict__ acol,
                                 const double* __restrict__ ja, const int* __restrict__ bptr,
@@ -450,42 +374,6 @@ __global__ void merge_map_kernel(int rows, const int* __restrict__ aptr, const i
             const int c = ocol[p];
             ia[p] = (pa < ea && acol[pa] == c) ? pa++ : -1;
             ib[p] = (pb < eb && bcol[pb] == c) ? pb++ : -1;
-        }
-    }
-}
-
-// ew_mapped_kernel four entries per thread per round (see ew_flat_ilp_kernel).
-__global__ void ew_mapped_ilp_kernel(Rule r, const int* __restrict__ rowidx, const int* __restrict__ ia,
-                                     const int* __restrict__ ib, const double* __restrict__ ja,
-                                     const double* __restrict__ jb, double* __restrict__ out, int64_t nnz)
-{
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < nnz; e0 += kIlp * stride) {
-        int row[kIlp], xa[kIlp], xb[kIlp];
-#pragma unroll
-        for (int u = 0; u < kIlp; ++u) {
-            const int64_t e = e0 + u * stride;
-            const bool ok = e < nnz;
-            row[u] = ok ? rowidx[e] : 0;
-            xa[u] = ok ? ia[e] : -1;
-            xb[u] = ok ? ib[e] : -1;
-        }
-        double a[kIlp], b[kIlp];
-#pragma unroll
-        for (int u = 0; u < kIlp; ++u) {
-            a[u] = xa[u] >= 0 ? ja[xa[u]] : 0.0;
-            b[u] = xb[u] >= 0 ? jb[xb[u]] : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < kIlp; ++u) {
-            const int64_t e = e0 + u * stride;
-            if (e >= nnz) break;
-            double wa, wb, post;
-            rule_weights(r, row[u], wa, wb, post);
-            double acc = 0.0;
-            if (xa[u] >= 0) acc += wa * a[u];
-            if (xb[u] >= 0) acc += wb * b[u];
-            out[e] = post * acc;
         }
     }
 }
@@ -617,14 +505,9 @@ void spgemm_numeric(Core& c, const OpMatrix& m, const Pattern& jp, const double*
         // output values
         const double bytes = 16.0 * op.nnz + 12.0 * op.plan_entries + 4.0 * (m.n_out + 1) + 8.0 * m.nnz;
         launch(c, "spgemm_planned", [&] {
-            if (c.param_i("ew_ilp", 1) != 0)
-                spgemm_planned_ilp_kernel<<<blocksFor((op.nnz + kIlp - 1) / kIlp), kThreads, 0, c.stream>>>(
-                    op.nnz, op.rowidx->as<int>(), m.ptr->as<int>(), m.w->as<double>(), op.plan_start->as<int>(),
-                    op.plan_contrib->as<int>(), jv, ov);
-            else
-                spgemm_planned_kernel<<<blocksFor(op.nnz), kThreads, 0, c.stream>>>(
-                    op.nnz, op.rowidx->as<int>(), m.ptr->as<int>(), m.w->as<double>(), op.plan_start->as<int>(),
-                    op.plan_contrib->as<int>(), jv, ov);
+            spgemm_planned_kernel<<<blocksFor(op.nnz), kThreads, 0, c.stream>>>(
+                op.nnz, op.rowidx->as<int>(), m.ptr->as<int>(), m.w->as<double>(), op.plan_start->as<int>(),
+                op.plan_contrib->as<int>(), jv, ov);
         }, bytes);
         return;
     }
@@ -884,14 +767,8 @@ void jacobian_elementwise(Core& c, const JacArgs& a, const Pattern& out, double*
     }
     if (flat) {
         pattern_build_rowidx(c, const_cast<Pattern&>(out));
-        launch(c, "jac_flat", [&] {
-            if (c.param_i("ew_ilp", 1) != 0)
-                ew_flat_ilp_kernel<<<blocksFor((out.nnz + kIlp - 1) / kIlp), kThreads, 0, c.stream>>>(
-                    r, out.rowidx->as<int>(), a.pa ? a.ja : nullptr, a.pb ? a.jb : nullptr, jout, out.nnz);
-            else
-                ew_flat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(
-                    r, out.rowidx->as<int>(), a.pa ? a.ja : nullptr, a.pb ? a.jb : nullptr, jout, out.nnz);
-        }, bytes);
+        launch(c, "jac_flat", [&] { ew_flat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(r, out.rowidx->as<int>(), a.pa ? a.ja : nullptr,
+                                                                      a.pb ? a.jb : nullptr, jout, out.nnz); }, bytes);
     } else if (out.nnz < (int64_t)INT_MAX / 2) {
         // through position maps kept with the output pattern
         Pattern& o = const_cast<Pattern&>(out);
@@ -908,14 +785,9 @@ void jacobian_elementwise(Core& c, const JacArgs& a, const Pattern& out, double*
             });
         }
         launch(c, "jac_merge", [&] {
-            if (c.param_i("ew_ilp", 1) != 0)
-                ew_mapped_ilp_kernel<<<blocksFor((out.nnz + kIlp - 1) / kIlp), kThreads, 0, c.stream>>>(
-                    r, out.rowidx->as<int>(), maps->as<int>(), maps->as<int>() + out.nnz, a.pa ? a.ja : nullptr,
-                    a.pb ? a.jb : nullptr, jout, out.nnz);
-            else
-                ew_mapped_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(
-                    r, out.rowidx->as<int>(), maps->as<int>(), maps->as<int>() + out.nnz, a.pa ? a.ja : nullptr,
-                    a.pb ? a.jb : nullptr, jout, out.nnz);
+            ew_mapped_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(
+                r, out.rowidx->as<int>(), maps->as<int>(), maps->as<int>() + out.nnz, a.pa ? a.ja : nullptr,
+                a.pb ? a.jb : nullptr, jout, out.nnz);
         }, bytes);
     } else {
         launch(c, "jac_merge", [&] { ew_merge_kernel<<<blocksFor(out.rows), kThreads, 0, c.stream>>>(
