@@ -247,6 +247,31 @@ OpMatrixP span_matrix(Core& c, int kind, int64_t start, int64_t len, int64_t n_s
     return m;
 }
 
+// The Jacobian values of x with its deferred rules applied, stored in x in
+// place of the deferred form (the collection's value does not change).
+const double* materialized_jacobian(Core& c, const eqg_coll* x)
+{
+    if (x->jdef.n > 0) {
+        eqg_coll* w = const_cast<eqg_coll*>(x);
+        Buf jv = c.allocN<double>(x->pat->nnz > 0 ? x->pat->nnz : 1);
+        jacobian_apply_deferred(c, x->jdef, *x->pat, x->jval->as<double>(), jv->as<double>());
+        w->jval = jv;
+        w->jdef = Deferred{};
+        w->jkeep.clear();
+    }
+    return x->jval->as<double>();
+}
+
+// out takes from's Jacobian as it is: pattern, stored values, deferred rules.
+eqg_coll* sharing_jacobian(eqg_coll* out, const eqg_coll* from)
+{
+    out->pat = from->pat;
+    out->jval = from->jval;
+    out->jdef = from->jdef;
+    out->jkeep = from->jkeep;
+    return out;
+}
+
 // out = M data: values by SpMV, Jacobian by the cached conservative product.
 eqg_coll* apply_operator(const CoreP& cp, const OpMatrix& m, const eqg_coll* x)
 {
@@ -256,23 +281,71 @@ eqg_coll* apply_operator(const CoreP& cp, const OpMatrix& m, const eqg_coll* x)
     opmat_apply_values(c, m, coll_values(c, x), val->as<double>());
     if (!x->pat) return new_coll(cp, m.n_out, val);
     PatternP p = pattern_spgemm(c, m, x->pat);
+    // deferred rules on x's values go into the planned product; without a
+    // plan, x is materialized first
+    if (x->jdef.n > 0 && !spgemm_has_plan(*p)) materialized_jacobian(c, x);
     Buf jv = c.allocN<double>(p->nnz > 0 ? p->nnz : 1);
-    spgemm_values(c, m, *x->pat, x->jval->as<double>(), *p, jv->as<double>());
+    spgemm_values(c, m, *x->pat, x->jval->as<double>(), *p, jv->as<double>(), &x->jdef);
     return new_coll(cp, m.n_out, val, p, jv);
 }
 
-eqg_coll* jac_rule(const CoreP& cp, int64_t n, Buf val, JacArgs a, const eqg_coll* ca, const eqg_coll* cb)
+// Rules that scale the rows of their one Jacobian operand (see DeferredRule).
+bool deferrable_rule(int rule)
+{
+    switch (rule) {
+    case JR_ADD:
+    case JR_SUB:
+    case JR_MUL:
+    case JR_DIV:
+    case JR_SCALE_CONST:
+    case JR_DIV_BY_CONST:
+    case JR_SQRT:
+    case JR_SIGN:
+    case JR_NEG:
+    case JR_SELECT: return true;
+    default: return false;
+    }
+}
+
+// An elementwise rule's result: value `val`, Jacobian by the rule over the
+// operands' Jacobians.  With one Jacobian operand the rule scales its rows:
+// it is deferred (kept on the result, applied by the readers) instead of
+// run, up to kMaxDeferred rules per Jacobian.  mask_keep: the mask buffer
+// the rule reads, if any.
+eqg_coll* jac_rule(const CoreP& cp, int64_t n, Buf val, JacArgs a, const eqg_coll* ca, const eqg_coll* cb,
+                   Buf mask_keep = nullptr)
 {
     Core& c = *cp;
     const PatternP pa = ca ? ca->pat : nullptr;
     const PatternP pb = cb ? cb->pat : nullptr;
     if (!pa && !pb) return new_coll(cp, n, val);
     if (pa && pb && pa->cols != pb->cols) fail(EQG_ERR_ARG, "Jacobians with different numbers of columns");
+    if ((!pa || !pb) && deferrable_rule(a.rule) && c.param_i("jac_defer", 1) != 0) {
+        const eqg_coll* op = pa ? ca : cb;
+        if (op->jdef.n >= kMaxDeferred) materialized_jacobian(c, op);
+        eqg_coll* out = sharing_jacobian(new_coll(cp, n, val), op);
+        DeferredRule& r = out->jdef.r[out->jdef.n++];
+        r.rule = a.rule;
+        r.side = pa ? 0 : 1;
+        r.va = a.va;
+        r.vb = a.vb;
+        r.vout = a.vout;
+        r.mask = a.mask;
+        r.s = a.s;
+        // the value arrays the rule reads stay alive with the result
+        if (ca && ca->val) out->jkeep.push_back(ca->val);
+        if (cb && cb->val) out->jkeep.push_back(cb->val);
+        out->jkeep.push_back(val);
+        if (mask_keep) out->jkeep.push_back(mask_keep);
+        return out;
+    }
     PatternP out = pa && pb ? pattern_union(c, pa, pb) : (pa ? pa : pb);
     a.pa = pa.get();
     a.ja = pa ? ca->jval->as<double>() : nullptr;
+    a.da = pa ? ca->jdef : Deferred{};
     a.pb = pb.get();
     a.jb = pb ? cb->jval->as<double>() : nullptr;
+    a.db = pb ? cb->jdef : Deferred{};
     Buf jv = c.allocN<double>(out->nnz > 0 ? out->nnz : 1);
     jacobian_elementwise(c, a, *out, jv->as<double>());
     return new_coll(cp, n, val, out, jv);
@@ -936,7 +1009,7 @@ int eqg_coll_jacobian_to_host(const eqg_coll* c, int64_t* rowptr, int32_t* colin
             for (size_t i = 0; i < rp.size(); ++i) rowptr[i] = rp[i];
         }
         if (colind) download(core, colind, p.colind->ptr, (size_t)p.nnz * 4);
-        if (vals) download(core, vals, c->jval->ptr, (size_t)p.nnz * 8);
+        if (vals) download(core, vals, materialized_jacobian(core, c), (size_t)p.nnz * 8);
     });
 }
 
@@ -994,11 +1067,11 @@ int eqg_binary(eqg_runtime* rt, int op, const eqg_coll* a, const eqg_coll* b, eq
         // A sum with one Jacobian shares that Jacobian unchanged (Zero + J).
         if (op == EQG_ADD && (!a->pat || !b->pat)) {
             const eqg_coll* j = a->pat ? a : b;
-            *out = new_coll(rt->core, a->n, val, j->pat, j->jval);
+            *out = sharing_jacobian(new_coll(rt->core, a->n, val), j);
             return;
         }
         if (op == EQG_SUB && !b->pat) {
-            *out = new_coll(rt->core, a->n, val, a->pat, a->jval);
+            *out = sharing_jacobian(new_coll(rt->core, a->n, val), a);
             return;
         }
         JacArgs ja;
@@ -1032,11 +1105,11 @@ int eqg_binary_scalar(eqg_runtime* rt, int op, const eqg_coll* a, double s, int 
         const eqg_coll* right = nullptr;
         switch (op) {
         case EQG_ADD:
-            *out = new_coll(rt->core, a->n, val, a->pat, a->jval);
+            *out = sharing_jacobian(new_coll(rt->core, a->n, val), a);
             return;
         case EQG_SUB:
             if (!scalar_left) {
-                *out = new_coll(rt->core, a->n, val, a->pat, a->jval);
+                *out = sharing_jacobian(new_coll(rt->core, a->n, val), a);
                 return;
             }
             ja.rule = JR_NEG;
@@ -1216,7 +1289,7 @@ int eqg_select(eqg_runtime* rt, const eqg_mask* pred, const eqg_coll* a, const e
         JacArgs ja;
         ja.rule = JR_SELECT;
         ja.mask = mv;
-        *out = jac_rule(rt->core, pred->n, val, ja, a, b);
+        *out = jac_rule(rt->core, pred->n, val, ja, a, b, pred->v);
     });
 }
 
@@ -1251,6 +1324,8 @@ int eqg_span_superset(eqg_runtime* rt, const eqg_coll* a, int64_t start, int64_t
         opmat_apply_values(c, *m, coll_values(c, a), val->as<double>());
         PatternP p = pattern_spgemm(c, *m, a->pat, false);
         if (p->nnz != a->pat->nnz) fail(EQG_ERR_DEVICE, "span superset changed the number of Jacobian entries");
+        // deferred rules index the operand's rows, which the superset shifts
+        materialized_jacobian(c, a);
         *out = new_coll(rt->core, total, val, p, a->jval);
     });
 }
@@ -1332,7 +1407,7 @@ int eqg_solve_for_update(eqg_runtime* rt, const eqg_coll* residual, eqg_coll** d
         if (!residual->pat) fail(EQG_ERR_ARG, "solveForUpdate: residual has no Jacobian");
         if (residual->pat->rows != residual->pat->cols) fail(EQG_ERR_ARG, "solveForUpdate: Jacobian is not square");
         Buf x = c.allocN<double>(residual->n > 0 ? residual->n : 1);
-        SolveResult r = linear_solve(c, residual->pat, residual->jval->as<double>(), coll_values(c, residual),
+        SolveResult r = linear_solve(c, residual->pat, materialized_jacobian(c, residual), coll_values(c, residual),
                                      x->as<double>());
         c.solver.linear_solves++;
         c.solver.krylov_iterations += r.iterations;

@@ -363,6 +363,29 @@ void k_is_strictly_sorted(Core& c, const int32_t* a, int64_t n, int32_t* flag);
 double k_reduce(Core& c, int op, const double* a, int64_t n);
 double k_two_norm(Core& c, const double* a, int64_t n);
 
+// An elementwise rule with one Jacobian operand (a row scaling: product or
+// quotient by a collection without Jacobian, by a constant, negation, sqrt,
+// sign, trinaryIf with one differentiable branch), kept on the result
+// instead of applied: the result shares the operand's pattern and stored
+// values, and every reader applies the deferred rules in order, row by row,
+// with the arithmetic of the eager kernel (post_i * (0 + w_i x), w_i the
+// rule's weight of the operand's side).  A chain of such rules then costs no
+// pass over the Jacobian of its own.
+struct DeferredRule {
+    int rule = 0;  // a JacRule
+    int side = 0;  // 0: the operand is a (weight wa), 1: b (weight wb)
+    const double* va = nullptr;
+    const double* vb = nullptr;
+    const double* vout = nullptr;
+    const uint8_t* mask = nullptr;
+    double s = 0.0;
+};
+constexpr int kMaxDeferred = 4;
+struct Deferred {
+    int n = 0;
+    DeferredRule r[kMaxDeferred];
+};
+
 // Operator matrices and Jacobians (jacobian.cu)
 OpMatrixP opmat_from_map(Core& c, const int32_t* map_dev, int n_out, int n_src, bool allow_missing);
 OpMatrixP opmat_from_host(Core& c, int n_out, int n_src, const std::vector<int32_t>& ptr,
@@ -376,8 +399,11 @@ PatternP pattern_identity(Core& c, int n);
 Buf ones(Core& c, int64_t n);
 // with_plan: also build the output's position plan (spgemm_plan_kernel)
 PatternP pattern_spgemm(Core& c, const OpMatrix& m, const PatternP& j, bool with_plan = true);
+// ov = M jv; with deferred rules on jv only through the output's position
+// plan (spgemm_has_plan), whose kernel applies them per source row.
 void spgemm_values(Core& c, const OpMatrix& m, const Pattern& jp, const double* jv, const Pattern& op,
-                   double* ov);
+                   double* ov, const Deferred* jd = nullptr);
+inline bool spgemm_has_plan(const Pattern& op) { return (bool)op.plan_start; }
 PatternP pattern_union(Core& c, const PatternP& a, const PatternP& b);
 // Elementwise Jacobian rule: out_row(i) = post_i * (wa_i * A_row(i) (+) wb_i * B_row(i)).
 // Weights come from the operand values per op (see jacobian.cu).
@@ -401,8 +427,11 @@ struct JacArgs {
     const double* ja = nullptr;
     const Pattern* pb = nullptr;
     const double* jb = nullptr;
+    Deferred da, db;  // rules deferred on the operands' stored values
 };
 void jacobian_elementwise(Core& c, const JacArgs& args, const Pattern& out, double* jout);
+// Stored values with the deferred rules applied (one pass), into out.
+void jacobian_apply_deferred(Core& c, const Deferred& d, Pattern& p, const double* j, double* out);
 void pattern_build_rowidx(Core& c, Pattern& p);
 // Inclusive scan of int64 per-row counts into an int32 rowptr; returns nnz.
 int64_t counts_to_rowptr(Core& c, Buf& counts, int rows, Buf& rowptr);
@@ -448,7 +477,9 @@ struct eqg_coll {
     int64_t n = 0;
     eqg::Buf val;           // double[n]; null while `lazy` is pending
     eqg::PatternP pat;      // null: no Jacobian
-    eqg::Buf jval;          // double[nnz]
+    eqg::Buf jval;          // double[nnz], before the rules in jdef
+    eqg::Deferred jdef;     // row rules deferred on jval (see DeferredRule)
+    std::vector<eqg::Buf> jkeep;  // value arrays those rules read
     eqg::LazyP lazy;        // deferred value-only expression
 };
 

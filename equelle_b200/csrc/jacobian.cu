@@ -27,6 +27,78 @@ namespace {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
 // ---------------------------------------------------------------------------
+// Elementwise Jacobian rules.
+// ---------------------------------------------------------------------------
+struct Rule {
+    int rule;
+    const double* va;
+    const double* vb;
+    const double* vout;
+    const uint8_t* mask;
+    double s;
+};
+
+__device__ __forceinline__ void rule_weights(const Rule& r, int64_t i, double& wa, double& wb, double& post)
+{
+    wa = 1.0;
+    wb = 1.0;
+    post = 1.0;
+    switch (r.rule) {
+    case JR_ADD: break;
+    case JR_SUB: wb = -1.0; break;
+    case JR_MUL: {
+        // D2*Ja + D1*Jb with D1 = diag(a), D2 = diag(b)
+        const double a = r.va ? r.va[i] : r.s;
+        const double b = r.vb ? r.vb[i] : r.s;
+        wa = b;
+        wb = a;
+        break;
+    }
+    case JR_DIV: {
+        // D3*(D2*Ja - D1*Jb), D3 = diag(1/(b*b))
+        const double a = r.va ? r.va[i] : r.s;
+        const double b = r.vb ? r.vb[i] : r.s;
+        wa = b;
+        wb = -a;
+        post = 1.0 / (b * b);
+        break;
+    }
+    case JR_SCALE_CONST: wa = r.s; break;
+    case JR_DIV_BY_CONST:
+        wa = r.s;
+        post = 1.0 / (r.s * r.s);
+        break;
+    case JR_SQRT: wa = 0.5 / r.vout[i]; break;
+    case JR_SIGN: wa = r.va[i] >= 0.0 ? 1.0 : -1.0; break;
+    case JR_NEG: wa = -1.0; break;
+    case JR_SELECT: {
+        const bool m = r.mask[i] != 0;
+        wa = m ? 1.0 : 0.0;
+        wb = m ? 0.0 : 1.0;
+        break;
+    }
+    }
+}
+
+
+// The deferred rules of an operand applied to one of its stored values in
+// row `row`, in order, each with the eager kernel's arithmetic.
+__device__ __forceinline__ double apply_deferred(const Deferred& d, int64_t row, double x)
+{
+    for (int k = 0; k < d.n; ++k) {
+        const DeferredRule& q = d.r[k];
+        const Rule r{q.rule, q.va, q.vb, q.vout, q.mask, q.s};
+        double wa, wb, post;
+        rule_weights(r, row, wa, wb, post);
+        double acc = 0.0;
+        acc += (q.side == 0 ? wa : wb) * x;
+        x = post * acc;
+    }
+    return x;
+}
+
+
+// ---------------------------------------------------------------------------
 // Conservative product M*J by K-way merge of the selected rows of J.
 // ---------------------------------------------------------------------------
 template <int KMAX>
@@ -175,7 +247,7 @@ __global__ void spgemm_plan_kernel(int n_out, const int* __restrict__ mptr, cons
 __global__ void spgemm_planned_kernel(int64_t nnz, const int* __restrict__ rowidx, const int* __restrict__ mptr,
                                       const double* __restrict__ mw, const int* __restrict__ start,
                                       const int* __restrict__ contrib, const double* __restrict__ jval,
-                                      double* __restrict__ oval)
+                                      double* __restrict__ oval, const int* __restrict__ msrc, const Deferred dj)
 {
     GRID_STRIDE(e, nnz)
     {
@@ -184,7 +256,10 @@ __global__ void spgemm_planned_kernel(int64_t nnz, const int* __restrict__ rowid
         double acc = 0.0;
         for (int k = start[e]; k < k1; ++k) {
             const int q = contrib[k];
-            acc += mw[m0 + (q >> kPlanShift)] * jval[q & kPlanMask];
+            const int t = q >> kPlanShift;
+            // J's value with its deferred rules, in J's row (M's source)
+            const double jv = dj.n ? apply_deferred(dj, msrc[m0 + t], jval[q & kPlanMask]) : jval[q & kPlanMask];
+            acc += mw[m0 + t] * jv;
         }
         oval[e] = acc;
     }
@@ -257,62 +332,13 @@ __global__ void i64_to_rowptr_kernel(const int64_t* incl, int n, int* rowptr)
 }
 
 // ---------------------------------------------------------------------------
-// Elementwise Jacobian rules.
+// Elementwise Jacobian rules over patterns (operands read through their
+// deferred rules da, db).
 // ---------------------------------------------------------------------------
-struct Rule {
-    int rule;
-    const double* va;
-    const double* vb;
-    const double* vout;
-    const uint8_t* mask;
-    double s;
-};
-
-__device__ __forceinline__ void rule_weights(const Rule& r, int64_t i, double& wa, double& wb, double& post)
-{
-    wa = 1.0;
-    wb = 1.0;
-    post = 1.0;
-    switch (r.rule) {
-    case JR_ADD: break;
-    case JR_SUB: wb = -1.0; break;
-    case JR_MUL: {
-        // D2*Ja + D1*Jb with D1 = diag(a), D2 = diag(b)
-        const double a = r.va ? r.va[i] : r.s;
-        const double b = r.vb ? r.vb[i] : r.s;
-        wa = b;
-        wb = a;
-        break;
-    }
-    case JR_DIV: {
-        // D3*(D2*Ja - D1*Jb), D3 = diag(1/(b*b))
-        const double a = r.va ? r.va[i] : r.s;
-        const double b = r.vb ? r.vb[i] : r.s;
-        wa = b;
-        wb = -a;
-        post = 1.0 / (b * b);
-        break;
-    }
-    case JR_SCALE_CONST: wa = r.s; break;
-    case JR_DIV_BY_CONST:
-        wa = r.s;
-        post = 1.0 / (r.s * r.s);
-        break;
-    case JR_SQRT: wa = 0.5 / r.vout[i]; break;
-    case JR_SIGN: wa = r.va[i] >= 0.0 ? 1.0 : -1.0; break;
-    case JR_NEG: wa = -1.0; break;
-    case JR_SELECT: {
-        const bool m = r.mask[i] != 0;
-        wa = m ? 1.0 : 0.0;
-        wb = m ? 0.0 : 1.0;
-        break;
-    }
-    }
-}
-
 // Operands share the output pattern: one thread per nonzero.
 __global__ void ew_flat_kernel(Rule r, const int* __restrict__ rowidx, const double* __restrict__ ja,
-                               const double* __restrict__ jb, double* __restrict__ out, int64_t nnz)
+                               const double* __restrict__ jb, double* __restrict__ out, int64_t nnz,
+                               const Deferred da, const Deferred db)
 {
     GRID_STRIDE(e, nnz)
     {
@@ -320,10 +346,17 @@ __global__ void ew_flat_kernel(Rule r, const int* __restrict__ rowidx, const dou
         double wa, wb, post;
         rule_weights(r, i, wa, wb, post);
         double acc = 0.0;
-        if (ja) acc += wa * ja[e];
-        if (jb) acc += wb * jb[e];
+        if (ja) acc += wa * apply_deferred(da, i, ja[e]);
+        if (jb) acc += wb * apply_deferred(db, i, jb[e]);
         out[e] = post * acc;
     }
+}
+
+// out = the stored values with their deferred rules applied.
+__global__ void apply_deferred_kernel(const Deferred d, const int* __restrict__ rowidx, const double* __restrict__ j,
+                                      double* __restrict__ out, int64_t nnz)
+{
+    GRID_STRIDE(e, nnz) out[e] = apply_deferred(d, rowidx[e], j[e]);
 }
 
 // Operands on different patterns: merge each row into the union pattern.
@@ -331,7 +364,7 @@ __global__ void ew_merge_kernel(Rule r, int rows, const int* __restrict__ aptr, 
                                 const double* __restrict__ ja, const int* __restrict__ bptr,
                                 const int* __restrict__ bcol, const double* __restrict__ jb,
                                 const int* __restrict__ optr, const int* __restrict__ ocol,
-                                double* __restrict__ out)
+                                double* __restrict__ out, const Deferred da, const Deferred db)
 {
     GRID_STRIDE(i, rows)
     {
@@ -343,8 +376,8 @@ __global__ void ew_merge_kernel(Rule r, int rows, const int* __restrict__ aptr, 
         for (int p = optr[i]; p < p1; ++p) {
             const int c = ocol[p];
             double acc = 0.0;
-            if (pa < ea && acol[pa] == c) acc += wa * ja[pa++];
-            if (pb < eb && bcol[pb] == c) acc += wb * jb[pb++];
+            if (pa < ea && acol[pa] == c) acc += wa * apply_deferred(da, i, ja[pa++]);
+            if (pb < eb && bcol[pb] == c) acc += wb * apply_deferred(db, i, jb[pb++]);
             out[p] = post * acc;
         }
     }
@@ -353,9 +386,15 @@ __global__ void ew_merge_kernel(Rule r, int rows, const int* __restrict__ aptr, 
 // out = [x (n1 values), y (n2 values)]: the sum of two Jacobians whose
 // entries lie in disjoint row ranges (each entry 1.0 * its one operand).
 __global__ void concat_kernel(const double* __restrict__ x, int64_t n1, const double* __restrict__ y, int64_t n2,
-                              double* __restrict__ out)
+                              double* __restrict__ out, const int* __restrict__ rowidx, const Deferred dx,
+                              const Deferred dy)
 {
-    GRID_STRIDE(e, n1 + n2) out[e] = e < n1 ? x[e] : y[e - n1];
+    if (dx.n == 0 && dy.n == 0) {
+        GRID_STRIDE(e, n1 + n2) out[e] = e < n1 ? x[e] : y[e - n1];
+    } else {
+        GRID_STRIDE(e, n1 + n2) out[e] = e < n1 ? apply_deferred(dx, rowidx[e], x[e])
+                                                : apply_deferred(dy, rowidx[e], y[e - n1]);
+    }
 }
 
 // Position in each operand of every entry of the union pattern (-1: absent),
@@ -382,7 +421,8 @@ __global__ void merge_map_kernel(int rows, const int* __restrict__ aptr, const i
 // same operations in the same order.
 __global__ void ew_mapped_kernel(Rule r, const int* __restrict__ rowidx, const int* __restrict__ ia,
                                  const int* __restrict__ ib, const double* __restrict__ ja,
-                                 const double* __restrict__ jb, double* __restrict__ out, int64_t nnz)
+                                 const double* __restrict__ jb, double* __restrict__ out, int64_t nnz,
+                                 const Deferred da, const Deferred db)
 {
     GRID_STRIDE(e, nnz)
     {
@@ -391,8 +431,8 @@ __global__ void ew_mapped_kernel(Rule r, const int* __restrict__ rowidx, const i
         rule_weights(r, i, wa, wb, post);
         const int xa = ia[e], xb = ib[e];
         double acc = 0.0;
-        if (xa >= 0) acc += wa * ja[xa];
-        if (xb >= 0) acc += wb * jb[xb];
+        if (xa >= 0) acc += wa * apply_deferred(da, i, ja[xa]);
+        if (xb >= 0) acc += wb * apply_deferred(db, i, jb[xb]);
         out[e] = post * acc;
     }
 }
@@ -496,9 +536,11 @@ void spgemm_build_plan(Core& c, const OpMatrix& m, const Pattern& j, Pattern& ou
 }
 
 template <int KMAX>
-void spgemm_numeric(Core& c, const OpMatrix& m, const Pattern& jp, const double* jv, const Pattern& op, double* ov)
+void spgemm_numeric(Core& c, const OpMatrix& m, const Pattern& jp, const double* jv, const Pattern& op, double* ov,
+                    const Deferred& jd)
 {
     if (m.n_out <= 0) return;
+    if (jd.n && !op.plan_start) fail(EQG_ERR_DEVICE, "operator product of deferred Jacobian values without a plan");
     if (op.plan_start) {
         // algorithmic bytes: the output's row indices and plan, the
         // contributing Jacobian values and M's row pointers and weights, the
@@ -507,8 +549,8 @@ void spgemm_numeric(Core& c, const OpMatrix& m, const Pattern& jp, const double*
         launch(c, "spgemm_planned", [&] {
             spgemm_planned_kernel<<<blocksFor(op.nnz), kThreads, 0, c.stream>>>(
                 op.nnz, op.rowidx->as<int>(), m.ptr->as<int>(), m.w->as<double>(), op.plan_start->as<int>(),
-                op.plan_contrib->as<int>(), jv, ov);
-        }, bytes);
+                op.plan_contrib->as<int>(), jv, ov, m.src->as<int>(), jd);
+        }, bytes + 16.0 * jd.n * jp.rows);
         return;
     }
     // algorithmic bytes: M (row pointers, sources, weights), the Jacobian
@@ -660,16 +702,28 @@ PatternP pattern_spgemm(Core& c, const OpMatrix& m, const PatternP& j, bool with
     return p;
 }
 
-void spgemm_values(Core& c, const OpMatrix& m, const Pattern& jp, const double* jv, const Pattern& op, double* ov)
+void spgemm_values(Core& c, const OpMatrix& m, const Pattern& jp, const double* jv, const Pattern& op, double* ov,
+                   const Deferred* jd)
 {
+    const Deferred none;
+    const Deferred& d = jd ? *jd : none;
     switch (kmax_for(m.max_row)) {
-    case 1: spgemm_numeric<1>(c, m, jp, jv, op, ov); break;
-    case 2: spgemm_numeric<2>(c, m, jp, jv, op, ov); break;
-    case 4: spgemm_numeric<4>(c, m, jp, jv, op, ov); break;
-    case 6: spgemm_numeric<6>(c, m, jp, jv, op, ov); break;
-    case 8: spgemm_numeric<8>(c, m, jp, jv, op, ov); break;
-    default: spgemm_numeric<16>(c, m, jp, jv, op, ov); break;
+    case 1: spgemm_numeric<1>(c, m, jp, jv, op, ov, d); break;
+    case 2: spgemm_numeric<2>(c, m, jp, jv, op, ov, d); break;
+    case 4: spgemm_numeric<4>(c, m, jp, jv, op, ov, d); break;
+    case 6: spgemm_numeric<6>(c, m, jp, jv, op, ov, d); break;
+    case 8: spgemm_numeric<8>(c, m, jp, jv, op, ov, d); break;
+    default: spgemm_numeric<16>(c, m, jp, jv, op, ov, d); break;
     }
+}
+
+void jacobian_apply_deferred(Core& c, const Deferred& d, Pattern& p, const double* j, double* out)
+{
+    if (p.nnz <= 0) return;
+    pattern_build_rowidx(c, p);
+    launch(c, "jac_deferred", [&] {
+        apply_deferred_kernel<<<blocksFor(p.nnz), kThreads, 0, c.stream>>>(d, p.rowidx->as<int>(), j, out, p.nnz);
+    }, 20.0 * p.nnz + 4.0 * p.nnz + 16.0 * d.n * p.rows);
 }
 
 PatternP pattern_union(Core& c, const PatternP& a, const PatternP& b)
@@ -752,7 +806,7 @@ void jacobian_elementwise(Core& c, const JacArgs& a, const Pattern& out, double*
     const int64_t na = a.pa ? a.pa->nnz : 0, nbv = a.pb ? a.pb->nnz : 0;
     const double per_row = 8.0 * ((a.va ? 1 : 0) + (a.vb ? 1 : 0) + (a.vout ? 1 : 0)) + (a.mask ? 1.0 : 0.0);
     const double bytes = 8.0 * (na + nbv + out.nnz) + 4.0 * (out.rows + 1) + per_row * out.rows +
-                         (flat ? 0.0 : 4.0 * (na + nbv + out.nnz));
+                         (flat ? 0.0 : 4.0 * (na + nbv + out.nnz)) + 16.0 * (a.da.n + a.db.n) * out.rows;
     if (a.rule == JR_ADD && a.pa && a.pb && out.concat_first && c.param_i("jac_concat", 1) != 0 &&
         ((a.pa->id == out.concat_first && a.pb->id == out.concat_second) ||
          (a.pb->id == out.concat_first && a.pa->id == out.concat_second))) {
@@ -760,15 +814,21 @@ void jacobian_elementwise(Core& c, const JacArgs& a, const Pattern& out, double*
         const double* x = a_first ? a.ja : a.jb;
         const double* y = a_first ? a.jb : a.ja;
         const int64_t n1 = a_first ? a.pa->nnz : a.pb->nnz, n2 = out.nnz - n1;
+        const Deferred& dx = a_first ? a.da : a.db;
+        const Deferred& dy = a_first ? a.db : a.da;
+        if (dx.n || dy.n) pattern_build_rowidx(c, const_cast<Pattern&>(out));
         launch(c, "jac_concat", [&] {
-            concat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(x, n1, y, n2, jout);
+            concat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(
+                x, n1, y, n2, jout, (dx.n || dy.n) ? out.rowidx->as<int>() : nullptr, dx, dy);
         }, 16.0 * out.nnz);
         return;
     }
     if (flat) {
         pattern_build_rowidx(c, const_cast<Pattern&>(out));
-        launch(c, "jac_flat", [&] { ew_flat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(r, out.rowidx->as<int>(), a.pa ? a.ja : nullptr,
-                                                                      a.pb ? a.jb : nullptr, jout, out.nnz); }, bytes);
+        launch(c, "jac_flat", [&] {
+            ew_flat_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(
+                r, out.rowidx->as<int>(), a.pa ? a.ja : nullptr, a.pb ? a.jb : nullptr, jout, out.nnz, a.da, a.db);
+        }, bytes);
     } else if (out.nnz < (int64_t)INT_MAX / 2) {
         // through position maps kept with the output pattern
         Pattern& o = const_cast<Pattern&>(out);
@@ -787,13 +847,13 @@ void jacobian_elementwise(Core& c, const JacArgs& a, const Pattern& out, double*
         launch(c, "jac_merge", [&] {
             ew_mapped_kernel<<<blocksFor(out.nnz), kThreads, 0, c.stream>>>(
                 r, out.rowidx->as<int>(), maps->as<int>(), maps->as<int>() + out.nnz, a.pa ? a.ja : nullptr,
-                a.pb ? a.jb : nullptr, jout, out.nnz);
+                a.pb ? a.jb : nullptr, jout, out.nnz, a.da, a.db);
         }, bytes);
     } else {
         launch(c, "jac_merge", [&] { ew_merge_kernel<<<blocksFor(out.rows), kThreads, 0, c.stream>>>(
             r, out.rows, a.pa ? a.pa->rowptr->as<int>() : nullptr, a.pa ? a.pa->colind->as<int>() : nullptr,
             a.pa ? a.ja : nullptr, a.pb ? a.pb->rowptr->as<int>() : nullptr, a.pb ? a.pb->colind->as<int>() : nullptr,
-            a.pb ? a.jb : nullptr, out.rowptr->as<int>(), out.colind->as<int>(), jout); }, bytes);
+            a.pb ? a.jb : nullptr, out.rowptr->as<int>(), out.colind->as<int>(), jout, a.da, a.db); }, bytes);
     }
 }
 

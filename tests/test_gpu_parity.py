@@ -229,10 +229,11 @@ def test_fused_coarse_cycle_identical(gpu_lib, shape, precision):
 def test_assembly_fast_paths_match_generic_kernels(gpu_lib, grid):
     """The Cartesian stencil kernels (gradient, divergence values), the
     position plans of operator products, the shared values of span
-    supersets and the concatenation of row-disjoint sums give the same
-    values and Jacobians as the generic CSR kernels they replace."""
+    supersets, the concatenation of row-disjoint sums and the row rules
+    deferred into their readers give the same values and Jacobians, bit for
+    bit, as the generic kernels they replace."""
     fast = opstream.op_stream(Runtime(gpu_lib, grid))
     generic = opstream.op_stream(Runtime(gpu_lib, dict(grid, stencil_ops=0, spgemm_plan=0, span_share=0,
-                                                      jac_concat=0)))
+                                                      jac_concat=0, jac_defer=0)))
     for k in generic:
         assert_colls(fast[k], generic[k], k, rtol=0.0)
