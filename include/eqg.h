@@ -140,7 +140,8 @@ const char* eqg_backend_name(void);
  * Jacobian pattern and precision; 0: 256 and the largest cluster),
  * linsolver_tune_file (a JSON file caching those choices; default
  * $EQG_TUNE_FILE, else none), spgemm_plan / span_share / jac_concat /
- * stencil_ops (1; 0 switches off an assembly fast path, for comparisons),
+ * jac_defer / stencil_ops (1; 0 switches off an assembly fast path, for
+ * comparisons),
  * gather_rows (0), time_kernel
  * (a kernel name, or "*", to time with CUDA events) and device (CUDA device
  * index; default: the calling thread's current device).  grid_filename
