@@ -320,7 +320,7 @@ eqg_coll* jac_rule(const CoreP& cp, int64_t n, Buf val, JacArgs a, const eqg_col
     const PatternP pb = cb ? cb->pat : nullptr;
     if (!pa && !pb) return new_coll(cp, n, val);
     if (pa && pb && pa->cols != pb->cols) fail(EQG_ERR_ARG, "Jacobians with different numbers of columns");
-    if ((!pa || !pb) && deferrable_rule(a.rule) && c.param_i("jac_defer", 1) != 0) {
+    if ((!pa || !pb) && deferrable_rule(a.rule) && c.jac_defer) {
         const eqg_coll* op = pa ? ca : cb;
         if (op->jdef.n >= kMaxDeferred) materialized_jacobian(c, op);
         eqg_coll* out = sharing_jacobian(new_coll(cp, n, val), op);
@@ -429,6 +429,10 @@ int eqg_runtime_create(int nparams, const char* const* keys, const char* const* 
         c.max_iter = c.param_i("max_iter", 10);
         c.abs_res_tol = c.param_d("abs_res_tol", 1e-6);
         c.timed_kernel = c.param_s("time_kernel", "");
+        c.jac_concat = c.param_i("jac_concat", 1) != 0;
+        c.jac_defer = c.param_i("jac_defer", 1) != 0;
+        c.stencil_ops = c.param_i("stencil_ops", 1) != 0;
+        c.span_share = c.param_i("span_share", 1) != 0;
         c.red_partials = c.allocN<double>((size_t)kRedBlocks * 4);
         c.red_counter = c.allocN<unsigned int>(1);
         if (c.params.count("grid_filename")) build_grid_from_file(c, c.params["grid_filename"], rt->builtin);
@@ -1312,7 +1316,7 @@ int eqg_span_superset(eqg_runtime* rt, const eqg_coll* a, int64_t start, int64_t
         if (start < 0 || start + a->n > total) fail(EQG_ERR_ARG, "span out of range");
         OpMatrixP m = span_matrix(*rt->core, MAP_SUPERSET, start, a->n, a->n, total);
         Core& c = *rt->core;
-        if (!a->pat || c.param_i("span_share", 1) == 0) {
+        if (!a->pat || !c.span_share) {
             *out = apply_operator(rt->core, *m, a);
             return;
         }

@@ -180,6 +180,8 @@ struct Core {
     // settings
     int verbose = 0, max_iter = 10;
     double abs_res_tol = 1e-6;
+    // assembly fast paths (parameters of the same names, read once)
+    bool jac_concat = true, jac_defer = true, stencil_ops = true, span_share = true;
 
     // accounting
     std::atomic<int64_t> launches{0};

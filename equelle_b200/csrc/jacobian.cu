@@ -630,7 +630,7 @@ OpMatrixP opmat_from_map(Core& c, const int32_t* map_dev, int n_out, int n_src, 
 void opmat_apply_values(Core& c, const OpMatrix& m, const double* x, double* y)
 {
     if (m.n_out <= 0) return;
-    if (m.stencil && c.param_i("stencil_ops", 1) != 0 && stencil_apply_values(c, m.stencil, x, y)) return;
+    if (m.stencil && c.stencil_ops && stencil_apply_values(c, m.stencil, x, y)) return;
     launch(c, "opmat_apply", [&] { opmat_apply_kernel<<<blocksFor(m.n_out), kThreads, 0, c.stream>>>(m.n_out, m.ptr->as<int>(), m.src->as<int>(),
                                                                      m.w->as<double>(), x, y); },
            4.0 * (m.n_out + 1) + 12.0 * m.nnz + 8.0 * m.n_src + 8.0 * m.n_out);
@@ -807,7 +807,7 @@ void jacobian_elementwise(Core& c, const JacArgs& a, const Pattern& out, double*
     const double per_row = 8.0 * ((a.va ? 1 : 0) + (a.vb ? 1 : 0) + (a.vout ? 1 : 0)) + (a.mask ? 1.0 : 0.0);
     const double bytes = 8.0 * (na + nbv + out.nnz) + 4.0 * (out.rows + 1) + per_row * out.rows +
                          (flat ? 0.0 : 4.0 * (na + nbv + out.nnz)) + 16.0 * (a.da.n + a.db.n) * out.rows;
-    if (a.rule == JR_ADD && a.pa && a.pb && out.concat_first && c.param_i("jac_concat", 1) != 0 &&
+    if (a.rule == JR_ADD && a.pa && a.pb && out.concat_first && c.jac_concat &&
         ((a.pa->id == out.concat_first && a.pb->id == out.concat_second) ||
          (a.pb->id == out.concat_first && a.pa->id == out.concat_second))) {
         const bool a_first = a.pa->id == out.concat_first;
