@@ -354,15 +354,14 @@ eqg_coll* jac_rule(const CoreP& cp, int64_t n, Buf val, JacArgs a, const eqg_col
 Buf upload(Core& c, const void* src, size_t bytes)
 {
     Buf b = c.alloc(bytes);
-    if (bytes) EQG_CUDA(cudaMemcpyAsync(b->ptr, src, bytes, cudaMemcpyHostToDevice, c.stream));
+    if (bytes) c.copy_to_device(b->ptr, src, bytes);
     return b;
 }
 
 void download(Core& c, void* dst, const void* src, size_t bytes)
 {
     if (!bytes) return;
-    EQG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c.stream));
-    c.sync();
+    c.copy_to_host(dst, src, bytes);
 }
 
 eqg_set* memo_set(const CoreP& cp, int op, const eqg_set* key_set)

@@ -106,6 +106,10 @@ Core::~Core()
         cudaStreamDestroy(stream);
     }
     if (pinned) cudaFreeHost(pinned);
+    for (int k = 0; k < 2; ++k) {
+        if (stage[k]) cudaFreeHost(stage[k]);
+        if (stage_done[k]) cudaEventDestroy(stage_done[k]);
+    }
 }
 
 // Size classes of the caching allocator: multiples of 256 B up to 64 KiB,
@@ -204,6 +208,61 @@ std::string Core::param_s(const std::string& k, const std::string& d) const
 {
     auto it = params.find(k);
     return it == params.end() ? d : it->second;
+}
+
+namespace {
+constexpr size_t kStageBytes = 16u << 20;
+
+void ensure_stage(Core& c)
+{
+    for (int k = 0; k < 2; ++k) {
+        if (!c.stage[k]) EQG_CUDA(cudaMallocHost((void**)&c.stage[k], kStageBytes));
+        if (!c.stage_done[k]) EQG_CUDA(cudaEventCreateWithFlags(&c.stage_done[k], cudaEventDisableTiming));
+    }
+}
+}  // namespace
+
+void Core::copy_to_device(void* dst, const void* src, size_t bytes)
+{
+    if (bytes < (1u << 20)) {  // small: one pageable copy
+        if (bytes) EQG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+        sync();
+        return;
+    }
+    ensure_stage(*this);
+    size_t off = 0;
+    for (int k = 0; off < bytes; k ^= 1) {
+        const size_t n = std::min(kStageBytes, bytes - off);
+        EQG_CUDA(cudaEventSynchronize(stage_done[k]));  // its previous chunk has left the buffer
+        std::memcpy(stage[k], (const char*)src + off, n);
+        EQG_CUDA(cudaMemcpyAsync((char*)dst + off, stage[k], n, cudaMemcpyHostToDevice, stream));
+        EQG_CUDA(cudaEventRecord(stage_done[k], stream));
+        off += n;
+    }
+    sync();
+}
+
+void Core::copy_to_host(void* dst, const void* src, size_t bytes)
+{
+    if (bytes < (1u << 20)) {
+        if (bytes) EQG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream));
+        sync();
+        return;
+    }
+    ensure_stage(*this);
+    const size_t chunks = (bytes + kStageBytes - 1) / kStageBytes;
+    auto start = [&](size_t i) {
+        const size_t off = i * kStageBytes, n = std::min(kStageBytes, bytes - off);
+        EQG_CUDA(cudaMemcpyAsync(stage[i & 1], (const char*)src + off, n, cudaMemcpyDeviceToHost, stream));
+        EQG_CUDA(cudaEventRecord(stage_done[i & 1], stream));
+    };
+    start(0);
+    for (size_t i = 0; i < chunks; ++i) {
+        if (i + 1 < chunks) start(i + 1);  // the next chunk's DMA while this one is copied out
+        EQG_CUDA(cudaEventSynchronize(stage_done[i & 1]));
+        const size_t off = i * kStageBytes, n = std::min(kStageBytes, bytes - off);
+        std::memcpy((char*)dst + off, stage[i & 1], n);
+    }
 }
 
 // ---------------------------------------------------------------------------

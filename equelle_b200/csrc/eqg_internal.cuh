@@ -202,6 +202,10 @@ struct Core {
     Buf red_partials;   // double[kRedBlocks * 4]
     Buf red_counter;    // unsigned int
     double* pinned = nullptr;  // small pinned host buffer
+    // pinned staging for large copies between device memory and pageable
+    // host memory (copy_to_device / copy_to_host), allocated on first use
+    char* stage[2] = {nullptr, nullptr};
+    cudaEvent_t stage_done[2] = {nullptr, nullptr};
     std::vector<Mark> marks;
     std::vector<eqg_solve_info> solves;
     // device timing of one named kernel (parameter time_kernel)
@@ -256,6 +260,11 @@ struct Core {
     void free(void* p, size_t bytes);
     void sync();
     void checkLaunch(const char* what);
+    // bytes between pageable host memory and device memory through the
+    // pinned staging buffers, in chunks, DMA of one chunk overlapping the
+    // host copy of the other; both return with the copy finished
+    void copy_to_device(void* dst, const void* src, size_t bytes);
+    void copy_to_host(void* dst, const void* src, size_t bytes);
     double param_d(const std::string& k, double d) const;
     int param_i(const std::string& k, int d) const;
     std::string param_s(const std::string& k, const std::string& d) const;

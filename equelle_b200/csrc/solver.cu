@@ -1765,7 +1765,7 @@ std::vector<int> stage_keys(const HostCsr& A, bool natural)
 Buf upload_ints(Core& c, const std::vector<int>& v)
 {
     Buf b = c.allocN<int>(v.empty() ? 1 : v.size());
-    if (!v.empty()) EQG_CUDA(cudaMemcpyAsync(b->ptr, v.data(), v.size() * 4, cudaMemcpyHostToDevice, c.stream));
+    if (!v.empty()) c.copy_to_device(b->ptr, v.data(), v.size() * 4);
     return b;
 }
 
@@ -2078,10 +2078,8 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     A.n = n;
     A.ptr.resize(n + 1);
     A.col.resize(p.nnz > 0 ? p.nnz : 1);
-    EQG_CUDA(cudaMemcpyAsync(A.ptr.data(), p.rowptr->ptr, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, c.stream));
-    if (p.nnz > 0)
-        EQG_CUDA(cudaMemcpyAsync(A.col.data(), p.colind->ptr, (size_t)p.nnz * 4, cudaMemcpyDeviceToHost, c.stream));
-    c.sync();
+    c.copy_to_host(A.ptr.data(), p.rowptr->ptr, (size_t)(n + 1) * 4);
+    if (p.nnz > 0) c.copy_to_host(A.col.data(), p.colind->ptr, (size_t)p.nnz * 4);
 
     const std::string pre = c.param_s("linsolver_preconditioner", "multigrid");
     if (pre != "multigrid" && pre != "ilu0") fail(EQG_ERR_ARG, "linsolver_preconditioner must be multigrid or ilu0");
