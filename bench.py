@@ -78,6 +78,8 @@ def parse():
                     help="batched: instances of the sequential FP64 arm (the first ones of the same seeded set)")
     ap.add_argument("--side-max", type=int, default=None, help="batched/serve: largest grid side")
     ap.add_argument("--max-steps", type=int, default=None, help="serve: most time steps of a request")
+    ap.add_argument("--host-threads", type=int, default=None,
+                    help="batched/serve: OpenMP threads of each runtime's solver analysis (default: cores / slots)")
     ap.add_argument("--nx", type=int)
     ap.add_argument("--ny", type=int)
     ap.add_argument("--nz", type=int)
@@ -374,7 +376,10 @@ def main():
 
         base_dir = os.path.join(tempfile.gettempdir(), "eqg_bench", "forms_r%d" % rank)
         _, sw64 = last_sw(os.path.join(base_dir, "double"), "double")
-        forms = {}
+        # the comparison is of the last step's saturation: water has entered
+        if not sw64.max() > 0.2 + 1e-3:
+            raise SystemExit("precision forms: the FP64 run's last saturation output is the initial state")
+        forms = {"sw_max_after_last_step": float(sw64.max())}
         for form in ("mixed", "refine"):
             r, sw = last_sw(os.path.join(base_dir, form), form)
             ms_f = rp.max(timed_window(r, W, K))
@@ -574,9 +579,9 @@ def main_many(a, rp):
         seq_reqs = serve.make_requests(min(a.seq_sample, a.instances), seed=1, programs=("twophase",),
                                        side=(32, side_max), steps=(a.steps, a.steps))
         seq = summary(*serve.Server(slots=1).run(prepared(seq_reqs, "double"), realtime=False))
-        bat64 = summary(*serve.Server(slots=a.slots).run(prepared(reqs, "double"), realtime=False))
+        bat64 = summary(*serve.Server(slots=a.slots, host_threads=a.host_threads).run(prepared(reqs, "double"), realtime=False))
         with ClockSampler(rp.local_rank) as clk:
-            bat = summary(*serve.Server(slots=a.slots).run(prepared(reqs, "mixed"), realtime=False))
+            bat = summary(*serve.Server(slots=a.slots, host_threads=a.host_threads).run(prepared(reqs, "mixed"), realtime=False))
         value = rp.throughput(bat["instance_steps"], 1000.0 * rp.max(bat["wall_s"]))
         line = {"metric": "instance-steps/s", "value": value, "unit": "instance-steps/s", "n_gpus": world,
                 "steps": a.steps, "warmup": 0, "ms_per_step": 1000.0 * bat["wall_s"] / bat["instance_steps"],
@@ -600,7 +605,7 @@ def main_many(a, rp):
         seq = summary(*serve.Server(slots=1).run(prepared(base, "double"), realtime=False))
         for lam in rates:
             reqs = serve.make_requests(a.requests, seed=2, rate=lam, side=(64, side_max), steps=(10, max_steps))
-            recs, wall = serve.Server(slots=a.slots).run(prepared(reqs, "mixed"), realtime=True)
+            recs, wall = serve.Server(slots=a.slots, host_threads=a.host_threads).run(prepared(reqs, "mixed"), realtime=True)
             per_rate["%g" % lam] = summary(recs, wall)
         top = per_rate["%g" % rates[-1]]
         line = {"metric": "requests/s", "value": rp.throughput(top["requests"], 1000.0 * rp.max(top["wall_s"])),
