@@ -53,6 +53,7 @@ class Stats(C.Structure):
         ("residual_evaluations", C.c_int64), ("residual_ms", C.c_double),
         ("factor_ms", C.c_double), ("krylov_ms", C.c_double),
         ("last_block_size", C.c_int64), ("last_matrix_blocks", C.c_int64),
+        ("fused_evaluations", C.c_int64),
     ]
 
     def as_dict(self):
@@ -108,6 +109,7 @@ SIGNATURES = {
     "eqg_coll_constant": (C.c_int, [vp, C.c_double, C.c_int64, vpp]),
     "eqg_coll_size": (C.c_int, [vp, c_i64_p]),
     "eqg_coll_to_host": (C.c_int, [vp, c_dbl_p]),
+    "eqg_coll_evaluate": (C.c_int, [vp, vp]),
     "eqg_output_begin": (C.c_int, [vp, vp, c_i64_p]),
     "eqg_output_wait": (C.c_int, [vp, C.c_int64, C.POINTER(c_dbl_p), c_i64_p]),
     "eqg_output_release": (C.c_int, [vp, C.c_int64]),

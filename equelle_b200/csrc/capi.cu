@@ -273,10 +273,12 @@ eqg_coll* sharing_jacobian(eqg_coll* out, const eqg_coll* from)
 }
 
 // out = M data: values by SpMV, Jacobian by the cached conservative product.
-eqg_coll* apply_operator(const CoreP& cp, const OpMatrix& m, const eqg_coll* x)
+eqg_coll* apply_operator(const CoreP& cp, const OpMatrixP& mp, const eqg_coll* x)
 {
     Core& c = *cp;
+    const OpMatrix& m = *mp;
     if (x->n != m.n_src) fail(EQG_ERR_ARG, "operator applied to a collection of the wrong size");
+    if (c.fuse && lazy_ok(c, x)) return lazy_coll(cp, m.n_out, lazy_opmat(mp, lazy_node(x)));
     Buf val = c.allocN<double>(m.n_out > 0 ? m.n_out : 1);
     opmat_apply_values(c, m, coll_values(c, x), val->as<double>());
     if (!x->pat) return new_coll(cp, m.n_out, val);
@@ -424,7 +426,6 @@ int eqg_runtime_create(int nparams, const char* const* keys, const char* const* 
         c.dy = c.param_d("dy", 1.0);
         c.dz = c.param_d("dz", 1.0);
         c.verbose = c.param_i("verbose", 0);
-        c.lazy = c.param_i("lazy", 0) != 0;
         c.max_iter = c.param_i("max_iter", 10);
         c.abs_res_tol = c.param_d("abs_res_tol", 1e-6);
         c.timed_kernel = c.param_s("time_kernel", "");
@@ -436,6 +437,12 @@ int eqg_runtime_create(int nparams, const char* const* keys, const char* const* 
         c.red_counter = c.allocN<unsigned int>(1);
         if (c.params.count("grid_filename")) build_grid_from_file(c, c.params["grid_filename"], rt->builtin);
         else build_grid(c, rt->builtin);
+        // deferred values: lazy=1 evaluates them with the expression kernel;
+        // otherwise fuse=1 (the default where a fused step exists: 2D
+        // Cartesian grids) records them for fused steps
+        c.lazy_vm = c.param_i("lazy", 0) != 0;
+        c.fuse = !c.lazy_vm && c.param_i("fuse", c.cartesian && c.dim == 2 ? 1 : 0) != 0;
+        c.lazy = c.lazy_vm || c.fuse;
         for (auto* s : rt->builtin) {
             s->core = rt->core;
             s->id = c.newId();
@@ -519,6 +526,7 @@ int eqg_runtime_stats(const eqg_runtime* rt, eqg_stats* out)
         out->residual_ms = c.residual_clock.total_ms();
         out->factor_ms = c.factor_clock.total_ms();
         out->krylov_ms = c.krylov_clock.total_ms();
+        out->fused_evaluations = c.fused_evaluations;
     });
 }
 
@@ -531,6 +539,7 @@ int eqg_runtime_reset_stats(eqg_runtime* rt)
         c.newton_solves = c.newton_iterations = 0;
         c.solver = SolverStats{};
         c.patterns_built = c.pattern_hits = 0;
+        c.fused_evaluations = 0;
         c.bytes_peak = c.bytes_in_use;
         for (auto& pr : c.timer_pairs) {
             cudaEventDestroy(pr.a);
@@ -974,6 +983,15 @@ int eqg_output_release(eqg_runtime* rt, int64_t ticket)
     });
 }
 
+int eqg_coll_evaluate(eqg_runtime* rt, const eqg_coll* x)
+{
+    return guarded(__func__, [&] {
+        need(rt, "runtime");
+        need(x, "collection");
+        settle(*rt->core, x);
+    });
+}
+
 int eqg_coll_to_host(const eqg_coll* c, double* out)
 {
     return guarded(__func__, [&] {
@@ -1205,7 +1223,7 @@ int eqg_gradient(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
         need(rt, "runtime");
         need(a, "collection");
         if (a->n != rt->core->nc) fail(EQG_ERR_ARG, "Gradient needs a collection on all cells");
-        *out = apply_operator(rt->core, *rt->core->grad, a);
+        *out = apply_operator(rt->core, rt->core->grad, a);
     });
 }
 
@@ -1215,7 +1233,7 @@ int eqg_neg_gradient(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
         need(rt, "runtime");
         need(a, "collection");
         if (a->n != rt->core->nc) fail(EQG_ERR_ARG, "negGradient needs a collection on all cells");
-        *out = apply_operator(rt->core, *rt->core->ngrad, a);
+        *out = apply_operator(rt->core, rt->core->ngrad, a);
     });
 }
 
@@ -1225,7 +1243,7 @@ int eqg_interior_divergence(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
         need(rt, "runtime");
         need(a, "collection");
         if (a->n != rt->core->nif) fail(EQG_ERR_ARG, "interiorDivergence needs a collection on interior faces");
-        *out = apply_operator(rt->core, *rt->core->div_interior, a);
+        *out = apply_operator(rt->core, rt->core->div_interior, a);
     });
 }
 
@@ -1236,11 +1254,11 @@ int eqg_divergence(eqg_runtime* rt, const eqg_coll* a, eqg_coll** out)
         need(a, "collection");
         const Core& c = *rt->core;
         if (a->n == c.nif) {
-            *out = apply_operator(rt->core, *c.div_interior, a);
+            *out = apply_operator(rt->core, c.div_interior, a);
             return;
         }
         if (a->n != c.nf) fail(EQG_ERR_ARG, "Divergence needs a collection on all or interior faces");
-        *out = apply_operator(rt->core, *c.div_full, a);
+        *out = apply_operator(rt->core, c.div_full, a);
     });
 }
 
@@ -1254,7 +1272,7 @@ int eqg_on(eqg_runtime* rt, const eqg_coll* data, const eqg_set* from, const eqg
         if (data->n != from->n) fail(EQG_ERR_ARG, "On: data size differs from its set");
         if (from->entity != to->entity) fail(EQG_ERR_ARG, "On: sets of different entity kinds");
         OpMatrixP m = on_matrix(*rt->core, const_cast<eqg_set*>(from), const_cast<eqg_set*>(to));
-        *out = apply_operator(rt->core, *m, data);
+        *out = apply_operator(rt->core, m, data);
     });
 }
 
@@ -1268,7 +1286,7 @@ int eqg_extend(eqg_runtime* rt, const eqg_coll* data, const eqg_set* from, const
         if (data->n != from->n) fail(EQG_ERR_ARG, "Extend: data size differs from its set");
         if (from->entity != to->entity) fail(EQG_ERR_ARG, "Extend: sets of different entity kinds");
         OpMatrixP m = extend_matrix(*rt->core, const_cast<eqg_set*>(from), const_cast<eqg_set*>(to));
-        *out = apply_operator(rt->core, *m, data);
+        *out = apply_operator(rt->core, m, data);
     });
 }
 
@@ -1303,7 +1321,7 @@ int eqg_span_subset(eqg_runtime* rt, const eqg_coll* a, int64_t start, int64_t n
         need(a, "collection");
         if (start < 0 || num < 0 || start + num > a->n) fail(EQG_ERR_ARG, "span out of range");
         OpMatrixP m = span_matrix(*rt->core, MAP_SUBSET, start, num, a->n, num);
-        *out = apply_operator(rt->core, *m, a);
+        *out = apply_operator(rt->core, m, a);
     });
 }
 
@@ -1316,7 +1334,7 @@ int eqg_span_superset(eqg_runtime* rt, const eqg_coll* a, int64_t start, int64_t
         OpMatrixP m = span_matrix(*rt->core, MAP_SUPERSET, start, a->n, a->n, total);
         Core& c = *rt->core;
         if (!a->pat || !c.span_share) {
-            *out = apply_operator(rt->core, *m, a);
+            *out = apply_operator(rt->core, m, a);
             return;
         }
         // The superset only inserts empty Jacobian rows: the product keeps
@@ -1340,7 +1358,9 @@ int eqg_reduce(eqg_runtime* rt, int op, const eqg_coll* a, double* out)
         need(a, "collection");
         if (op < EQG_MIN || op > EQG_PROD) fail(EQG_ERR_ARG, "unknown reduction");
         if (a->n == 0 && (op == EQG_MIN || op == EQG_MAX)) fail(EQG_ERR_ARG, "min/maxReduce of an empty collection");
-        *out = k_reduce(*rt->core, op, coll_values(*rt->core, a), a->n);
+        Core& c = *rt->core;
+        if (c.fuse && a->lazy && a->lazy->op != LZ_LEAF && fused_reduce(c, op, a->lazy.get(), out)) return;
+        *out = k_reduce(c, op, coll_values(c, a), a->n);
     });
 }
 
@@ -1435,6 +1455,19 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
         need(u0, "initial guess");
         if (!fn) fail(EQG_ERR_ARG, "null residual function");
         Core& c = *rt->core;
+        // values deferred before the solve are evaluated now; inside it
+        // every operation runs when it is called (the residual callbacks)
+        settle_all(c);
+        struct NoDeferral {
+            Core& c;
+            bool lazy, fuse;
+            ~NoDeferral()
+            {
+                c.lazy = lazy;
+                c.fuse = fuse;
+            }
+        } no_deferral{c, c.lazy, c.fuse};
+        c.lazy = c.fuse = false;
         const int m0 = mark(c);
         c.newton_solves++;
         const int64_t krylov0 = c.solver.krylov_iterations;

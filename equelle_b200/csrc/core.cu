@@ -75,6 +75,7 @@ Core::~Core()
     // Release cached device objects before the stream goes away.
     for (auto& kv : derived_sets) eqg_set_release(kv.second);
     derived_sets.clear();
+    fuse_state.reset();
     pattern_cache.clear();
     opmat_cache.clear();
     identity_patterns.clear();

@@ -218,12 +218,19 @@ struct Core {
     };
     std::vector<TimedLaunch> timer_pairs;
     PhaseClock residual_clock, factor_clock, krylov_clock;
-    // deferred elementwise expressions: mode, handles with pending values,
-    // evaluation passes run
-    bool lazy = true;
+    // deferred value expressions: recording on (`lazy`), evaluated by the
+    // expression kernel (`lazy_vm`, parameter lazy=1) or, when recorded for
+    // fusion (parameter fuse), by a fused step that matches the recorded
+    // DAG (fused.cu) or one kernel per node; handles with pending values,
+    // evaluation passes run, fused evaluations run
+    bool lazy = false;
+    bool lazy_vm = false;
+    bool fuse = false;
     std::unordered_set<eqg_coll*> lazy_colls;
     std::unordered_set<eqg_mask*> lazy_masks;
     int64_t lazy_passes = 0;
+    int64_t fused_evaluations = 0;
+    std::shared_ptr<struct FuseState> fuse_state;  // fused.cu: verified operators and arrays, cached maxima
     // asynchronous output copies (eqg_output_*): device -> pinned host on
     // their own stream.  The ticket table and the pinned pool are shared with
     // the thread that waits for copies (mutex); device buffers of finished
@@ -272,18 +279,22 @@ struct Core {
 
 using CoreP = std::shared_ptr<Core>;
 
-// ---- deferred elementwise expressions (lazy.cu) -------------------------
-// Value-only elementwise operations (arithmetic, with a scalar, unary,
-// comparisons, trinaryIf, mask logic) and constant collections are recorded
-// as nodes of a DAG over materialized arrays instead of being launched.  The
-// first operation that needs values (any other operation, a reduction, a
-// host copy) evaluates every pending node of that length in one kernel pass
-// (one thread per element, shared subexpressions computed once), with the
-// same floating-point operations, in the same order, as the
-// one-kernel-per-operation path.  Runtime parameter lazy=1 turns it on (off
-// by default: with its intermediates in shared memory an evaluation pass
-// costs about as much as the launches it replaces).
-enum LazyOp { LZ_LEAF, LZ_CONST, LZ_BIN, LZ_BINS, LZ_UNARY, LZ_CMP, LZ_CMPS, LZ_SEL, LZ_LOGIC };
+// ---- deferred value expressions (lazy.cu, fused.cu) ----------------------
+// Value-only operations (arithmetic, with a scalar, unary, comparisons,
+// trinaryIf, mask logic, constant collections and, when recorded for
+// fusion, On/Extend/gradient/divergence) are recorded as nodes of a DAG
+// over materialized arrays instead of being launched.  The first operation
+// that needs values (any other operation, a reduction, a host copy, an
+// output) evaluates them.  Two evaluators, both with the same
+// floating-point operations, in the same order, as the
+// one-kernel-per-operation path:
+//   - lazy=1: every pending node of that length in one pass of an
+//     expression kernel (intermediates in shared memory; about as costly as
+//     the launches it replaces, so off by default);
+//   - fuse=1 (the default on two-dimensional Cartesian grids, outside Newton
+//     solves): a fused step when the DAG matches one (fused.cu), else one
+//     kernel per node, the kernel the operation launches when not deferred.
+enum LazyOp { LZ_LEAF, LZ_CONST, LZ_BIN, LZ_BINS, LZ_UNARY, LZ_CMP, LZ_CMPS, LZ_SEL, LZ_LOGIC, LZ_OPMAT };
 
 struct LazyNode {
     int op = LZ_LEAF;
@@ -292,9 +303,10 @@ struct LazyNode {
     int scalar_left = 0;
     bool mask = false;     // a mask (uint8) rather than doubles
     int64_t n = 0;
-    int cost = 1;          // nodes below (an upper bound; shared nodes counted twice)
+    double cost = 1;       // nodes below (an upper bound; shared nodes counted twice)
     std::shared_ptr<LazyNode> a, b, c;
     Buf leaf;              // LZ_LEAF: the values
+    OpMatrixP m;           // LZ_OPMAT: the helper operator applied to `a`
 };
 using LazyP = std::shared_ptr<LazyNode>;
 
@@ -310,10 +322,26 @@ LazyP lazy_node(const eqg_coll* x);
 LazyP lazy_node(const eqg_mask* m);
 LazyP lazy_make(int op, int sub, int64_t n, bool mask, LazyP a, LazyP b = nullptr, LazyP c = nullptr,
                 double s = 0.0, int scalar_left = 0);
+LazyP lazy_opmat(const OpMatrixP& m, LazyP a);
 eqg_coll* lazy_coll(const CoreP& core, int64_t n, LazyP node);
 eqg_mask* lazy_mask(const CoreP& core, int64_t n, LazyP node);
 void lazy_forget(eqg_coll* x);
 void lazy_forget(eqg_mask* m);
+// Evaluates every pending handle (before a Newton solve).
+void settle_all(Core& c);
+// Evaluates a pending node (a fused step when one matches, else one kernel
+// per node); it becomes a leaf.
+void lazy_evaluate(Core& c, LazyNode* v);
+// The node becomes a leaf over `values` (its operands are released).
+void lazy_make_leaf(LazyNode* v, Buf values);
+
+// ---- fused steps (fused.cu) -------------------------------------------------
+// The pending expression under `root`, or its reduction, when it matches a
+// fused step and the grid and operands meet that step's conditions: the
+// values are computed and every matched handle settled (true); false leaves
+// everything as it was.
+bool fused_materialize(Core& c, LazyNode* root);
+bool fused_reduce(Core& c, int op, LazyNode* root, double* out);
 
 // Launches a kernel through `f`, checks the launch, and brackets it with
 // CUDA events on the runtime stream when `name` is the timed kernel.

@@ -1,0 +1,1247 @@
+// Fused explicit steps over deferred expressions.
+//
+// With fuse=1 the runtime records value-only operations as a DAG (lazy.cu)
+// instead of launching them.  When a value is needed, the DAG under it is
+// compared with the DAG of a known explicit step, written below with the
+// same operations in the same arrangement as the generated program that
+// makes it.  On a match, and when the grid and the operands meet the
+// step's conditions (checked once per operator or array, on the device),
+// hand-written kernels compute the step's results; otherwise every node
+// runs its own kernel.  Each fused kernel performs, element by element, the
+// same IEEE double operations in the same order as the kernels of the
+// one-operation path (round-to-nearest intrinsics, so that nothing is
+// contracted into a fused multiply-add), so both give the same bits.
+//
+// The step here is the shallow-water step of equelle_b200/sims/swe.cpp (the
+// reference's examples/dsl/swe.equelle:396-452 with a Rusanov flux): two
+// forward-Euler stages of a finite-volume update with the face fluxes of
+// both sides, wall fluxes on the boundary and the bathymetry source term,
+// averaged as Heun's method, and the CFL wave-speed maximum of the state.
+// Conditions: a two-dimensional Cartesian grid with uniform cell volumes and
+// uniform face areas per direction, unit face normals, the runtime's own
+// first/second-cell and boundary-cell selections and extensions, and every
+// cell array of the grid's size.
+//
+// Per cell and time step the fused path reads the state and five bottom
+// arrays in each stage and the step's start state in the second, and writes
+// the state twice: 200 bytes, against the 112 of the step's minimum (one
+// bottom array per stage).  The one-operation path runs ~250 kernels per
+// step.
+#include "eqg_internal.cuh"
+
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <unordered_map>
+
+namespace eqg {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Patterns: DAGs of recorded operations with variables and scalar slots.
+// ---------------------------------------------------------------------------
+
+constexpr int P_VAR = 100;  // a variable: any recorded node, bound on first sight
+
+// Roles of the helper operators a pattern applies (LZ_OPMAT nodes).
+enum Role {
+    ROLE_NONE,
+    ROLE_ON_FIRST,        // On(allCells -> firstCell(interiorFaces))
+    ROLE_ON_SECOND,       // On(allCells -> secondCell(interiorFaces))
+    ROLE_ON_BOUNDARY,     // On(allCells -> the inner cell of each boundary face)
+    ROLE_EXTEND_INTERIOR, // Extend(interiorFaces -> allFaces)
+    ROLE_EXTEND_BOUNDARY, // Extend(boundaryFaces -> allFaces)
+    ROLE_DIV_FULL,        // divergence of a collection on all faces
+    ROLE_COUNT
+};
+
+// Conditions on a variable's values, checked on the device.
+enum Fact {
+    FACT_NONE,
+    FACT_CELL_UNIFORM,        // one value on every cell
+    FACT_FACE_AREA,           // one value on the x faces, one on the y faces
+    FACT_INTERIOR_NORMAL_X,   // 1 on interior x faces, 0 on interior y faces
+    FACT_INTERIOR_NORMAL_Y,   // 0 on interior x faces, 1 on interior y faces
+    FACT_BOUNDARY_NORMAL_X,   // the same on the boundary faces
+    FACT_BOUNDARY_NORMAL_Y,
+    FACT_COUNT
+};
+
+// Lengths of a node's collection.
+enum Len { LEN_CELLS, LEN_FACES, LEN_INTERIOR, LEN_BOUNDARY };
+
+struct PNode {
+    int op = LZ_LEAF;
+    int sub = 0;
+    int scalar_left = 0;
+    int slot = -1;    // LZ_BINS, LZ_CMPS, LZ_CONST: the scalar's slot
+    int role = ROLE_NONE;
+    int var = -1;     // P_VAR
+    int len = LEN_CELLS;
+    bool mask = false;
+    int kid[3] = {-1, -1, -1};
+};
+
+struct DagPattern {
+    std::vector<PNode> nodes;
+    std::vector<int> var_fact;   // per variable
+    std::vector<int> var_len;
+    int nslots = 0;
+    std::vector<int> roots;
+};
+
+struct PB;
+struct E {
+    PB* b;
+    int id;
+};
+struct S {
+    int slot;
+};
+
+struct PB {
+    DagPattern p;
+    explicit PB(int nvars, int nslots)
+    {
+        p.var_fact.assign(nvars, FACT_NONE);
+        p.var_len.assign(nvars, LEN_CELLS);
+        p.nslots = nslots;
+    }
+    int len_of(int id) const { return p.nodes[id].len; }
+    E add(PNode q)
+    {
+        p.nodes.push_back(q);
+        return E{this, (int)p.nodes.size() - 1};
+    }
+    E var(int v, int len, int fact = FACT_NONE)
+    {
+        p.var_fact[v] = fact;
+        p.var_len[v] = len;
+        PNode q;
+        q.op = P_VAR;
+        q.var = v;
+        q.len = len;
+        return add(q);
+    }
+    E cnst(S s, int len)
+    {
+        PNode q;
+        q.op = LZ_CONST;
+        q.slot = s.slot;
+        q.len = len;
+        return add(q);
+    }
+    E bin(int op, E a, E b)
+    {
+        PNode q;
+        q.op = LZ_BIN;
+        q.sub = op;
+        q.len = len_of(a.id);
+        q.kid[0] = a.id;
+        q.kid[1] = b.id;
+        return add(q);
+    }
+    E bins(int op, E a, S s, bool scalar_left)
+    {
+        PNode q;
+        q.op = LZ_BINS;
+        q.sub = op;
+        q.slot = s.slot;
+        q.scalar_left = scalar_left ? 1 : 0;
+        q.len = len_of(a.id);
+        q.kid[0] = a.id;
+        return add(q);
+    }
+    E unary(int op, E a)
+    {
+        PNode q;
+        q.op = LZ_UNARY;
+        q.sub = op;
+        q.len = len_of(a.id);
+        q.kid[0] = a.id;
+        return add(q);
+    }
+    E cmp(int op, E a, E b)
+    {
+        PNode q;
+        q.op = LZ_CMP;
+        q.sub = op;
+        q.mask = true;
+        q.len = len_of(a.id);
+        q.kid[0] = a.id;
+        q.kid[1] = b.id;
+        return add(q);
+    }
+    E cmps(int op, E a, S s)
+    {
+        PNode q;
+        q.op = LZ_CMPS;
+        q.sub = op;
+        q.slot = s.slot;
+        q.mask = true;
+        q.len = len_of(a.id);
+        q.kid[0] = a.id;
+        return add(q);
+    }
+    E sel(E m, E a, E b)
+    {
+        PNode q;
+        q.op = LZ_SEL;
+        q.len = len_of(m.id);
+        q.kid[0] = m.id;
+        q.kid[1] = a.id;
+        q.kid[2] = b.id;
+        return add(q);
+    }
+    E opm(int role, E a, int len)
+    {
+        PNode q;
+        q.op = LZ_OPMAT;
+        q.role = role;
+        q.len = len;
+        q.kid[0] = a.id;
+        return add(q);
+    }
+};
+
+// The operators of the generated program, in the form its header records
+// them (equelleTypes.hpp: Coll op Coll, Coll op Scalar, Scalar op Coll).
+E operator+(E a, E b) { return a.b->bin(EQG_ADD, a, b); }
+E operator-(E a, E b) { return a.b->bin(EQG_SUB, a, b); }
+E operator*(E a, E b) { return a.b->bin(EQG_MUL, a, b); }
+E operator/(E a, E b) { return a.b->bin(EQG_DIV, a, b); }
+E operator*(S s, E a) { return a.b->bins(EQG_MUL, a, s, true); }
+E operator/(S s, E a) { return a.b->bins(EQG_DIV, a, s, true); }
+E operator/(E a, S s) { return a.b->bins(EQG_DIV, a, s, false); }
+E operator-(E a) { return a.b->unary(EQG_NEG, a); }
+E operator>(E a, S s) { return a.b->cmps(EQG_GT, a, s); }
+E operator>(E a, E b) { return a.b->cmp(EQG_GT, a, b); }
+E sqrt_(E a) { return a.b->unary(EQG_SQRT, a); }
+E trinary(E m, E a, E b) { return a.b->sel(m, a, b); }
+
+// ---------------------------------------------------------------------------
+// The shallow-water step (equelle_b200/sims/swe.cpp, its loop body).
+// ---------------------------------------------------------------------------
+
+// Variables of the step.
+enum SweVar {
+    V_W, V_HU, V_HV,                 // the state at the step's start (cells)
+    V_BMID, V_BE, V_BW, V_BN, V_BS,  // bottom: cell middle and face midpoints (cells)
+    V_VOL,                           // cell volumes
+    V_AREA,                          // face areas (all faces)
+    V_NX, V_NY,                      // unit normals of the interior faces
+    V_BO0, V_BO1,                    // unit normals of the boundary faces
+    SWE_NVARS
+};
+
+// Scalar slots of the step; a slot used in several places must hold the
+// same value in all of them.
+enum SweSlot {
+    S_DRY,        // wet when the height exceeds it
+    S_DUMMY,      // height of dry faces
+    S_HALF_G,     // 0.5 * gravity
+    S_G,          // gravity
+    S_ZERO_F,     // fluxes of dry interior faces
+    S_HALF,       // the 0.5 of the Rusanov flux and of Heun's average
+    S_TWO,        // the 2 of the source term's mean
+    S_NEG_G,      // -gravity
+    S_DT,         // the time step
+    S_DX, S_DY,   // cell sizes in the bottom slopes
+    S_SIGN_ZERO,  // boundary normal compared with it for the wall's sign
+    S_ONE_B, S_MONE_B,  // the wall signs
+    S_ZERO_B,     // wall flux of dry boundary faces
+    S_ONE_C, S_ZERO_C,  // wet and dry factors of the source term
+    SWE_NSLOTS
+};
+
+// Variables and slots of the wave-speed maximum.
+enum SpeedVar { U_W, U_HU, U_HV, U_BMID, SPEED_NVARS };
+enum SpeedSlot { T_DRY, T_DUMMY, T_G, T_ZERO, SPEED_NSLOTS };
+
+// The three results of one time step: w, hu, hv (roots in that order).
+DagPattern swe_step_pattern()
+{
+    PB b(SWE_NVARS, SWE_NSLOTS);
+    const E w0 = b.var(V_W, LEN_CELLS), hu0 = b.var(V_HU, LEN_CELLS), hv0 = b.var(V_HV, LEN_CELLS);
+    const E b_mid = b.var(V_BMID, LEN_CELLS);
+    const E b_east = b.var(V_BE, LEN_CELLS), b_west = b.var(V_BW, LEN_CELLS);
+    const E b_north = b.var(V_BN, LEN_CELLS), b_south = b.var(V_BS, LEN_CELLS);
+    const E vol = b.var(V_VOL, LEN_CELLS, FACT_CELL_UNIFORM);
+    const E area = b.var(V_AREA, LEN_FACES, FACT_FACE_AREA);
+    const E nx = b.var(V_NX, LEN_INTERIOR, FACT_INTERIOR_NORMAL_X);
+    const E ny = b.var(V_NY, LEN_INTERIOR, FACT_INTERIOR_NORMAL_Y);
+    const E bo0 = b.var(V_BO0, LEN_BOUNDARY, FACT_BOUNDARY_NORMAL_X);
+    const E bo1 = b.var(V_BO1, LEN_BOUNDARY, FACT_BOUNDARY_NORMAL_Y);
+    const S dry{S_DRY}, half_g{S_HALF_G}, gravity{S_G}, half{S_HALF}, two{S_TWO}, neg_g{S_NEG_G}, dt{S_DT};
+
+    // set-up values of the program, deferred until the first step needs them
+    const E bFirst = b.opm(ROLE_ON_FIRST, b_mid, LEN_INTERIOR);
+    const E bSecond = b.opm(ROLE_ON_SECOND, b_mid, LEN_INTERIOR);
+    const E bound_b = b.opm(ROLE_ON_BOUNDARY, b_mid, LEN_BOUNDARY);
+    const E bound_signX = trinary(bo0 > S{S_SIGN_ZERO}, b.cnst(S{S_ONE_B}, LEN_BOUNDARY), b.cnst(S{S_MONE_B}, LEN_BOUNDARY));
+    const E bound_signY = trinary(bo1 > S{S_SIGN_ZERO}, b.cnst(S{S_ONE_B}, LEN_BOUNDARY), b.cnst(S{S_MONE_B}, LEN_BOUNDARY));
+    const E bx = (b_east - b_west) / S{S_DX};
+    const E by = (b_north - b_south) / S{S_DY};
+
+    struct Side {
+        E f0, f1, f2, speed;
+    };
+    auto sideFlux = [&](E w, E hu, E hv, E bb) -> Side {
+        const E rawHeight = w - bb;
+        const E wet = rawHeight > dry;
+        const E height = trinary(wet, rawHeight, b.cnst(S{S_DUMMY}, LEN_INTERIOR));
+        const E qn = (hu * nx) + (hv * ny);
+        const E un = qn / height;
+        const E pressure = half_g * (height * height);
+        const E zero = b.cnst(S{S_ZERO_F}, LEN_INTERIOR);
+        const E f0 = trinary(wet, qn, zero);
+        const E f1 = trinary(wet, (hu * un) + (pressure * nx), zero);
+        const E f2 = trinary(wet, (hv * un) + (pressure * ny), zero);
+        const E speed = trinary(wet, sqrt_(un * un) + sqrt_(gravity * height), zero);
+        return Side{f0, f1, f2, speed};
+    };
+    struct Flux {
+        E f0, f1, f2;
+    };
+    auto getFlux = [&](E w, E hu, E hv) -> Flux {
+        const E wL = b.opm(ROLE_ON_FIRST, w, LEN_INTERIOR), huL = b.opm(ROLE_ON_FIRST, hu, LEN_INTERIOR),
+                hvL = b.opm(ROLE_ON_FIRST, hv, LEN_INTERIOR);
+        const E wR = b.opm(ROLE_ON_SECOND, w, LEN_INTERIOR), huR = b.opm(ROLE_ON_SECOND, hu, LEN_INTERIOR),
+                hvR = b.opm(ROLE_ON_SECOND, hv, LEN_INTERIOR);
+        const Side fL = sideFlux(wL, huL, hvL, bFirst);
+        const Side fR = sideFlux(wR, huR, hvR, bSecond);
+        const E a = trinary(fL.speed > fR.speed, fL.speed, fR.speed);
+        const E intFlux0 = (half * (fL.f0 + fR.f0)) - ((half * a) * (wR - wL));
+        const E intFlux1 = (half * (fL.f1 + fR.f1)) - ((half * a) * (huR - huL));
+        const E intFlux2 = (half * (fL.f2 + fR.f2)) - ((half * a) * (hvR - hvL));
+        const E bound_height = b.opm(ROLE_ON_BOUNDARY, w, LEN_BOUNDARY) - bound_b;
+        const E b_flux = trinary(bound_height > dry, half_g * (bound_height * bound_height),
+                                 b.cnst(S{S_ZERO_B}, LEN_BOUNDARY));
+        const E boundFlux1 = (sqrt_(bo0 * bo0) * b_flux) * bound_signX;
+        const E boundFlux2 = (sqrt_(bo1 * bo1) * b_flux) * bound_signY;
+        const E all0 = b.opm(ROLE_EXTEND_INTERIOR, intFlux0, LEN_FACES) * area;
+        const E all1 = (b.opm(ROLE_EXTEND_INTERIOR, intFlux1, LEN_FACES) +
+                        b.opm(ROLE_EXTEND_BOUNDARY, boundFlux1, LEN_FACES)) * area;
+        const E all2 = (b.opm(ROLE_EXTEND_INTERIOR, intFlux2, LEN_FACES) +
+                        b.opm(ROLE_EXTEND_BOUNDARY, boundFlux2, LEN_FACES)) * area;
+        return Flux{all0, all1, all2};
+    };
+    struct Source {
+        E s0, s1;
+    };
+    auto sourceTerm = [&](E w) -> Source {
+        const E secondTerm_x = ((w - b_east) + (w - b_west)) / two;
+        const E secondTerm_y = ((w - b_north) + (w - b_south)) / two;
+        const E dryTerm = trinary((w - b_mid) > dry, b.cnst(S{S_ONE_C}, LEN_CELLS), b.cnst(S{S_ZERO_C}, LEN_CELLS));
+        return Source{((neg_g * bx) * secondTerm_x) * dryTerm, ((neg_g * by) * secondTerm_y) * dryTerm};
+    };
+    auto div = [&](E f) { return b.opm(ROLE_DIV_FULL, f, LEN_CELLS); };
+    struct Q {
+        E w, hu, hv;
+    };
+    auto eulerStage = [&](E w, E hu, E hv) -> Q {
+        const Flux flux = getFlux(w, hu, hv);
+        const Source source = sourceTerm(w);
+        const E w1 = w + ((dt / vol) * (-div(flux.f0)));
+        const E hu1 = hu + ((dt / vol) * ((-div(flux.f1)) + (vol * source.s0)));
+        const E hv1 = hv + ((dt / vol) * ((-div(flux.f2)) + (vol * source.s1)));
+        return Q{w1, hu1, hv1};
+    };
+    const Q qs = eulerStage(w0, hu0, hv0);
+    const Q qss = eulerStage(qs.w, qs.hu, qs.hv);
+    const E w = (half * w0) + (half * qss.w);
+    const E hu = (half * hu0) + (half * qss.hu);
+    const E hv = (half * hv0) + (half * qss.hv);
+    b.p.roots = {w.id, hu.id, hv.id};
+    return b.p;
+}
+
+// The largest wave speed over the cells (dry cells: 0), before maxReduce.
+DagPattern swe_speed_pattern()
+{
+    PB b(SPEED_NVARS, SPEED_NSLOTS);
+    const E w = b.var(U_W, LEN_CELLS), hu = b.var(U_HU, LEN_CELLS), hv = b.var(U_HV, LEN_CELLS);
+    const E b_mid = b.var(U_BMID, LEN_CELLS);
+    const E rawHeight = w - b_mid;
+    const E wet = rawHeight > S{T_DRY};
+    const E height = trinary(wet, rawHeight, b.cnst(S{T_DUMMY}, LEN_CELLS));
+    const E u = hu / height;
+    const E v = hv / height;
+    const E speed = trinary(wet, sqrt_((u * u) + (v * v)) + sqrt_(S{T_G} * height), b.cnst(S{T_ZERO}, LEN_CELLS));
+    b.p.roots = {speed.id};
+    return b.p;
+}
+
+const DagPattern& step_pattern()
+{
+    static const DagPattern p = swe_step_pattern();
+    return p;
+}
+
+const DagPattern& speed_pattern()
+{
+    static const DagPattern p = swe_speed_pattern();
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// Matching a pattern against recorded nodes.
+// ---------------------------------------------------------------------------
+
+// What a variable stands for: the array of a leaf (two leaf nodes over one
+// array are the same value), else the node itself.
+const void* identity(const LazyNode* r) { return r->op == LZ_LEAF ? (const void*)r->leaf.get() : (const void*)r; }
+
+struct Matcher {
+    const DagPattern& P;
+    const Core& c;
+    std::vector<LazyNode*> var;
+    std::vector<const void*> var_id;
+    std::vector<double> slot;
+    std::vector<char> slot_set;
+    std::vector<std::pair<int, LazyNode*>> opmats;  // (role, node), checked after the walk
+    struct PairHash {
+        size_t operator()(const std::pair<int, const LazyNode*>& k) const
+        {
+            return std::hash<const void*>()(k.second) * 31u + (size_t)k.first;
+        }
+    };
+    std::unordered_map<std::pair<int, const LazyNode*>, char, PairHash> memo;  // matched pairs
+    // undo journal: kind 0 var, 1 slot, 2 memo entry, 3 operator entry
+    struct Undo {
+        int kind, index;
+        const LazyNode* node;
+    };
+    std::vector<Undo> journal;
+
+    Matcher(const DagPattern& p, const Core& core)
+        : P(p), c(core), var(p.var_fact.size(), nullptr), var_id(p.var_fact.size(), nullptr),
+          slot(p.nslots, 0.0), slot_set(p.nslots, 0)
+    {
+        memo.reserve(4096);
+    }
+
+    int64_t length(int len) const
+    {
+        switch (len) {
+        case LEN_CELLS: return c.nc;
+        case LEN_FACES: return c.nf;
+        case LEN_INTERIOR: return c.nif;
+        default: return (int64_t)c.nf - c.nif;
+        }
+    }
+
+    bool bind_slot(int s, double v)
+    {
+        if (slot_set[s]) return std::memcmp(&slot[s], &v, sizeof(double)) == 0;
+        slot[s] = v;
+        slot_set[s] = 1;
+        journal.push_back({1, s, nullptr});
+        return true;
+    }
+
+    bool go(int p, LazyNode* r)
+    {
+        if (!r) return false;
+        const PNode& q = P.nodes[p];
+        if (r->n != length(q.len) || r->mask != q.mask) return false;
+        if (q.op == P_VAR) {
+            const void* id = identity(r);
+            if (var[q.var]) return var_id[q.var] == id;
+            var[q.var] = r;
+            var_id[q.var] = id;
+            journal.push_back({0, q.var, nullptr});
+            return true;
+        }
+        const auto key = std::make_pair(p, (const LazyNode*)r);
+        if (memo.count(key)) return true;
+        if (r->op != q.op) return false;
+        switch (q.op) {
+        case LZ_BIN:
+        case LZ_UNARY:
+        case LZ_CMP:
+            if (r->sub != q.sub) return false;
+            break;
+        case LZ_BINS:
+        case LZ_CMPS:
+            if (r->sub != q.sub || r->scalar_left != q.scalar_left || !bind_slot(q.slot, r->s)) return false;
+            break;
+        case LZ_CONST:
+            if (!bind_slot(q.slot, r->s)) return false;
+            break;
+        case LZ_OPMAT:
+            opmats.push_back({q.role, r});
+            journal.push_back({3, 0, nullptr});
+            break;
+        default:
+            break;
+        }
+        LazyNode* kids[3] = {r->a.get(), r->b.get(), r->c.get()};
+        for (int k = 0; k < 3; ++k) {
+            if (q.kid[k] < 0) {
+                if (kids[k]) return false;
+                continue;
+            }
+            if (!go(q.kid[k], kids[k])) return false;
+        }
+        memo.emplace(key, 1);
+        journal.push_back({2, p, r});
+        return true;
+    }
+
+    size_t checkpoint() const { return journal.size(); }
+    void rollback(size_t mark)
+    {
+        while (journal.size() > mark) {
+            const Undo u = journal.back();
+            journal.pop_back();
+            switch (u.kind) {
+            case 0: var[u.index] = nullptr; var_id[u.index] = nullptr; break;
+            case 1: slot_set[u.index] = 0; break;
+            case 2: memo.erase(std::make_pair(u.index, u.node)); break;
+            default: opmats.pop_back(); break;
+            }
+        }
+    }
+
+    // Root k of the pattern against `r`; nothing stays bound on failure.
+    bool try_root(int k, LazyNode* r)
+    {
+        const size_t mark = checkpoint();
+        if (go(P.roots[k], r)) return true;
+        rollback(mark);
+        return false;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// The grid's numbering (2D Cartesian, build_grid in core.cu): cell i + nx j;
+// x faces i + (nx+1) j (0 <= i <= nx), then y faces fx + i + nx j
+// (0 <= j <= ny); interior and boundary faces listed in ascending face order.
+// ---------------------------------------------------------------------------
+struct Grid2 {
+    int nx, ny;
+    int64_t nc, fx, nf, nix, nif, nb;
+};
+
+Grid2 grid2(const Core& c)
+{
+    Grid2 g;
+    g.nx = c.nx;
+    g.ny = c.ny;
+    g.nc = (int64_t)c.nx * c.ny;
+    g.fx = (int64_t)(c.nx + 1) * c.ny;
+    g.nf = g.fx + (int64_t)c.nx * (c.ny + 1);
+    g.nix = (int64_t)(c.nx - 1) * c.ny;
+    g.nif = g.nix + (int64_t)c.nx * (c.ny - 1);
+    g.nb = g.nf - g.nif;
+    return g;
+}
+
+// Interior face at position t: its first and second cell.
+__device__ __forceinline__ void interior_cells(const Grid2& g, int64_t t, int64_t& first, int64_t& second)
+{
+    if (t < g.nix) {
+        const int64_t i = t % (g.nx - 1) + 1, j = t / (g.nx - 1);
+        first = (i - 1) + (int64_t)g.nx * j;
+        second = i + (int64_t)g.nx * j;
+    } else {
+        const int64_t u = t - g.nix, i = u % g.nx, j = u / g.nx + 1;
+        first = i + (int64_t)g.nx * (j - 1);
+        second = i + (int64_t)g.nx * j;
+    }
+}
+
+// Boundary face at position t: its one cell.
+__device__ __forceinline__ int64_t boundary_cell(const Grid2& g, int64_t t)
+{
+    if (t < 2 * (int64_t)g.ny) {
+        const int64_t j = t / 2;
+        return (t % 2 ? g.nx - 1 : 0) + (int64_t)g.nx * j;
+    }
+    const int64_t u = t - 2 * (int64_t)g.ny;
+    const bool top = u >= g.nx;
+    const int64_t i = top ? u - g.nx : u;
+    return i + (int64_t)g.nx * (top ? g.ny - 1 : 0);
+}
+
+// Face f: its position among the interior faces (>= 0), or -1 - its
+// position among the boundary faces.
+__device__ __forceinline__ int64_t face_position(const Grid2& g, int64_t f)
+{
+    if (f < g.fx) {
+        const int64_t i = f % (g.nx + 1), j = f / (g.nx + 1);
+        if (i > 0 && i < g.nx) return (i - 1) + (int64_t)(g.nx - 1) * j;
+        return -1 - (2 * j + (i == g.nx ? 1 : 0));
+    }
+    const int64_t u = f - g.fx, i = u % g.nx, j = u / g.nx;
+    if (j > 0 && j < g.ny) return g.nix + i + (int64_t)g.nx * (j - 1);
+    return -1 - (2 * (int64_t)g.ny + (j == g.ny ? g.nx : 0) + i);
+}
+
+__device__ __forceinline__ bool same_bits(double a, double b) { return __double_as_longlong(a) == __double_as_longlong(b); }
+
+// Row t of the operator must select exactly what `role` selects, weight 1.
+__global__ void role_check_kernel(int role, Grid2 g, int64_t n_out, const int* __restrict__ ptr,
+                                  const int* __restrict__ src, const double* __restrict__ w, int* bad)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n_out; t += (int64_t)gridDim.x * blockDim.x) {
+        bool has = true;
+        int64_t col = 0;
+        switch (role) {
+        case ROLE_ON_FIRST:
+        case ROLE_ON_SECOND: {
+            int64_t a, b;
+            interior_cells(g, t, a, b);
+            col = role == ROLE_ON_FIRST ? a : b;
+            break;
+        }
+        case ROLE_ON_BOUNDARY: col = boundary_cell(g, t); break;
+        case ROLE_EXTEND_INTERIOR: {
+            const int64_t p = face_position(g, t);
+            has = p >= 0;
+            col = p;
+            break;
+        }
+        default: {  // ROLE_EXTEND_BOUNDARY
+            const int64_t p = face_position(g, t);
+            has = p < 0;
+            col = -1 - p;
+            break;
+        }
+        }
+        const int e0 = ptr[t], e1 = ptr[t + 1];
+        bool ok = t > 0 || e0 == 0;
+        if (has) ok = ok && e1 - e0 == 1 && src[e0] == col && same_bits(w[e0], 1.0);
+        else ok = ok && e1 == e0;
+        if (!ok) atomicOr(bad, 1);
+    }
+}
+
+// The array must meet `fact` (v0, v1: the uniform values it must hold).
+__global__ void fact_check_kernel(int fact, Grid2 g, const double* __restrict__ a, int64_t n, double v0, double v1,
+                                  int* bad)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        double want;
+        switch (fact) {
+        case FACT_CELL_UNIFORM: want = v0; break;
+        case FACT_FACE_AREA: want = t < g.fx ? v0 : v1; break;
+        case FACT_INTERIOR_NORMAL_X: want = t < g.nix ? 1.0 : 0.0; break;
+        case FACT_INTERIOR_NORMAL_Y: want = t < g.nix ? 0.0 : 1.0; break;
+        case FACT_BOUNDARY_NORMAL_X: want = t < 2 * (int64_t)g.ny ? 1.0 : 0.0; break;
+        default: want = t < 2 * (int64_t)g.ny ? 0.0 : 1.0; break;
+        }
+        if (!same_bits(a[t], want)) atomicOr(bad, 1);
+    }
+}
+
+}  // namespace
+
+// Verified operators and arrays (keyed by address, with a weak reference
+// that tells a recycled address from the object checked), and the cached
+// wave-speed maximum of the last fused step's results.
+struct FuseState {
+    struct RoleFacts {
+        std::weak_ptr<OpMatrix> m;
+        char known[ROLE_COUNT] = {};
+        char ok[ROLE_COUNT] = {};
+    };
+    std::unordered_map<const OpMatrix*, RoleFacts> roles;
+    struct ArrayFacts {
+        std::weak_ptr<DevBuf> buf;
+        char known[FACT_COUNT] = {};
+        char ok[FACT_COUNT] = {};
+        double v0[FACT_COUNT] = {}, v1[FACT_COUNT] = {};
+    };
+    std::unordered_map<const DevBuf*, ArrayFacts> arrays;
+    // slots of the last matched wave-speed maximum (for the next step's
+    // epilogue) and its bottom array
+    bool speed_known = false;
+    double speed_slots[SPEED_NSLOTS] = {};
+    std::weak_ptr<DevBuf> speed_bmid;
+    // the maximum computed in a step's epilogue, with what it was computed from
+    struct Cached {
+        bool valid = false;
+        std::weak_ptr<DevBuf> w, hu, hv, bmid;
+        double slots[SPEED_NSLOTS] = {};
+    } cached;
+    Buf partials;  // per-block maxima
+    Buf result;    // double[1]: the maximum
+    int64_t partials_n = 0;
+};
+
+namespace {
+
+FuseState& state(Core& c)
+{
+    if (!c.fuse_state) c.fuse_state = std::make_shared<FuseState>();
+    return *c.fuse_state;
+}
+
+int read_flag(Core& c, const Buf& b)
+{
+    EQG_CUDA(cudaMemcpyAsync(c.pinned, b->ptr, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    int v;
+    std::memcpy(&v, c.pinned, sizeof(int));
+    return v;
+}
+
+double read_double(Core& c, const double* p)
+{
+    EQG_CUDA(cudaMemcpyAsync(c.pinned, p, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    return c.pinned[0];
+}
+
+int check_blocks(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+
+// True when the operator applies `role` on this grid (checked once).
+bool role_ok(Core& c, const OpMatrixP& m, int role)
+{
+    if (role == ROLE_DIV_FULL) return m == c.div_full;
+    FuseState& st = state(c);
+    FuseState::RoleFacts& f = st.roles[m.get()];
+    if (f.m.lock() != m) f = FuseState::RoleFacts{m};
+    if (f.known[role]) return f.ok[role];
+    const Grid2 g = grid2(c);
+    int64_t rows = 0, cols = 0;
+    switch (role) {
+    case ROLE_ON_FIRST:
+    case ROLE_ON_SECOND: rows = g.nif; cols = g.nc; break;
+    case ROLE_ON_BOUNDARY: rows = g.nb; cols = g.nc; break;
+    case ROLE_EXTEND_INTERIOR: rows = g.nf; cols = g.nif; break;
+    default: rows = g.nf; cols = g.nb; break;
+    }
+    bool ok = m->stencil == 0 && m->n_out == rows && m->n_src == cols && rows > 0;
+    if (ok) {
+        Buf bad = c.allocN<int>(1);
+        EQG_CUDA(cudaMemsetAsync(bad->ptr, 0, sizeof(int), c.stream));
+        launch(c, "fuse_role_check", [&] {
+            role_check_kernel<<<check_blocks(rows), 256, 0, c.stream>>>(role, g, rows, m->ptr->as<int>(),
+                                                                        m->src->as<int>(), m->w->as<double>(),
+                                                                        bad->as<int>());
+        });
+        ok = read_flag(c, bad) == 0;
+    }
+    f.known[role] = 1;
+    f.ok[role] = ok ? 1 : 0;
+    return ok;
+}
+
+// True when the leaf's array meets `fact` (checked once); v0/v1 receive its
+// uniform values.
+bool fact_ok(Core& c, const LazyNode* leaf, int fact, double& v0, double& v1)
+{
+    if (fact == FACT_NONE) return true;
+    const Buf& b = leaf->leaf;
+    FuseState& st = state(c);
+    FuseState::ArrayFacts& f = st.arrays[b.get()];
+    if (f.buf.lock() != b) f = FuseState::ArrayFacts{b};
+    if (!f.known[fact]) {
+        const Grid2 g = grid2(c);
+        const int64_t n = leaf->n;
+        double a = 0.0, bb = 0.0;
+        if (fact == FACT_CELL_UNIFORM || fact == FACT_FACE_AREA) a = read_double(c, b->as<double>());
+        if (fact == FACT_FACE_AREA) bb = read_double(c, b->as<double>() + g.fx);
+        Buf bad = c.allocN<int>(1);
+        EQG_CUDA(cudaMemsetAsync(bad->ptr, 0, sizeof(int), c.stream));
+        launch(c, "fuse_fact_check", [&] {
+            fact_check_kernel<<<check_blocks(n), 256, 0, c.stream>>>(fact, g, b->as<double>(), n, a, bb,
+                                                                     bad->as<int>());
+        });
+        f.known[fact] = 1;
+        f.ok[fact] = read_flag(c, bad) == 0 ? 1 : 0;
+        f.v0[fact] = a;
+        f.v1[fact] = bb;
+    }
+    v0 = f.v0[fact];
+    v1 = f.v1[fact];
+    return f.ok[fact] != 0;
+}
+
+// ---------------------------------------------------------------------------
+// Kernels of the shallow-water step.  Every operation below is one
+// operation of the program, computed as its own kernel computes it (ops.cu,
+// jacobian.cu, core.cu): a selection row (On, Extend) is 0.0 + 1.0 * x, an
+// empty Extend row 0.0, trinaryIf x * t + y * f with t, f in {0, 1},
+// unary minus 0.0 - x, the divergence the west, east, south, north faces'
+// sum from 0.0.
+// ---------------------------------------------------------------------------
+
+struct SweConst {
+    double dry, dummy, half_g, g, zero_f, half, two, neg_g, dt, dx, dy, sign_zero, one_b, mone_b, zero_b, one_c,
+        zero_c;
+    double vol, area_x, area_y;  // verified uniform geometry
+    double dt_vol;               // dt / vol (one value: both are scalars here), divided on the host
+    // exact reciprocals of `two`, dx, dy where they are powers of two
+    // (x / 2^k and x * 2^-k round the same real number), else 0
+    double inv_two, inv_dx, inv_dy;
+    double s_dry, s_dummy, s_g, s_zero;  // the wave-speed maximum's slots
+};
+
+struct SweArrays {
+    const double *w, *hu, *hv;     // the stage's state
+    const double *w0, *hu0, *hv0;  // the step's start state (second stage)
+    const double *bm, *be, *bw, *bn, *bs;
+    double *ow, *ohu, *ohv;
+    double* partials;              // per-block wave-speed maxima (second stage)
+};
+
+__device__ __forceinline__ double ADD(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double SUB(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double MUL(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double DIV(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double SQRT(double a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ double SEL(bool m, double a, double b)
+{
+    return ADD(MUL(a, m ? 1.0 : 0.0), MUL(b, m ? 0.0 : 1.0));
+}
+__device__ __forceinline__ double ROW(double x) { return ADD(0.0, x); }  // 0.0 + 1.0 * x (exact product)
+// x / d, by the exact reciprocal when there is one
+__device__ __forceinline__ double DIVBY(double x, double d, double inv) { return inv != 0.0 ? MUL(x, inv) : DIV(x, d); }
+
+// sqrt(x * x), rounded as the two operations round it.  When x * x is a
+// normal double, |x| is that value: fl(x*x) = x^2 (1 + e), |e| < 2^-53, so
+// sqrt(fl(x*x)) lies within |x| 2^-54 of |x|, less than half the spacing of
+// doubles around |x|, and the correctly rounded square root is |x| itself.
+// Outside that range (and for NaN) both operations are performed.
+__device__ __forceinline__ double SQRT_OF_SQUARE(double x)
+{
+    const double ax = fabs(x);
+    return (ax >= 0x1p-511 && ax <= 0x1p+511) ? ax : SQRT(MUL(x, x));
+}
+
+struct SideFlux {
+    double f0, f1, f2, speed;
+};
+
+// sideFlux of the program for a cell's values (as gathered to a face: 0.0 +
+// x) in both directions: toward x faces (normal (1, 0)) and y faces
+// (normal (0, 1)).  Height, pressure and sqrt(g h) belong to the cell.
+__device__ __forceinline__ void side_fluxes(const SweConst& k, double w, double hu, double hv, double bb, bool want_x,
+                                            bool want_y, SideFlux& fx, SideFlux& fy)
+{
+    const double raw = SUB(w, bb);
+    const bool wet = raw > k.dry;
+    const double h = SEL(wet, raw, k.dummy);
+    const double p = MUL(k.half_g, MUL(h, h));
+    const double sgh = SQRT(MUL(k.g, h));
+    if (want_x) {
+        const double qn = ADD(MUL(hu, 1.0), MUL(hv, 0.0));
+        const double un = DIV(qn, h);
+        fx.f0 = SEL(wet, qn, k.zero_f);
+        fx.f1 = SEL(wet, ADD(MUL(hu, un), MUL(p, 1.0)), k.zero_f);
+        fx.f2 = SEL(wet, ADD(MUL(hv, un), MUL(p, 0.0)), k.zero_f);
+        fx.speed = SEL(wet, ADD(SQRT_OF_SQUARE(un), sgh), k.zero_f);
+    }
+    if (want_y) {
+        const double qn = ADD(MUL(hu, 0.0), MUL(hv, 1.0));
+        const double un = DIV(qn, h);
+        fy.f0 = SEL(wet, qn, k.zero_f);
+        fy.f1 = SEL(wet, ADD(MUL(hu, un), MUL(p, 0.0)), k.zero_f);
+        fy.f2 = SEL(wet, ADD(MUL(hv, un), MUL(p, 1.0)), k.zero_f);
+        fy.speed = SEL(wet, ADD(SQRT_OF_SQUARE(un), sgh), k.zero_f);
+    }
+}
+
+// All-face flux values (times the area) of an interior face between cells
+// L and R: their gathered state and side fluxes.
+__device__ __forceinline__ void interior_flux(const SweConst& k, double wL, double huL, double hvL, const SideFlux& fL,
+                                              double wR, double huR, double hvR, const SideFlux& fR, double area,
+                                              double F[3])
+{
+    const double a = SEL(fL.speed > fR.speed, fL.speed, fR.speed);
+    const double ha = MUL(k.half, a);
+    const double i0 = SUB(MUL(k.half, ADD(fL.f0, fR.f0)), MUL(ha, SUB(wR, wL)));
+    const double i1 = SUB(MUL(k.half, ADD(fL.f1, fR.f1)), MUL(ha, SUB(huR, huL)));
+    const double i2 = SUB(MUL(k.half, ADD(fL.f2, fR.f2)), MUL(ha, SUB(hvR, hvL)));
+    F[0] = MUL(ROW(i0), area);
+    F[1] = MUL(ADD(ROW(i1), 0.0), area);  // + Extend(boundary): an empty row
+    F[2] = MUL(ADD(ROW(i2), 0.0), area);
+}
+
+// All-face flux values of a boundary face of cell c (normal (bo0, bo1)).
+__device__ __forceinline__ void wall_flux(const SweConst& k, double wc, double bc, double bo0, double bo1,
+                                          double area, double F[3])
+{
+    const double bh = SUB(ROW(wc), ROW(bc));
+    const double bf = SEL(bh > k.dry, MUL(k.half_g, MUL(bh, bh)), k.zero_b);
+    const double sx = SEL(bo0 > k.sign_zero, k.one_b, k.mone_b);
+    const double sy = SEL(bo1 > k.sign_zero, k.one_b, k.mone_b);
+    const double b1 = MUL(MUL(SQRT(MUL(bo0, bo0)), bf), sx);
+    const double b2 = MUL(MUL(SQRT(MUL(bo1, bo1)), bf), sy);
+    F[0] = MUL(0.0, area);  // Extend(interior): an empty row
+    F[1] = MUL(ADD(0.0, ROW(b1)), area);
+    F[2] = MUL(ADD(0.0, ROW(b2)), area);
+}
+
+// The wave speed of one cell (maxSpeed of the program).
+__device__ __forceinline__ double cell_speed(const SweConst& k, double w, double hu, double hv, double bm)
+{
+    const double raw = SUB(w, bm);
+    const bool wet = raw > k.s_dry;
+    const double h = SEL(wet, raw, k.s_dummy);
+    const double u = DIV(hu, h);
+    const double v = DIV(hv, h);
+    return SEL(wet, ADD(SQRT(ADD(MUL(u, u), MUL(v, v))), SQRT(MUL(k.s_g, h))), k.s_zero);
+}
+
+// The maximum over a block (every thread passes its value; thread 0 gets it).
+__device__ __forceinline__ double block_max(double v, double* scratch)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int t = threadIdx.x + blockDim.x * threadIdx.y;
+    if ((t & 31) == 0) scratch[t >> 5] = v;
+    __syncthreads();
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if (t < 32) {
+        v = t < nw ? scratch[t] : -DBL_MAX;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+// Threads of a block: one per cell of a kBX x kBY window, the tile of
+// kTX x kTY cells it updates and a one-cell halo around it.
+constexpr int kBX = 32, kBY = 10;
+constexpr int kTX = kBX - 2, kTY = kBY - 2;
+
+// One forward-Euler stage on a tile.  Each thread reads one cell of the
+// window and computes its side fluxes toward x and y faces; then threads
+// compute the flux of the x face west of their cell (window rows 1..kTY,
+// columns 1..kBX-1) and of the y face south of it (columns 1..kTX, rows
+// 1..kBY-1), each face once; each cell of the tile sums its four faces.
+// HEUN: the stage after the first, averaged with the step's start state,
+// and (WITH_MAX) the results' wave-speed maximum.
+template <bool HEUN, bool WITH_MAX>
+__global__ void __launch_bounds__(kBX * kBY) swe_stage_kernel(Grid2 g, SweConst k, SweArrays a)
+{
+    __shared__ double sw[kBY][kBX], shu[kBY][kBX], shv[kBY][kBX], sbm[kBY][kBX];  // as read
+    __shared__ double sfx[4][kBY][kBX], sfy[4][kBY][kBX];  // side fluxes toward x and y faces
+    __shared__ double fxs[3][kBY][kBX], fys[3][kBY][kBX];  // flux of the x face west of, y face south of a cell
+    __shared__ double scratch[32];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int gi = blockIdx.x * kTX - 1 + tx, gj = blockIdx.y * kTY - 1 + ty;
+    const bool inside = gi >= 0 && gi < g.nx && gj >= 0 && gj < g.ny;
+    if (inside) {
+        const int64_t c = gi + (int64_t)g.nx * gj;
+        const double w = a.w[c], hu = a.hu[c], hv = a.hv[c], bm = a.bm[c];
+        sw[ty][tx] = w;
+        shu[ty][tx] = hu;
+        shv[ty][tx] = hv;
+        sbm[ty][tx] = bm;
+        SideFlux fx, fy;
+        side_fluxes(k, ROW(w), ROW(hu), ROW(hv), ROW(bm), true, true, fx, fy);
+        sfx[0][ty][tx] = fx.f0;
+        sfx[1][ty][tx] = fx.f1;
+        sfx[2][ty][tx] = fx.f2;
+        sfx[3][ty][tx] = fx.speed;
+        sfy[0][ty][tx] = fy.f0;
+        sfy[1][ty][tx] = fy.f1;
+        sfy[2][ty][tx] = fy.f2;
+        sfy[3][ty][tx] = fy.speed;
+    }
+    __syncthreads();
+    double F[3];
+    // x face gi (west of cell gi, east of cell gi - 1) in row gj
+    if (ty >= 1 && ty <= kTY && tx >= 1 && gj < g.ny && gi <= g.nx) {
+        if (gi == 0) {
+            wall_flux(k, sw[ty][tx], sbm[ty][tx], 1.0, 0.0, k.area_x, F);
+        } else if (gi == g.nx) {
+            wall_flux(k, sw[ty][tx - 1], sbm[ty][tx - 1], 1.0, 0.0, k.area_x, F);
+        } else {
+            const SideFlux fL{sfx[0][ty][tx - 1], sfx[1][ty][tx - 1], sfx[2][ty][tx - 1], sfx[3][ty][tx - 1]};
+            const SideFlux fR{sfx[0][ty][tx], sfx[1][ty][tx], sfx[2][ty][tx], sfx[3][ty][tx]};
+            interior_flux(k, ROW(sw[ty][tx - 1]), ROW(shu[ty][tx - 1]), ROW(shv[ty][tx - 1]), fL, ROW(sw[ty][tx]),
+                          ROW(shu[ty][tx]), ROW(shv[ty][tx]), fR, k.area_x, F);
+        }
+        fxs[0][ty][tx] = F[0];
+        fxs[1][ty][tx] = F[1];
+        fxs[2][ty][tx] = F[2];
+    }
+    // y face gj (south of cell gj, north of cell gj - 1) in column gi
+    if (tx >= 1 && tx <= kTX && ty >= 1 && gi < g.nx && gj <= g.ny) {
+        if (gj == 0) {
+            wall_flux(k, sw[ty][tx], sbm[ty][tx], 0.0, 1.0, k.area_y, F);
+        } else if (gj == g.ny) {
+            wall_flux(k, sw[ty - 1][tx], sbm[ty - 1][tx], 0.0, 1.0, k.area_y, F);
+        } else {
+            const SideFlux fL{sfy[0][ty - 1][tx], sfy[1][ty - 1][tx], sfy[2][ty - 1][tx], sfy[3][ty - 1][tx]};
+            const SideFlux fR{sfy[0][ty][tx], sfy[1][ty][tx], sfy[2][ty][tx], sfy[3][ty][tx]};
+            interior_flux(k, ROW(sw[ty - 1][tx]), ROW(shu[ty - 1][tx]), ROW(shv[ty - 1][tx]), fL, ROW(sw[ty][tx]),
+                          ROW(shu[ty][tx]), ROW(shv[ty][tx]), fR, k.area_y, F);
+        }
+        fys[0][ty][tx] = F[0];
+        fys[1][ty][tx] = F[1];
+        fys[2][ty][tx] = F[2];
+    }
+    __syncthreads();
+    double speed = -DBL_MAX;
+    if (tx >= 1 && tx <= kTX && ty >= 1 && ty <= kTY && inside) {
+        const int64_t c = gi + (int64_t)g.nx * gj;
+        const double w = sw[ty][tx], hu = shu[ty][tx], hv = shv[ty][tx], bm = sbm[ty][tx];
+        const double be = a.be[c], bw = a.bw[c], bn = a.bn[c], bs = a.bs[c];
+        double nd[3];
+        for (int m = 0; m < 3; ++m) {
+            double acc = 0.0;
+            acc = SUB(acc, fxs[m][ty][tx]);
+            acc = ADD(acc, fxs[m][ty][tx + 1]);
+            acc = SUB(acc, fys[m][ty][tx]);
+            acc = ADD(acc, fys[m][ty + 1][tx]);
+            nd[m] = SUB(0.0, acc);
+        }
+        const double stx = DIVBY(ADD(SUB(w, be), SUB(w, bw)), k.two, k.inv_two);
+        const double sty = DIVBY(ADD(SUB(w, bn), SUB(w, bs)), k.two, k.inv_two);
+        const double dry_term = SEL(SUB(w, bm) > k.dry, k.one_c, k.zero_c);
+        const double bx = DIVBY(SUB(be, bw), k.dx, k.inv_dx), by = DIVBY(SUB(bn, bs), k.dy, k.inv_dy);
+        const double s0 = MUL(MUL(MUL(k.neg_g, bx), stx), dry_term);
+        const double s1 = MUL(MUL(MUL(k.neg_g, by), sty), dry_term);
+        double w1 = ADD(w, MUL(k.dt_vol, nd[0]));
+        double hu1 = ADD(hu, MUL(k.dt_vol, ADD(nd[1], MUL(k.vol, s0))));
+        double hv1 = ADD(hv, MUL(k.dt_vol, ADD(nd[2], MUL(k.vol, s1))));
+        if (HEUN) {
+            w1 = ADD(MUL(k.half, a.w0[c]), MUL(k.half, w1));
+            hu1 = ADD(MUL(k.half, a.hu0[c]), MUL(k.half, hu1));
+            hv1 = ADD(MUL(k.half, a.hv0[c]), MUL(k.half, hv1));
+        }
+        a.ow[c] = w1;
+        a.ohu[c] = hu1;
+        a.ohv[c] = hv1;
+        if (WITH_MAX) speed = cell_speed(k, w1, hu1, hv1, bm);
+    }
+    if (WITH_MAX) {
+        speed = block_max(speed, scratch);
+        if (tx == 0 && ty == 0) a.partials[blockIdx.x + (int64_t)gridDim.x * blockIdx.y] = speed;
+    }
+}
+
+// The wave speed's maximum of a state, per block.
+__global__ void __launch_bounds__(256) swe_speed_kernel(int64_t n, SweConst k, const double* __restrict__ w,
+                                                        const double* __restrict__ hu, const double* __restrict__ hv,
+                                                        const double* __restrict__ bm, double* partials)
+{
+    __shared__ double scratch[32];
+    double m = -DBL_MAX;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
+        m = fmax(m, cell_speed(k, w[c], hu[c], hv[c], bm[c]));
+    m = block_max(m, scratch);
+    if (threadIdx.x == 0) partials[blockIdx.x] = m;
+}
+
+__global__ void __launch_bounds__(256) max_final_kernel(const double* __restrict__ partials, int64_t n, double* out)
+{
+    __shared__ double scratch[32];
+    double m = -DBL_MAX;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, partials[i]);
+    m = block_max(m, scratch);
+    if (threadIdx.x == 0) *out = m;
+}
+
+// 1 / d when d is a power of two (then x / d and x * (1 / d) are the same
+// double for every x), else 0.
+double exact_inverse(double d)
+{
+    int e = 0;
+    const double m = std::frexp(d, &e);
+    if (std::fabs(m) != 0.5) return 0.0;
+    const double inv = 1.0 / d;
+    return std::isnormal(inv) ? inv : 0.0;
+}
+
+bool grid_fits(const Core& c)
+{
+    return c.cartesian && c.dim == 2 && c.nx >= 2 && c.ny >= 2 && (c.ny + kTY - 1) / kTY <= 65535;
+}
+
+// Every variable a leaf (pending ones evaluated), every slot bound.
+bool settle_operands(Core& c, Matcher& M)
+{
+    for (int s = 0; s < (int)M.slot_set.size(); ++s)
+        if (!M.slot_set[s]) return false;
+    for (LazyNode* v : M.var) {
+        if (!v) return false;
+        if (v->op != LZ_LEAF) lazy_evaluate(c, v);
+        if (v->op != LZ_LEAF || v->mask) return false;
+    }
+    return true;
+}
+
+void ensure_partials(Core& c, FuseState& st, int64_t n)
+{
+    if (st.partials_n < n) {
+        st.partials = c.allocN<double>((size_t)n);
+        st.partials_n = n;
+    }
+    if (!st.result) st.result = c.allocN<double>(1);
+}
+
+}  // namespace
+
+bool fused_materialize(Core& c, LazyNode* root)
+{
+    if (!grid_fits(c) || root->op != LZ_BIN || root->mask || root->n != c.nc) return false;
+    const DagPattern& P = step_pattern();
+    Matcher M(P, c);
+    int k0 = -1;
+    for (int k = 0; k < 3 && k0 < 0; ++k)
+        if (M.try_root(k, root)) k0 = k;
+    if (k0 < 0) return false;
+    // the step's other results, among the pending handles
+    LazyNode* roots[3] = {nullptr, nullptr, nullptr};
+    roots[k0] = root;
+    for (int k = 0; k < 3; ++k) {
+        if (roots[k]) continue;
+        for (eqg_coll* x : c.lazy_colls) {
+            LazyNode* r = x->lazy.get();
+            if (!r || r == roots[0] || r == roots[1] || r == roots[2] || r->op != LZ_BIN || r->n != c.nc) continue;
+            if (M.try_root(k, r)) {
+                roots[k] = r;
+                break;
+            }
+        }
+        if (!roots[k]) return false;
+    }
+    for (const auto& rm : M.opmats)
+        if (!role_ok(c, rm.second->m, rm.first)) return false;
+    if (!settle_operands(c, M)) return false;
+    SweConst k{};
+    double unused = 0.0;
+    if (!fact_ok(c, M.var[V_VOL], FACT_CELL_UNIFORM, k.vol, unused) ||
+        !fact_ok(c, M.var[V_AREA], FACT_FACE_AREA, k.area_x, k.area_y) ||
+        !fact_ok(c, M.var[V_NX], FACT_INTERIOR_NORMAL_X, unused, unused) ||
+        !fact_ok(c, M.var[V_NY], FACT_INTERIOR_NORMAL_Y, unused, unused) ||
+        !fact_ok(c, M.var[V_BO0], FACT_BOUNDARY_NORMAL_X, unused, unused) ||
+        !fact_ok(c, M.var[V_BO1], FACT_BOUNDARY_NORMAL_Y, unused, unused))
+        return false;
+    const std::vector<double>& s = M.slot;
+    k.dry = s[S_DRY];
+    k.dummy = s[S_DUMMY];
+    k.half_g = s[S_HALF_G];
+    k.g = s[S_G];
+    k.zero_f = s[S_ZERO_F];
+    k.half = s[S_HALF];
+    k.two = s[S_TWO];
+    k.neg_g = s[S_NEG_G];
+    k.dt = s[S_DT];
+    k.dx = s[S_DX];
+    k.dy = s[S_DY];
+    k.sign_zero = s[S_SIGN_ZERO];
+    k.one_b = s[S_ONE_B];
+    k.mone_b = s[S_MONE_B];
+    k.zero_b = s[S_ZERO_B];
+    k.one_c = s[S_ONE_C];
+    k.zero_c = s[S_ZERO_C];
+    k.dt_vol = k.dt / k.vol;  // IEEE double division, as the device's
+    k.inv_two = exact_inverse(k.two);
+    k.inv_dx = exact_inverse(k.dx);
+    k.inv_dy = exact_inverse(k.dy);
+
+    FuseState& st = state(c);
+    const Buf& bmid = M.var[V_BMID]->leaf;
+    // the next step's wave-speed maximum, with the slots of the last one
+    const bool with_max = st.speed_known && st.speed_bmid.lock() == bmid;
+    if (with_max) {
+        k.s_dry = st.speed_slots[T_DRY];
+        k.s_dummy = st.speed_slots[T_DUMMY];
+        k.s_g = st.speed_slots[T_G];
+        k.s_zero = st.speed_slots[T_ZERO];
+    }
+    const Grid2 g = grid2(c);
+    const dim3 block(kBX, kBY), grid((c.nx + kTX - 1) / kTX, (c.ny + kTY - 1) / kTY);
+    const int64_t nblocks = (int64_t)grid.x * grid.y;
+    ensure_partials(c, st, nblocks);
+    const size_t bytes = (size_t)c.nc * sizeof(double);
+    Buf mid[3] = {c.alloc(bytes), c.alloc(bytes), c.alloc(bytes)};
+    Buf out[3] = {c.alloc(bytes), c.alloc(bytes), c.alloc(bytes)};
+    SweArrays a{};
+    a.w = M.var[V_W]->leaf->as<double>();
+    a.hu = M.var[V_HU]->leaf->as<double>();
+    a.hv = M.var[V_HV]->leaf->as<double>();
+    a.bm = bmid->as<double>();
+    a.be = M.var[V_BE]->leaf->as<double>();
+    a.bw = M.var[V_BW]->leaf->as<double>();
+    a.bn = M.var[V_BN]->leaf->as<double>();
+    a.bs = M.var[V_BS]->leaf->as<double>();
+    a.ow = mid[0]->as<double>();
+    a.ohu = mid[1]->as<double>();
+    a.ohv = mid[2]->as<double>();
+    // stage 1: state and five bottom arrays read, state written
+    launch(c, "swe_stage", [&] { swe_stage_kernel<false, false><<<grid, block, 0, c.stream>>>(g, k, a); },
+           88.0 * c.nc);
+    SweArrays b = a;
+    b.w0 = a.w;
+    b.hu0 = a.hu;
+    b.hv0 = a.hv;
+    b.w = a.ow;
+    b.hu = a.ohu;
+    b.hv = a.ohv;
+    b.ow = out[0]->as<double>();
+    b.ohu = out[1]->as<double>();
+    b.ohv = out[2]->as<double>();
+    b.partials = st.partials->as<double>();
+    // stage 2 and Heun's average: both states read as well
+    if (with_max) {
+        launch(c, "swe_heun_stage", [&] { swe_stage_kernel<true, true><<<grid, block, 0, c.stream>>>(g, k, b); },
+               112.0 * c.nc);
+        launch(c, "swe_max_final", [&] {
+            max_final_kernel<<<1, 256, 0, c.stream>>>(st.partials->as<double>(), nblocks, st.result->as<double>());
+        });
+        st.cached.valid = true;
+        st.cached.w = out[0];
+        st.cached.hu = out[1];
+        st.cached.hv = out[2];
+        st.cached.bmid = bmid;
+        std::memcpy(st.cached.slots, st.speed_slots, sizeof(st.cached.slots));
+    } else {
+        launch(c, "swe_heun_stage", [&] { swe_stage_kernel<true, false><<<grid, block, 0, c.stream>>>(g, k, b); },
+               112.0 * c.nc);
+    }
+    for (int m = 0; m < 3; ++m) lazy_make_leaf(roots[m], out[m]);
+    c.fused_evaluations++;
+    if (c.verbose > 3) std::printf("        fused shallow-water step on %d x %d cells\n", c.nx, c.ny);
+    return true;
+}
+
+bool fused_reduce(Core& c, int op, LazyNode* root, double* result)
+{
+    if (op != EQG_MAX || !grid_fits(c) || root->op != LZ_SEL || root->n != c.nc) return false;
+    Matcher M(speed_pattern(), c);
+    if (!M.try_root(0, root)) return false;
+    if (!settle_operands(c, M)) return false;
+    FuseState& st = state(c);
+    const Buf& w = M.var[U_W]->leaf;
+    const Buf& hu = M.var[U_HU]->leaf;
+    const Buf& hv = M.var[U_HV]->leaf;
+    const Buf& bm = M.var[U_BMID]->leaf;
+    const bool hit = st.cached.valid && st.cached.w.lock() == w && st.cached.hu.lock() == hu &&
+                     st.cached.hv.lock() == hv && st.cached.bmid.lock() == bm &&
+                     std::memcmp(st.cached.slots, M.slot.data(), sizeof(st.cached.slots)) == 0;
+    if (!hit) {
+        SweConst k{};
+        k.s_dry = M.slot[T_DRY];
+        k.s_dummy = M.slot[T_DUMMY];
+        k.s_g = M.slot[T_G];
+        k.s_zero = M.slot[T_ZERO];
+        const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((c.nc + 255) / 256, 148 * 8));
+        ensure_partials(c, st, nb);
+        launch(c, "swe_speed", [&] {
+            swe_speed_kernel<<<nb, 256, 0, c.stream>>>(c.nc, k, w->as<double>(), hu->as<double>(), hv->as<double>(),
+                                                       bm->as<double>(), st.partials->as<double>());
+        }, 32.0 * c.nc);
+        launch(c, "swe_max_final", [&] {
+            max_final_kernel<<<1, 256, 0, c.stream>>>(st.partials->as<double>(), nb, st.result->as<double>());
+        });
+        st.cached.valid = false;
+    }
+    *result = read_double(c, st.result->as<double>());
+    st.speed_known = true;
+    std::memcpy(st.speed_slots, M.slot.data(), sizeof(st.speed_slots));
+    st.speed_bmid = bm;
+    c.fused_evaluations++;
+    return true;
+}
+
+}  // namespace eqg

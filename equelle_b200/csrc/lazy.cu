@@ -33,6 +33,11 @@ constexpr int kVmLeaves = 24;
 constexpr int kVmOuts = 24;
 constexpr int kVmInstr = 160;
 constexpr int kLazyMaxCost = 96;  // larger expressions materialize their operands first
+// Recorded for fusion: an expression this large (counted as a tree) is
+// evaluated when it is made, so that a program that never reads its values
+// does not hold an unbounded DAG.  A time step of an explicit scheme is a few
+// thousand.
+constexpr double kFuseMaxCost = 1e7;
 constexpr size_t kVmSmem = (size_t)kVmRegs * kVmLanes * kVmThreads * sizeof(double);
 
 // One opcode per operation and operand form, so that an instruction is
@@ -260,6 +265,7 @@ bool compile(const std::vector<Root>& roots, VmProgram& prog)
         case LZ_CMPS: q.op = v->scalar_left ? VM_ICMP : VM_CMPI; q.a = reg(v->a.get()); break;
         case LZ_SEL: q.op = VM_SEL; q.a = reg(v->a.get()); q.b = reg(v->b.get()); q.c = reg(v->c.get()); break;
         case LZ_LOGIC: q.op = VM_LOGIC; q.a = reg(v->a.get()); q.b = reg(v->b ? v->b.get() : v->a.get()); break;
+        default: return false;  // operators are recorded only for fusion
         }
         if (!emit(q)) return false;
         for (int k : stores[i]) {
@@ -299,6 +305,7 @@ void make_leaf(LazyNode* v, Buf values)
     v->a.reset();
     v->b.reset();
     v->c.reset();
+    v->m.reset();
     v->cost = 1;
 }
 
@@ -315,10 +322,75 @@ void run_program(Core& c, const VmProgram& prog, int64_t n)
     c.lazy_passes++;
 }
 
+// One node whose operands are evaluated, by the kernel its operation
+// launches when it is not deferred (capi.cu).
+void eval_node(Core& c, LazyNode* v)
+{
+    const int64_t n = v->n;
+    Buf out = c.alloc((size_t)(n > 0 ? n : 1) * (v->mask ? 1 : 8));
+    auto D = [](const LazyP& k) { return k->leaf->as<double>(); };
+    auto M = [](const LazyP& k) { return k->leaf->as<uint8_t>(); };
+    switch (v->op) {
+    case LZ_CONST: k_fill(c, out->as<double>(), v->s, n); break;
+    case LZ_BIN: k_binary(c, v->sub, D(v->a), D(v->b), out->as<double>(), n); break;
+    case LZ_BINS: k_binary_scalar(c, v->sub, D(v->a), v->s, v->scalar_left, out->as<double>(), n); break;
+    case LZ_UNARY: k_unary_value(c, v->sub, D(v->a), out->as<double>(), n); break;
+    case LZ_CMP: k_compare(c, v->sub, D(v->a), D(v->b), out->as<uint8_t>(), n); break;
+    case LZ_CMPS: k_compare_scalar(c, v->sub, D(v->a), v->s, v->scalar_left, out->as<uint8_t>(), n); break;
+    case LZ_SEL: k_select_value(c, M(v->a), D(v->b), D(v->c), out->as<double>(), n); break;
+    case LZ_LOGIC: k_mask_logic(c, v->sub, M(v->a), v->b ? M(v->b) : M(v->a), out->as<uint8_t>(), n); break;
+    case LZ_OPMAT: opmat_apply_values(c, *v->m, D(v->a), out->as<double>()); break;
+    default: fail(EQG_ERR_UNSUPPORTED, "unknown deferred operation");
+    }
+    make_leaf(v, out);
+}
+
+// Every pending node under `root`, operands first, one kernel per node.
+void eval_per_node(Core& c, LazyNode* root)
+{
+    std::vector<std::pair<LazyNode*, int>> stack{{root, 0}};
+    while (!stack.empty()) {
+        const size_t top = stack.size() - 1;
+        LazyNode* v = stack[top].first;
+        if (v->op == LZ_LEAF) {
+            stack.pop_back();
+            continue;
+        }
+        const int k = stack[top].second;
+        if (k < 3) {
+            stack[top].second = k + 1;
+            LazyNode* kid = k == 0 ? v->a.get() : k == 1 ? v->b.get() : v->c.get();
+            if (kid && kid->op != LZ_LEAF) stack.push_back({kid, 0});
+            continue;
+        }
+        stack.pop_back();
+        eval_node(c, v);
+    }
+}
+
+// The handle takes the values of its node, which has become a leaf.
+void adopt(Core& c, const Root& r)
+{
+    if (r.coll) {
+        r.coll->val = r.node->leaf;
+        r.coll->lazy.reset();
+        c.lazy_colls.erase(r.coll);
+    } else if (r.mask) {
+        r.mask->v = r.node->leaf;
+        r.mask->lazy.reset();
+        c.lazy_masks.erase(r.mask);
+    }
+}
+
 // Evaluates `first` (pending) and every other pending handle of its length
 // that fits into the same program.
 void materialize(Core& c, Root first)
 {
+    if (!c.lazy_vm) {
+        lazy_evaluate(c, first.node);
+        adopt(c, first);
+        return;
+    }
     const int64_t n = first.node->n;
     std::vector<Root> roots{first};
     VmProgram prog;
@@ -378,12 +450,35 @@ void materialize(Core& c, Root first)
 
 void settle(Core& c, const eqg_coll* x)
 {
-    if (x && x->lazy) materialize(c, Root{x->lazy.get(), const_cast<eqg_coll*>(x), nullptr});
+    if (!x || !x->lazy) return;
+    const Root r{x->lazy.get(), const_cast<eqg_coll*>(x), nullptr};
+    // evaluated with another handle (a fused step's other results, or a
+    // shared subexpression)
+    if (r.node->op == LZ_LEAF) adopt(c, r);
+    else materialize(c, r);
 }
 
 void settle(Core& c, const eqg_mask* m)
 {
-    if (m && m->lazy) materialize(c, Root{m->lazy.get(), nullptr, const_cast<eqg_mask*>(m)});
+    if (!m || !m->lazy) return;
+    const Root r{m->lazy.get(), nullptr, const_cast<eqg_mask*>(m)};
+    if (r.node->op == LZ_LEAF) adopt(c, r);
+    else materialize(c, r);
+}
+
+void lazy_make_leaf(LazyNode* v, Buf values) { make_leaf(v, std::move(values)); }
+
+void lazy_evaluate(Core& c, LazyNode* v)
+{
+    if (v->op == LZ_LEAF) return;
+    if (c.fuse && fused_materialize(c, v)) return;
+    eval_per_node(c, v);
+}
+
+void settle_all(Core& c)
+{
+    while (!c.lazy_colls.empty()) settle(c, *c.lazy_colls.begin());
+    while (!c.lazy_masks.empty()) settle(c, *c.lazy_masks.begin());
 }
 
 const double* coll_values(Core& c, const eqg_coll* x)
@@ -437,6 +532,17 @@ LazyP lazy_make(int op, int sub, int64_t n, bool mask, LazyP a, LazyP b, LazyP c
     return v;
 }
 
+LazyP lazy_opmat(const OpMatrixP& m, LazyP a)
+{
+    auto v = std::make_shared<LazyNode>();
+    v->op = LZ_OPMAT;
+    v->n = m->n_out;
+    v->m = m;
+    v->cost = 1 + a->cost;
+    v->a = std::move(a);
+    return v;
+}
+
 eqg_coll* lazy_coll(const CoreP& core, int64_t n, LazyP node)
 {
     auto* x = new eqg_coll;
@@ -444,7 +550,7 @@ eqg_coll* lazy_coll(const CoreP& core, int64_t n, LazyP node)
     x->n = n;
     x->lazy = std::move(node);
     core->lazy_colls.insert(x);
-    if (x->lazy->cost > kLazyMaxCost) settle(*core, x);
+    if (x->lazy->cost > (core->lazy_vm ? kLazyMaxCost : kFuseMaxCost)) settle(*core, x);
     return x;
 }
 
@@ -455,7 +561,7 @@ eqg_mask* lazy_mask(const CoreP& core, int64_t n, LazyP node)
     m->n = n;
     m->lazy = std::move(node);
     core->lazy_masks.insert(m);
-    if (m->lazy->cost > kLazyMaxCost) settle(*core, m);
+    if (m->lazy->cost > (core->lazy_vm ? kLazyMaxCost : kFuseMaxCost)) settle(*core, m);
     return m;
 }
 

@@ -208,10 +208,13 @@ def two_phase_case(nx, ny, nz=None, steps=2, dt=86400.0, seed=0, corr_len=8.0, c
     return grid, case
 
 
-def swe(er, h_init, u_init, v_init, b_north, b_south, b_east, b_west, dx, dy, cfl, num_steps, on_step=None):
+def swe(er, h_init, u_init, v_init, b_north, b_south, b_east, b_west, dx, dy, cfl, num_steps, on_step=None,
+        heun_weight=0.5):
     """Explicit shallow-water equations (equelle_b200/sims/swe.cpp, op for
     op): Rusanov fluxes, wall fluxes, bathymetry source, Heun steps with the
-    CFL time step.  Returns [(w, hu, hv)] after each step (host arrays)."""
+    CFL time step.  Returns [(w, hu, hv)] after each step (host arrays).
+    heun_weight: the weights of the final average (0.5: Heun's method;
+    another value makes a different program, for tests)."""
     col = er.collection
     b_north, b_south, b_east, b_west = col(b_north), col(b_south), col(b_east), col(b_west)
     h_init, u_init, v_init = col(h_init), col(u_init), col(v_init)
@@ -306,9 +309,9 @@ def swe(er, h_init, u_init, v_init, b_north, b_south, b_east, b_west, dx, dy, cf
         dt = (cfl * h_min) / maxSpeed(w0, hu0, hv0)
         qs = eulerStage(w0, hu0, hv0, dt)
         qss = eulerStage(qs[0], qs[1], qs[2], dt)
-        w0 = (0.5 * w0) + (0.5 * qss[0])
-        hu0 = (0.5 * hu0) + (0.5 * qss[1])
-        hv0 = (0.5 * hv0) + (0.5 * qss[2])
+        w0 = (heun_weight * w0) + (heun_weight * qss[0])
+        hu0 = (heun_weight * hu0) + (heun_weight * qss[1])
+        hv0 = (heun_weight * hv0) + (heun_weight * qss[2])
         out.append((w0.value(), hu0.value(), hv0.value()))
         if on_step:
             on_step(w0, hu0, hv0)

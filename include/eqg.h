@@ -102,6 +102,8 @@ typedef struct eqg_stats {
      * scalar layout; the oracle always reports a scalar layout). */
     int64_t last_block_size;
     int64_t last_matrix_blocks;
+    /* Deferred expressions evaluated by a fused step (parameter fuse). */
+    int64_t fused_evaluations;
 } eqg_stats;
 
 /* ---- errors and identity -------------------------------------------- */
@@ -134,6 +136,10 @@ const char* eqg_backend_name(void);
  * linsolver_tail_trace (0; 1: print the SM clock cycles of every step of the
  * last fused cycle after each linear solve), lazy (0; 1:
  * defer value-only elementwise operations and evaluate them in batches),
+ * fuse (1 on two-dimensional Cartesian grids, else 0: outside Newton solves,
+ * defer value-only operations, On/Extend/gradient/divergence included, and
+ * evaluate them as a fused explicit step where the deferred expressions are
+ * one, else one kernel per operation; results are the same bits either way),
  * host_threads (0: OpenMP's default for the solver analysis),
  * linsolver_autotune (1: choose threads per block of the launch-per-step
  * V-cycle levels and the fused cycle's cluster size by timing, once per
@@ -236,6 +242,10 @@ int eqg_coll_from_host(eqg_runtime* rt, const double* v, int64_t n, eqg_coll** o
 int eqg_coll_constant(eqg_runtime* rt, double v, int64_t n, eqg_coll** out);
 int eqg_coll_size(const eqg_coll* c, int64_t* n);
 int eqg_coll_to_host(const eqg_coll* c, double* out);
+/* Computes a collection's values now if the runtime has deferred them (the
+ * fuse and lazy parameters); no effect otherwise.  The header's output()
+ * calls it before its timing marks. */
+int eqg_coll_evaluate(eqg_runtime* rt, const eqg_coll* c);
 /* Asynchronous output (the copies behind EquelleRuntimeCPU::output,
  * EquelleRuntimeCPU_impl.hpp:342-365): eqg_output_begin starts copying the
  * values to library-owned host memory after the work already enqueued and

@@ -327,6 +327,9 @@ public:
     {
         rethrowOutputError();
         int before = 0, after = 0;
+        // values the runtime has deferred are computed here, before the
+        // marks, so that they belong to the time step that made them
+        detail::check(eqg_coll_evaluate(rt_, vals.handle()));
         detail::check(eqg_runtime_mark(rt_, &before));
         if (!output_off_) {
             int64_t ticket = 0;

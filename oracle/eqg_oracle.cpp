@@ -1272,6 +1272,15 @@ int eqg_coll_to_host(const eqg_coll* c, double* out)
     });
 }
 
+// Nothing is deferred here: every operation computes its values when called.
+int eqg_coll_evaluate(eqg_runtime* rt, const eqg_coll* c)
+{
+    return guarded([&] {
+        need(rt, "runtime");
+        need(c, "collection");
+    });
+}
+
 int eqg_output_begin(eqg_runtime* rt, const eqg_coll* c, int64_t* ticket)
 {
     return guarded([&] {
