@@ -795,9 +795,12 @@ __device__ __forceinline__ double SUB(double a, double b) { return __dsub_rn(a, 
 __device__ __forceinline__ double MUL(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double DIV(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ double SQRT(double a) { return __dsqrt_rn(a); }
+// a * t + b * f with t, f = 1, 0 (m) or 0, 1: both products are exact, so
+// the sum is the chosen operand plus the other one times 0 (addition
+// commutes), one product and one sum.
 __device__ __forceinline__ double SEL(bool m, double a, double b)
 {
-    return ADD(MUL(a, m ? 1.0 : 0.0), MUL(b, m ? 0.0 : 1.0));
+    return ADD(m ? a : b, MUL(m ? b : a, 0.0));
 }
 __device__ __forceinline__ double ROW(double x) { return ADD(0.0, x); }  // 0.0 + 1.0 * x (exact product)
 // x / d, by the exact reciprocal when there is one
@@ -917,7 +920,7 @@ constexpr int kTX = kBX - 2, kTY = kBY - 2;
 // HEUN: the stage after the first, averaged with the step's start state,
 // and (WITH_MAX) the results' wave-speed maximum.
 template <bool HEUN, bool WITH_MAX>
-__global__ void __launch_bounds__(kBX * kBY) swe_stage_kernel(Grid2 g, SweConst k, SweArrays a)
+__global__ void __launch_bounds__(kBX * kBY, 4) swe_stage_kernel(Grid2 g, SweConst k, SweArrays a)
 {
     __shared__ double sw[kBY][kBX], shu[kBY][kBX], shv[kBY][kBX], sbm[kBY][kBX];  // as read
     __shared__ double sfx[4][kBY][kBX], sfy[4][kBY][kBX];  // side fluxes toward x and y faces
