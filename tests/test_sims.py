@@ -105,6 +105,38 @@ def test_reference_heat_program_matches_oracle(tmp_path):
     _check_heat(dev, ora, 20)
 
 
+def _check_swe(dev, ora, steps):
+    for tag in ("q1", "q2", "q3"):
+        g, o = _series(dev, tag), _series(ora, tag)
+        assert len(g) == len(o) == steps + 1
+        for k, (a, b) in enumerate(zip(g, o)):
+            scale = max(float(np.max(np.abs(b))), 1e-300)
+            assert float(np.max(np.abs(a - b))) <= 1e-9 * scale, "%s after step %d" % (tag, k)
+
+
+def test_reference_swe_program_matches_oracle(tmp_path):
+    """sintefmath/equelle's examples/app/out_swe.cpp (Kurganov-Levy fluxes,
+    time steps read from a file), unchanged: every output field within 1e-9
+    of its largest magnitude after every step.  On the device its values
+    are deferred (fuse=1, a 2D Cartesian grid) and, its step not being the
+    fused one, evaluated one kernel per operation: the same bits as
+    without deferral (fuse=0)."""
+    args = cases.swe_reference(str(tmp_path / "in"), 40, 30, steps=6, dt=0.3)
+    device = _need(os.path.join(REF_BUILD, "libref_out_swe_device.so"))
+    dev, ora, rd, _ = _pair("out_swe", device, _need(os.path.join(REF_BUILD, "libref_out_swe_oracle.so")), args,
+                            str(tmp_path))
+    _check_swe(dev, ora, 6)
+    assert rd.stats.fused_evaluations == 0
+    last = {}
+    for fuse in (1, 0):
+        d = str(tmp_path / ("last%d" % fuse))
+        os.makedirs(d)
+        simrun.run("out_swe", args + ["output_values=last", "output_dir=%s/" % d, "fuse=%d" % fuse], path=device)
+        last[fuse] = [np.loadtxt(os.path.join(d, "%s-last.output" % t)) for t in ("q1", "q2", "q3")]
+    for a, b in zip(last[1], last[0]):
+        assert np.array_equal(a, b)
+
+
 TWO_PHASE_TOL = ["abs_res_tol=1e-8", "linsolver_residual_tolerance=1e-8", "linsolver_max_iterations=50000"]
 
 
