@@ -83,6 +83,9 @@ struct Pattern {
     // a union)
     uint64_t concat_first = 0, concat_second = 0;
     std::shared_ptr<SolverAnalysis> analysis;  // linear-solver analysis, built on demand
+    // the analysis without multigrid, for a solve that the multigrid
+    // preconditioner did not converge (linsolver_fallback)
+    std::shared_ptr<SolverAnalysis> analysis_fallback;
 };
 using PatternP = std::shared_ptr<Pattern>;
 
@@ -485,6 +488,8 @@ struct SolveResult {
     double rel_residual = 0.0;
     int block_size = 1;   // layout of the system in the preconditioner
     int64_t blocks = 0;   // block entries of the matrix pattern
+    bool multigrid = false;  // the preconditioner was the multigrid V-cycle
+    int fallbacks = 0;       // solves repeated with block ILU(0) alone
 };
 SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const double* rhs, double* x);
 

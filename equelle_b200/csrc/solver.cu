@@ -2059,7 +2059,7 @@ void build_ap(Core& c, Level& L, const std::vector<int>& aggb)
     L.ap64 = c.allocN<double>((size_t)(slots > 0 ? slots : 1) * L.bs * L.bs);
 }
 
-std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
+std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural, bool allow_multigrid)
 {
     const auto t_start = std::chrono::steady_clock::now();
     auto since = [&] {
@@ -2088,7 +2088,8 @@ std::shared_ptr<SolverAnalysis> analyse(Core& c, const Pattern& p, bool natural)
     // coarsening stops at linsolver_mg_coarsest unknowns (at most kCoarsest)
     const int coarsest = std::max(1, std::min(kCoarsest, c.param_i("linsolver_mg_coarsest", kCoarsest)));
     // (the aggregation is geometric: Cartesian grids only)
-    const bool mg_wanted = pre == "multigrid" && c.cartesian && ncomp >= 1 && ncomp <= 8 && n > coarsest;
+    const bool mg_wanted =
+        allow_multigrid && pre == "multigrid" && c.cartesian && ncomp >= 1 && ncomp <= 8 && n > coarsest;
     // Block ILU(0) sweeps with FP32 vectors (precision "refine") converge much
     // more slowly than scalar ones on the two-phase systems; with FP64
     // vectors, FP32 matrix values ("mixed") do not change the iteration
@@ -3057,6 +3058,10 @@ SolveResult bicgstab(Core& c, SolverAnalysis& an, const T* a, Vecs<T> v, double 
         c.sync();
         std::memcpy(&h, c.pinned, sizeof(KScal));
         if (h.status != ST_RUN || enq >= max_iter) break;
+        // diverged: the residual 1e8 times the right-hand side's norm
+        // (BiCGStab's excursions on systems it solves stay far below)
+        const double bb = tol > 0 ? h.thr / (tol * tol) : 0.0;
+        if (bb > 0 && h.rr > 1e16 * bb) break;
     }
     res.converged = h.status == ST_CONV;
     res.iterations = h.iterations;
@@ -3093,7 +3098,12 @@ void to_float(Core& c, const Buf& src, Buf& dst, int64_t n)
 
 }  // namespace
 
-SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const double* rhs, double* xout)
+namespace {
+
+// One solve with the analysis in `slot` (built on first use; without
+// multigrid when allow_multigrid is false).
+SolveResult solve_with(Core& c, const PatternP& p, std::shared_ptr<SolverAnalysis>& slot, bool allow_multigrid,
+                       const double* jval, const double* rhs, double* xout)
 {
     if (p->rows != p->cols) fail(EQG_ERR_ARG, "solveForUpdate: Jacobian is not square");
     const std::string ordering = c.param_s("linsolver_ordering", "multicolor");
@@ -3112,9 +3122,9 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     // time per step)
     const int check_every = std::max(1, c.param_i("linsolver_check_every", 4));
 
-    if (!p->analysis || p->analysis->natural != natural) p->analysis = analyse(c, *p, natural);
+    if (!slot || slot->natural != natural) slot = analyse(c, *p, natural, allow_multigrid);
     c.pdl_launch = c.param_i("linsolver_pdl", 1) != 0;
-    SolverAnalysis& an = *p->analysis;
+    SolverAnalysis& an = *slot;
     SolveResult res;
     if (!an.ok) return res;  // structurally missing diagonal: ILU(0) cannot factor
     const int n = an.n;
@@ -3266,6 +3276,28 @@ SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const d
     res.block_size = L0.bs;
     res.blocks = L0.blocks;
     return res;
+}
+
+}  // namespace
+
+// A solve that the multigrid-preconditioned BiCGStab does not converge (a
+// breakdown, a zero pivot, or the iteration limit) is repeated once with
+// block ILU(0) alone (linsolver_fallback=1, the default): on systems that
+// are singular on both sides, such as the conservation form of the
+// two-phase equations, the V-cycle's coarse corrections can keep the
+// iteration from converging where the single-level preconditioner does.
+SolveResult linear_solve(Core& c, const PatternP& p, const double* jval, const double* rhs, double* xout)
+{
+    SolveResult res = solve_with(c, p, p->analysis, true, jval, rhs, xout);
+    res.multigrid = p->analysis && p->analysis->multigrid;
+    if (res.converged || !res.multigrid || c.param_i("linsolver_fallback", 1) == 0) return res;
+    if (c.verbose > 0)
+        std::printf("        linear solve: multigrid did not converge after %d iterations; block ILU(0) alone\n",
+                    res.iterations);
+    SolveResult again = solve_with(c, p, p->analysis_fallback, false, jval, rhs, xout);
+    again.iterations += res.iterations;
+    again.fallbacks = 1;
+    return again;
 }
 
 }  // namespace eqg

@@ -141,7 +141,9 @@ const char* eqg_backend_name(void);
  * evaluate them as a fused explicit step where the deferred expressions are
  * one, else one kernel per operation; results are the same bits either way),
  * host_threads (0: OpenMP's default for the solver analysis),
- * linsolver_autotune (1: choose threads per block of the launch-per-step
+ * linsolver_fallback (1: a solve that the multigrid preconditioner does not
+ * converge is repeated once with block ILU(0) alone; 0: reported as a
+ * failure), linsolver_autotune (1: choose threads per block of the launch-per-step
  * V-cycle levels and the fused cycle's cluster size by timing, once per
  * Jacobian pattern and precision; 0: 256 and the largest cluster),
  * linsolver_tune_file (a JSON file caching those choices; default
