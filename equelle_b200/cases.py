@@ -73,7 +73,7 @@ def swe(dirpath, nx=4096, ny=4096, steps=200, seed=0, sigma=40.0, binary=None):
     return args
 
 
-def swe_reference(dirpath, nx=64, ny=48, steps=6, dt=0.3, seed=0, sigma=5.0, d=10.0):
+def swe_reference(dirpath, nx=64, ny=48, steps=6, dt=0.3, seed=0, sigma=5.0, d=10.0, binary=None):
     """Inputs of the reference's generated shallow-water program
     (examples/app/out_swe.cpp, from examples/dsl/swe.equelle): the same
     seeded depth and bottom as swe() on cells of size d (the program's
@@ -82,9 +82,15 @@ def swe_reference(dirpath, nx=64, ny=48, steps=6, dt=0.3, seed=0, sigma=5.0, d=1
     computing a CFL step)."""
     os.makedirs(dirpath, exist_ok=True)
     grid, c = programs.swe_case(nx, ny, steps=steps, seed=seed, sigma=sigma, dx=d, dy=d)
+    if binary is None:
+        binary = nx * ny > 1 << 20
     args = ["%s=%s" % kv for kv in grid.items()]
     for name in ("h_init", "b_north", "b_south", "b_east", "b_west"):
-        path = _write(os.path.join(dirpath, name + ".txt"), c[name], "%.17g")
+        if binary:
+            path = os.path.join(dirpath, name + ".f64")
+            np.asarray(c[name], dtype="<f8").tofile(path)
+        else:
+            path = _write(os.path.join(dirpath, name + ".txt"), c[name], "%.17g")
         args += [name + "_from_file=true", name + "_filename=" + path]
     args += ["u_init=0", "v_init=0",
              "timesteps_filename=" + _write(os.path.join(dirpath, "timesteps.txt"), [dt] * steps, "%.17g")]

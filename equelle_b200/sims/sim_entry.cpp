@@ -79,9 +79,12 @@ int eqg_sim_main(int argc, char** argv, eqg_sim_report* report)
         if (first_start >= 0) equelle::detail::check(eqg_runtime_elapsed_ms(rt, first_start, last_end, &report->total_ms));
         if (k == 0 && !er.outputTags().empty()) {
             // an explicit program: its time steps are the intervals between
-            // the outputs of its first output tag (the end of output s to the
-            // start of output s + 1)
-            const auto& marks = er.outputMarks(er.outputTags().front());
+            // the outputs of the tag it outputs most often (the first such
+            // tag; the end of output s to the start of output s + 1)
+            std::string step_tag = er.outputTags().front();
+            for (const auto& t : er.outputTags())
+                if (er.outputMarks(t).size() > er.outputMarks(step_tag).size()) step_tag = t;
+            const auto& marks = er.outputMarks(step_tag);
             int64_t steps = 0;
             for (size_t s = 0; s + 1 < marks.size() && s < 4096; ++s, ++steps) {
                 double ms = 0.0;
