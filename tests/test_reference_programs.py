@@ -89,7 +89,7 @@ def _run(name, lib, args, out):
 
 
 @pytest.mark.parametrize("name,inputs,tol,unanchored,device_args", PROGRAMS,
-                         ids=[p[0] if isinstance(p, tuple) else None for p in PROGRAMS])
+                         ids=[None if hasattr(p, "marks") else p[0] for p in PROGRAMS])
 def test_reference_program_device_matches_oracle(tmp_path, name, inputs, tol, unanchored, device_args):
     libs = {}
     for side in ("device", "oracle"):
