@@ -318,12 +318,18 @@ def main():
     args += a.extra
     if a.kernel_profile:
         args.append("time_kernel=*")
+    flushed = a.workload in FLUSHED
+    if flushed:
+        args.append("flush_l2=256")
     rp.barrier()
     with ClockSampler(local_rank) as clk:
         rep = simrun.run(name, args)
     if rep.solves < W + K:
         raise SystemExit("simulator ran %d solves, expected %d" % (rep.solves, W + K))
-    ms = rp.max(timed_window(rep, W, K))
+    if flushed:
+        ms = rp.max(sum(rep.solve_ms[i] for i in range(W, W + K)))
+    else:
+        ms = rp.max(timed_window(rep, W, K))
     infos = window_counts(rep, W, K)
     value = rp.throughput(K, ms)
     st = rep.stats
@@ -527,12 +533,20 @@ def forms_vs_oracle(local_rank, a, n=(32, 32, 32), steps=3):
     return res
 
 
+# Workloads whose working set fits in the 126 MB L2: 256 MB are written
+# before each time step's start mark (runtime parameter flush_l2), and each
+# step is timed between its own marks, which exclude that write.
+FLUSHED = ("heat",)
+
+
 def config(a, desc, cells):
     """The workload, the same in both arms (each line names its solver
     outside the config)."""
+    l2 = ("working set smaller than L2: 256 MB written before each time step, each step timed between its own "
+          "marks (the write excluded)" if a.workload in FLUSHED else
+          "working set larger than L2 (126 MB), no flush")
     return {"workload": desc, "cells": cells, "precision": a.precision,
-            "dt": "1 day" if a.workload != "heat" else "0.5",
-            "l2": "working set larger than L2 (126 MB), no flush", "parallelism": "replicas"}
+            "dt": "1 day" if a.workload != "heat" else "0.5", "l2": l2, "parallelism": "replicas"}
 
 
 def main_many(a, rp):

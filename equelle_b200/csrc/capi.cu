@@ -1468,6 +1468,15 @@ int eqg_newton_solve(eqg_runtime* rt, eqg_residual_fn fn, void* user, const eqg_
             }
         } no_deferral{c, c.lazy, c.fuse};
         c.lazy = c.fuse = false;
+        // flush_l2=<MB>: that many MB written before the solve's start mark,
+        // so that a solve timed between its own marks finds none of its data
+        // in L2 (for working sets smaller than L2)
+        const int flush_mb = c.param_i("flush_l2", 0);
+        if (flush_mb > 0) {
+            const size_t nbytes = (size_t)flush_mb << 20;
+            if (!c.flush_buf || c.flush_buf->bytes < nbytes) c.flush_buf = c.alloc(nbytes);
+            EQG_CUDA(cudaMemsetAsync(c.flush_buf->ptr, 0, nbytes, c.stream));
+        }
         const int m0 = mark(c);
         c.newton_solves++;
         const int64_t krylov0 = c.solver.krylov_iterations;

@@ -76,6 +76,7 @@ Core::~Core()
     for (auto& kv : derived_sets) eqg_set_release(kv.second);
     derived_sets.clear();
     fuse_state.reset();
+    flush_buf.reset();
     pattern_cache.clear();
     opmat_cache.clear();
     identity_patterns.clear();

@@ -234,6 +234,7 @@ struct Core {
     int64_t lazy_passes = 0;
     int64_t fused_evaluations = 0;
     std::shared_ptr<struct FuseState> fuse_state;  // fused.cu: verified operators and arrays, cached maxima
+    Buf flush_buf;  // written before each Newton solve under flush_l2
     // asynchronous output copies (eqg_output_*): device -> pinned host on
     // their own stream.  The ticket table and the pinned pool are shared with
     // the thread that waits for copies (mutex); device buffers of finished

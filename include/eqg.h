@@ -150,7 +150,9 @@ const char* eqg_backend_name(void);
  * $EQG_TUNE_FILE, else none), spgemm_plan / span_share / jac_concat /
  * jac_defer / stencil_ops (1; 0 switches off an assembly fast path, for
  * comparisons),
- * gather_rows (0), time_kernel
+ * gather_rows (0), flush_l2 (0; n: n MB written before each Newton solve's
+ * start mark, so that a solve timed between its marks starts with a cold L2),
+ * time_kernel
  * (a kernel name, or "*", to time with CUDA events) and device (CUDA device
  * index; default: the calling thread's current device).  grid_filename
  * (instead of grid_dim, nx, ...) reads the grid from a file: the arrays of an
