@@ -606,6 +606,8 @@ def main_many(a, rp):
                                        % (a.instances, side_max, a.steps, a.slots),
                            "precision": "mixed (batched), double (sequential and batched_fp64)",
                            "sequential_sample": "the first %d of the same instances" % len(seq_reqs),
+                           "l2": "no flush: whole runs on the host clock; a small instance run alone keeps its "
+                                 "data in L2 between steps, instances run together share it",
                            "parallelism": "replicas"},
                 "batched": bat, "batched_fp64": bat64, "sequential_fp64": seq,
                 "speedup_vs_sequential": bat["instance_steps_per_s"] / seq["instance_steps_per_s"],
@@ -630,6 +632,8 @@ def main_many(a, rp):
                         "10-%d steps)" % (side_max, max_steps),
                 "config": {"workload": "serving loop, Poisson arrivals at %s req/s, %d requests per rate, up to %d on "
                                        "the GPU at once, admission under 150 GB" % (a.rates, a.requests, a.slots),
+                           "l2": "no flush: whole requests on the host clock; a small request run alone keeps "
+                                 "its data in L2 between steps, requests run together share it",
                            "parallelism": "replicas"},
                 "per_rate": per_rate, "one_at_a_time_fp64": seq,
                 "throughput_vs_one_at_a_time": top["requests_per_s"] / seq["requests_per_s"]}
